@@ -1,0 +1,143 @@
+/*
+ * om.h -- CPU restatement of ProteusGPU's per-timestep mesh-and-flux path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the oracle that the CUDA path is
+ * checked against (and the "port" CPU baseline); the product never links it.
+ *
+ * It restates, in plain C with runtime dimension and K, the reference's
+ *   - periodic ghost layer + unit-box scaling   (src/voronoi/periodic_mesh.cpp:16-184)
+ *   - exact K nearest neighbours               (src/knn/knn.cpp:16-347)
+ *   - Ray et al. half-space clipping + security-radius certificate
+ *                                              (src/voronoi/cell.cpp:42-411,
+ *                                               src/voronoi/voronoi.cpp:201-241)
+ *   - cell -> mesh extraction                  (src/voronoi/cell.cpp:416-669)
+ *   - CFL time step and HLL flux update        (src/hydro/finite_volume_solver.cpp:43-186,
+ *                                               src/hydro/riemann.cpp:7-124)
+ * with the same FP64 operation sequence (build with -ffp-contract=off), so that
+ * its results are bit-identical to the reference build in oracle/_ref.
+ *
+ * It also defines the semantics of what the reference does not have and the
+ * moving-mesh workloads need: reflective (mirror) ghosts, mesh-point drift,
+ * conserved-variable carry across re-meshing, face-pair-symmetric areas, the
+ * outward-normal ("physical") flux sign, the certified-K record and cell
+ * centroids.  Each such function says so.
+ */
+#ifndef PGPU_ORACLE_OM_H
+#define PGPU_ORACLE_OM_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Cell status codes, same values as the reference's `Status` (allvars.h:13-20). */
+enum {
+    OM_TRIANGLE_OVERFLOW = 0,
+    OM_VERTEX_OVERFLOW = 1,
+    OM_INCONSISTENT_BOUNDARY = 2,
+    OM_SECURITY_RADIUS_NOT_REACHED = 3,
+    OM_SUCCESS = 4,
+    OM_NEEDS_EXACT_PREDICATES = 5,
+    OM_NOT_COMPUTED = 6 /* ghost cell skipped by a hydro-only build */
+};
+
+enum { OM_PERIODIC = 0, OM_REFLECTIVE = 1 };
+
+/* Clipping pool limits, the reference's defaults (Config.sh:37-38). */
+#define OM_MAX_P 64
+#define OM_MAX_T 96
+
+typedef struct {
+    int dim;
+    long n_seeds;   /* hydro + ghost cells */
+    long n_hydro;
+    long num_faces;
+    double *seeds;      /* n_seeds * 3, physical coordinates (z = 0 in 2D) */
+    double *volumes;    /* n_seeds */
+    long *face_counts;  /* n_seeds */
+    long *face_ptr;     /* n_seeds, CSR start in the face arrays */
+    int *neighbor;      /* num_faces; input/ghost id of the other cell, -1 = box face */
+    double *normal;     /* num_faces * 3; unit plane normal, pointing into the cell (reference convention) */
+    double *area;       /* num_faces; edge length (2D) or face area (3D), physical units */
+    long *ghost_ids;    /* n_seeds - n_hydro; hydro id each ghost copies */
+    int *ghost_code;    /* n_seeds - n_hydro; image code, see om_image_code() */
+    int *status;        /* n_seeds */
+    int *cert_k;        /* n_seeds; 1-based neighbour index where the certificate closed, 0 if never */
+    double *centroid;   /* n_seeds * 3, physical coordinates */
+} om_mesh;
+
+/* ---- ghosts -------------------------------------------------------------- */
+
+/* Image code of a ghost: per axis a in 0..dim-1 a base-3 digit d_a, with
+ * d_a = 0 for no change, 1 for the image across the low wall (periodic shift
+ * +1 or mirror x -> -x), 2 for the image across the high wall (shift -1 or
+ * mirror x -> 2 - x).  code = d_0 + 3 d_1 + 9 d_2. */
+int om_image_code(const int *shift, int dim);
+
+/* Number of ghost regions (8 in 2D, 26 in 3D) and their shift vectors in the
+ * reference's order (periodic_mesh.cpp:71-110). */
+int om_num_regions(int dim);
+void om_region_shift(int dim, int r, int *shift3);
+
+/* Builds the extended point set (hydro points first, then ghosts in the
+ * reference's order) scaled into the unit box as the reference does
+ * (periodic_mesh.cpp:63-126).  `ext` needs capacity (1 + num_regions) * n * dim.
+ * Returns the number of extended points. */
+long om_ghosts(int dim, int boundary, double buff, const double *pts, long n,
+               double *ext, long *ghost_src, int *ghost_code);
+
+/* ---- KNN --------------------------------------------------------------- */
+
+/* Exact K nearest neighbours of every point of `pts` (n x dim, unit box),
+ * excluding itself, ascending by (squared distance, index).  Unfilled slots are
+ * UINT32_MAX.  Uses a uniform grid with Chebyshev-ring search as in
+ * knn.cpp:16-315.  Returns 0. */
+int om_knn(int dim, const double *pts, long n, int K, uint32_t *out);
+
+/* ---- cells ------------------------------------------------------------- */
+
+/* Clips and extracts cells [0, n_cells) of the extended unit-box point set
+ * (cells >= n_compute are skipped and get OM_NOT_COMPUTED), producing a mesh
+ * in unit-box units.  knn is n_ext x K in extended ids. */
+int om_cells(int dim, const double *ext, long n_ext, long n_hydro, const uint32_t *knn, int K,
+             long n_compute, om_mesh *mesh);
+
+/* The whole mesh build: ghosts (periodic or reflective within `buff`), unit-box
+ * scaling, KNN, clipping, extraction and the rescale back
+ * (periodic_mesh.cpp:44-184).  hydro_only skips the ghost cells. */
+int om_build_mesh(int dim, int boundary, double buff, int K, const double *pts, long n,
+                  int hydro_only, om_mesh *mesh);
+
+void om_mesh_free(om_mesh *mesh);
+
+/* ---- hydro ------------------------------------------------------------- */
+
+/* hydro::dt_CFL (finite_volume_solver.cpp:151-186). v is n_hydro x dim. */
+double om_dt_cfl(const om_mesh *mesh, double cfl, double gamma, const double *rho,
+                 const double *v, const double *E);
+
+/* hydro::hydro_step (finite_volume_solver.cpp:43-123) in place, reference
+ * arithmetic: inward stored normal, each side's own face area. Returns the
+ * number of faces whose neighbour is a box face (the reference would crash). */
+long om_hydro_step_ref(const om_mesh *mesh, double dt, double gamma, double *rho, double *v, double *E);
+
+/* Extension.  One moving-mesh step on conserved variables:
+ *   W = (m/V, p/m, e/V); dt = CFL min (reference formula);
+ *   Q_i -= dt * sum_faces HLL(W_i, W_j, n_out) A_sym;  x_i += v_i dt (v at step start),
+ * then wrap (periodic) or reflect (reflective) into [0,1)^dim.
+ * n_out is the outward normal (the negated stored one); A_sym is the area computed
+ * by the lower hydro id of the face pair, so the update is antisymmetric.
+ * mirror ghosts flip the velocity components normal to their walls.
+ * If fixed_dt > 0 it is used instead of the CFL step.  Returns dt. */
+double om_step_moving(const om_mesh *mesh, double cfl, double fixed_dt, double gamma, int boundary,
+                      double *x, double *mass, double *mom, double *energy, long *n_unpaired);
+
+/* Face-pair symmetric areas (extension): out[f] = area of the same face as seen from
+ * the lower hydro id.  Returns the number of faces with no partner found. */
+long om_symmetric_area(const om_mesh *mesh, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

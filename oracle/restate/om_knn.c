@@ -1,0 +1,134 @@
+#define _GNU_SOURCE
+/*
+ * Exact K nearest neighbours (test-infrastructure oracle).
+ *
+ * Restates knn::init / sort_points_into_grid / cpu_knearest
+ * (src/knn/knn.cpp:16-315): points are binned into an N_grid^D uniform grid
+ * (N_grid from the same expression, knn.cpp:22), and each query scans
+ * Chebyshev rings of bins outwards, stopping before ring r once its K-th best
+ * squared distance is below ((r-1)/N_grid)^2 (knn.cpp:267-273).  The squared
+ * distance is dist2_point's dx*dx + dy*dy (+ dz*dz) (knn.h:64-75); the query
+ * itself is skipped (knn.cpp:285).
+ *
+ * Differences, all of which leave the result equal to the reference's whenever
+ * squared distances are distinct:
+ *   - neighbours are ordered by (squared distance, index) instead of the
+ *     heap's unspecified order among equal distances;
+ *   - bins are addressed by (i, j, k) and rings clipped to the grid, so no bin
+ *     is visited twice (the reference's linear offsets alias across rows,
+ *     knn.cpp:58,77, which only adds candidates);
+ *   - the ring count is not capped at 15 and grids below 16^D are allowed.
+ */
+#include "om.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+static int n_grid_for(long n, int dim) {
+    int g = (int)round(pow((double)(n / 3.1f), (double)(1.0f / (float)dim)));
+    return g < 1 ? 1 : g;
+}
+
+static int bin_coord(double x, int G) {
+    int i = (int)floor(x * (double)G);
+    if (i < 0) i = 0;
+    if (i > G - 1) i = G - 1;
+    return i;
+}
+
+static double dist2(const double *a, const double *b, int dim) {
+    double dx = a[0] - b[0];
+    double dy = a[1] - b[1];
+    if (dim == 2) return dx * dx + dy * dy;
+    double dz = a[2] - b[2];
+    return dx * dx + dy * dy + dz * dz;
+}
+
+/* insert (d, id) into the ascending list of length *cnt (capacity K) */
+static void topk_insert(double *bd, uint32_t *bi, int *cnt, int K, double d, uint32_t id) {
+    int c = *cnt;
+    if (c == K) {
+        if (d > bd[K - 1] || (d == bd[K - 1] && id >= bi[K - 1])) return;
+        c = K - 1;
+    }
+    int pos = c;
+    while (pos > 0 && (bd[pos - 1] > d || (bd[pos - 1] == d && bi[pos - 1] > id))) {
+        bd[pos] = bd[pos - 1];
+        bi[pos] = bi[pos - 1];
+        pos--;
+    }
+    bd[pos] = d;
+    bi[pos] = id;
+    if (*cnt < K) (*cnt)++;
+}
+
+int om_knn(int dim, const double *pts, long n, int K, uint32_t *out) {
+    const int G = n_grid_for(n, dim);
+    const long nb = dim == 2 ? (long)G * G : (long)G * G * G;
+    long *start = (long *)calloc(nb + 1, sizeof(long));
+    long *order = (long *)malloc((n > 0 ? n : 1) * sizeof(long));
+    int *bin = (int *)malloc((n > 0 ? n : 1) * sizeof(int));
+    for (long i = 0; i < n; i++) {
+        const double *p = pts + i * dim;
+        int b = bin_coord(p[0], G) + G * bin_coord(p[1], G);
+        if (dim == 3) b += G * G * bin_coord(p[2], G);
+        bin[i] = b;
+        start[b + 1]++;
+    }
+    for (long b = 0; b < nb; b++) start[b + 1] += start[b];
+    {
+        long *fill = (long *)calloc(nb, sizeof(long));
+        for (long i = 0; i < n; i++) order[start[bin[i]] + fill[bin[i]]++] = i;
+        free(fill);
+    }
+
+#pragma omp parallel
+    {
+        double *bd = (double *)malloc(K * sizeof(double));
+        uint32_t *bi = (uint32_t *)malloc(K * sizeof(uint32_t));
+#pragma omp for schedule(dynamic, 256)
+        for (long q = 0; q < n; q++) {
+            const double *p = pts + q * dim;
+            int c[3] = {bin_coord(p[0], G), bin_coord(p[1], G), dim == 3 ? bin_coord(p[2], G) : 0};
+            int cnt = 0;
+            for (int r = 0; r <= G; r++) {
+                if (r >= 1 && cnt == K) {
+                    double md = (double)(r - 1) / (double)G;
+                    if (bd[K - 1] < md * md) break;
+                }
+                int zlo = dim == 3 ? -r : 0, zhi = dim == 3 ? r : 0;
+                for (int dz = zlo; dz <= zhi; dz++) {
+                    int z = c[2] + dz;
+                    if (dim == 3 && (z < 0 || z >= G)) continue;
+                    for (int dy = -r; dy <= r; dy++) {
+                        int y = c[1] + dy;
+                        if (y < 0 || y >= G) continue;
+                        for (int dx = -r; dx <= r; dx++) {
+                            int ar = abs(dx);
+                            if (abs(dy) > ar) ar = abs(dy);
+                            if (abs(dz) > ar) ar = abs(dz);
+                            if (ar != r) continue;
+                            int x = c[0] + dx;
+                            if (x < 0 || x >= G) continue;
+                            long b = x + (long)G * y + (long)G * G * z;
+                            for (long s = start[b]; s < start[b + 1]; s++) {
+                                long j = order[s];
+                                if (j == q) continue;
+                                topk_insert(bd, bi, &cnt, K, dist2(p, pts + j * dim, dim), (uint32_t)j);
+                            }
+                        }
+                    }
+                }
+            }
+            for (int t = 0; t < K; t++) out[q * K + t] = t < cnt ? bi[t] : UINT32_MAX;
+        }
+        free(bd);
+        free(bi);
+    }
+    free(start);
+    free(order);
+    free(bin);
+    return 0;
+}
