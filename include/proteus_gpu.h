@@ -1,0 +1,189 @@
+/*
+ * proteus_gpu.h -- C ABI of the B200 (sm_100a) mesh-and-flux path.
+ *
+ * Plain pointers and sizes only.  One context owns one CUDA stream and all
+ * device buffers of one simulation; calls on one context are not reentrant,
+ * different contexts are independent.  Every entry point returns 0 on success
+ * or a negative PGPU_E* code; pgpu_last_error() gives the message.
+ *
+ * Which reference interface each entry point replaces is cited beside it
+ * (paths relative to the reference project's root).  The reference's C++
+ * signatures themselves are kept by the drop-in translation units in
+ * proteusgpu_b200/dropin/, which forward to this ABI.
+ *
+ * Layouts follow the reference's VMesh (src/voronoi/voronoi.h:22-41):
+ *   cells  : seeds double[3] (z = 0 in 2D), volumes, face_counts, face_ptr (u64)
+ *   faces  : neighbor_cell int32 (-1 = bounding-box face), face_normal double[3]
+ *            (unit, pointing from the neighbour into the cell), face_area
+ *   ghosts : ghost_ids u64, the hydro id each ghost cell copies
+ * and primitives follow primvars (src/global/allvars.h:203-207): rho, v
+ * (dim doubles per cell), E (total energy per unit volume).
+ */
+#ifndef PROTEUS_GPU_H
+#define PROTEUS_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PGPU_ABI_VERSION 1
+
+/* error codes */
+#define PGPU_OK 0
+#define PGPU_EINVAL (-1)   /* bad argument */
+#define PGPU_ECUDA (-2)    /* CUDA runtime error */
+#define PGPU_ESTATE (-3)   /* call out of order (e.g. no mesh yet) */
+#define PGPU_ECAPACITY (-4) /* a size exceeds a fixed limit */
+#define PGPU_EMESH (-5)    /* mesh unusable for the requested step (failed cells, box faces) */
+
+/* boundary handling of the ghost layer */
+#define PGPU_PERIODIC 0   /* shifted copies, src/voronoi/periodic_mesh.cpp:63-112 */
+#define PGPU_REFLECTIVE 1 /* mirrored copies (extension) */
+
+/* flux conventions */
+#define PGPU_FLUX_REFERENCE 0 /* stored (inward) normal, each cell's own face area: riemann.cpp:7-45 as is */
+#define PGPU_FLUX_PHYSICAL 1  /* outward normal, face-pair-symmetric area: conservative to round-off */
+
+/* cell status codes: the reference's Status enum, src/global/allvars.h:13-20 */
+#define PGPU_TRIANGLE_OVERFLOW 0
+#define PGPU_VERTEX_OVERFLOW 1
+#define PGPU_INCONSISTENT_BOUNDARY 2
+#define PGPU_SECURITY_RADIUS_NOT_REACHED 3
+#define PGPU_SUCCESS 4
+#define PGPU_NEEDS_EXACT_PREDICATES 5
+#define PGPU_NOT_COMPUTED 6 /* ghost cell, skipped by the per-step path */
+
+typedef struct pgpu_ctx pgpu_ctx;
+
+typedef struct {
+    int dim;          /* 2 or 3 (the reference's dim_2D / dim_3D) */
+    int k;            /* neighbour budget, the reference's _K_ (Config.sh:34); 1..256 */
+    int boundary;     /* PGPU_PERIODIC or PGPU_REFLECTIVE */
+    int flux_mode;    /* PGPU_FLUX_REFERENCE or PGPU_FLUX_PHYSICAL */
+    double buff;      /* ghost layer width, the reference's global `buff` (allvars.cpp:13) */
+    double gamma;     /* adiabatic index, the reference's global `_gamma_` (allvars.cpp:14) */
+    int device;       /* CUDA device ordinal */
+    int verbose;      /* 0 = silent */
+} pgpu_params;
+
+/* Fills p with the reference's defaults: dim 3, K 190, periodic, reference flux,
+ * buff 0.04, gamma 5/3, device 0. */
+void pgpu_default_params(pgpu_params *p);
+
+int pgpu_create(const pgpu_params *p, pgpu_ctx **out);
+void pgpu_destroy(pgpu_ctx *ctx);
+const char *pgpu_last_error(const pgpu_ctx *ctx);
+int pgpu_abi_version(void);
+
+/* ---------------------------------------------------------------- KNN ---
+ * knn::init + knn::solve + knn::get_knearest + knn::get_permutation
+ * (src/knn/knn.h:36-57, src/knn/knn.cpp:16-234).  pts: n x dim doubles in the
+ * unit box, host memory.  out: n x k neighbour ids (input ids, ascending by
+ * squared distance then id; UINT32_MAX where fewer than k exist).  The sorted
+ * order is internal; it is returned by pgpu_knn_sorted for the drop-in's
+ * knn_problem. */
+int pgpu_knn(pgpu_ctx *ctx, const double *pts, int64_t n, uint32_t *out);
+
+/* After pgpu_knn: the internal grid order (knn::get_points / get_permutation,
+ * src/knn/knn.cpp:445-455): sorted points (n x dim) and perm[sorted] = input id;
+ * and the grid resolution.  Any pointer may be NULL. */
+int pgpu_knn_sorted(pgpu_ctx *ctx, double *sorted_pts, uint32_t *perm, int *n_grid);
+
+/* ---------------------------------------------------------------- mesh ---
+ * voronoi::compute_periodic_mesh (src/voronoi/periodic_mesh.cpp:44-184):
+ * ghosts within buff (periodic or mirrored), unit-box scaling, KNN, clipping
+ * with the security-radius certificate, extraction and rescale.  All cells,
+ * hydro and ghost, are computed, as in the reference.  The mesh stays on the
+ * device; sizes are returned. */
+int pgpu_periodic_mesh(pgpu_ctx *ctx, const double *pts, int64_t n, int64_t *n_seeds, int64_t *num_faces);
+
+/* voronoi::compute_mesh (src/voronoi/voronoi.cpp:103-151) on n points already
+ * in the unit box: no ghosts, no scaling; n_hydro = n. */
+int pgpu_compute_mesh(pgpu_ctx *ctx, const double *pts, int64_t n, int64_t *num_faces);
+
+/* Copies the current mesh to host arrays in the reference's VMesh layout,
+ * cells in input order with faces contiguous per cell
+ * (src/voronoi/voronoi.cpp:298-419 unpermute_vmesh).  Any pointer may be NULL.
+ * status and cert_k are per cell; cert_k is the 1-based neighbour index at which
+ * the certificate closed (0 if it did not); centroid is an extension. */
+int pgpu_download_mesh(pgpu_ctx *ctx, double *seeds, double *volumes, uint64_t *face_counts,
+                       uint64_t *face_ptr, int32_t *neighbor, double *normal, double *area,
+                       uint64_t *ghost_ids, int32_t *status, int32_t *cert_k, double *centroid);
+
+/* Mesh sizes: cells (hydro + ghost), hydro cells, faces. */
+int pgpu_mesh_sizes(pgpu_ctx *ctx, int64_t *n_seeds, int64_t *n_hydro, int64_t *num_faces);
+
+/* Replaces the device mesh by a host VMesh (for the drop-in hydro:: calls on a
+ * mesh built elsewhere).  normal is num_faces x 3. */
+int pgpu_upload_mesh(pgpu_ctx *ctx, int64_t n_seeds, int64_t n_hydro, int64_t num_faces, const double *volumes,
+                     const uint64_t *face_counts, const uint64_t *face_ptr, const int32_t *neighbor,
+                     const double *normal, const double *area, const uint64_t *ghost_ids);
+
+/* --------------------------------------------------------------- hydro ---
+ * Primitive state of the n_hydro cells (hydro::init, finite_volume_solver.cpp:8-31). */
+int pgpu_set_prim(pgpu_ctx *ctx, const double *rho, const double *v, const double *E, int64_t n);
+int pgpu_get_prim(pgpu_ctx *ctx, double *rho, double *v, double *E);
+
+/* hydro::dt_CFL (src/hydro/finite_volume_solver.cpp:151-186) on the current mesh. */
+int pgpu_dt_cfl(pgpu_ctx *ctx, double cfl, double *dt);
+
+/* hydro::hydro_step (src/hydro/finite_volume_solver.cpp:43-123) on the current
+ * mesh and primitives, in the context's flux_mode. */
+int pgpu_hydro_step(pgpu_ctx *ctx, double dt);
+
+/* -------------------------------------------------- moving-mesh stepping ---
+ * Extension (the reference's time loop, src/main.cpp:50-63, keeps its mesh
+ * fixed).  The simulation state is conserved mass, momentum and energy per
+ * cell plus the generating points.  pgpu_sim_init builds the first mesh,
+ * converts the primitives (and an optional per-cell energy deposit, e.g. a
+ * Sedov blast) to conserved variables.  Host arrays: pos n x dim, v n x dim. */
+int pgpu_sim_init(pgpu_ctx *ctx, const double *pos, const double *rho, const double *v, const double *E,
+                  const double *deposit, int64_t n);
+
+/* One full step on the device: ghosts, sort, KNN, clip + certificate,
+ * extraction (hydro cells only), CFL dt (unless fixed_dt > 0), HLL fluxes with
+ * the conserved update, and drift of the points with their cells' velocity.
+ * dt_out (host, may be NULL) receives the step's dt; passing NULL keeps the
+ * step free of device-to-host synchronisation. */
+int pgpu_sim_step(pgpu_ctx *ctx, double cfl, double fixed_dt, double *dt_out);
+
+/* Same step with the inputs given in, and the results read back to, host
+ * memory: positions and conserved state are copied to the device before the
+ * step and back after it (the end-to-end form of the call). */
+int pgpu_sim_step_host(pgpu_ctx *ctx, double cfl, double fixed_dt, double *pos, double *mass, double *mom,
+                       double *energy, double *dt_out);
+
+/* Current simulation state (host arrays; any may be NULL). */
+int pgpu_sim_get(pgpu_ctx *ctx, double *pos, double *mass, double *mom, double *energy);
+int pgpu_sim_set(pgpu_ctx *ctx, const double *pos, const double *mass, const double *mom, const double *energy);
+
+typedef struct {
+    int64_t n_hydro, n_ext, num_faces;
+    int64_t failed_cells;       /* hydro cells whose status is not SUCCESS */
+    int64_t box_faces;          /* hydro faces on the bounding box (ghost layer too thin) */
+    int64_t unpaired_faces;     /* faces whose reverse face was not found */
+    int64_t knn_candidates;     /* distance evaluations in the last KNN (if counted) */
+    double last_dt;
+    double total_mass, total_energy, total_mom[3]; /* deterministic sums over hydro cells */
+    int32_t cert_k_max;
+    int32_t n_grid;
+} pgpu_stats;
+
+/* Statistics of the last step (synchronises the stream). */
+int pgpu_sim_stats(pgpu_ctx *ctx, pgpu_stats *out);
+
+/* Per-stage device times of the last step in milliseconds, measured with CUDA
+ * events when timing is enabled: ghosts, sort, knn, clip, hydro. */
+int pgpu_enable_timing(pgpu_ctx *ctx, int on);
+int pgpu_stage_times(pgpu_ctx *ctx, float *ms5);
+
+/* The CUDA stream of the context (a cudaStream_t), for callers that time or
+ * order work around it. */
+void *pgpu_stream(pgpu_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PROTEUS_GPU_H */

@@ -536,9 +536,6 @@ int om_cells(int dim, const double *ext, long n_ext, long n_hydro, const uint32_
 #pragma omp parallel for schedule(dynamic, 64)
         for (long i = c0; i < c1; i++) {
             cell_out_t *o = &outs[i - c0];
-            m->seeds[3 * i] = ext[dim * i];
-            m->seeds[3 * i + 1] = ext[dim * i + 1];
-            m->seeds[3 * i + 2] = dim == 3 ? ext[dim * i + 2] : 0.0;
             if (i >= n_compute) {
                 m->status[i] = OM_NOT_COMPUTED;
                 o->nf = 0;
@@ -546,6 +543,13 @@ int om_cells(int dim, const double *ext, long n_ext, long n_hydro, const uint32_
                 continue;
             }
             one_cell(dim, ext, i, knn, K, o, &m->status[i], &m->cert_k[i]);
+            /* extract_cell_to_vmesh writes the seed only for extracted cells
+               (cell.cpp:418-420); the others keep calloc's zeros */
+            if (m->status[i] == OM_SUCCESS) {
+                m->seeds[3 * i] = ext[dim * i];
+                m->seeds[3 * i + 1] = ext[dim * i + 1];
+                m->seeds[3 * i + 2] = dim == 3 ? ext[dim * i + 2] : 0.0;
+            }
         }
         for (long i = c0; i < c1; i++) {
             const cell_out_t *o = &outs[i - c0];

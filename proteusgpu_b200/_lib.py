@@ -1,0 +1,103 @@
+"""ctypes binding of libproteus_gpu.so (the C ABI in include/proteus_gpu.h).
+
+The library is built in-tree by proteusgpu_b200/build.py.  There is no CPU
+fallback: if the library cannot be loaded, or no CUDA device is present, the
+calls raise.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libproteus_gpu.so")
+
+PGPU_PERIODIC, PGPU_REFLECTIVE = 0, 1
+PGPU_FLUX_REFERENCE, PGPU_FLUX_PHYSICAL = 0, 1
+ERRORS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "call out of order",
+          -4: "capacity exceeded", -5: "mesh unusable"}
+
+# every symbol include/proteus_gpu.h declares
+EXPORTED = [
+    "pgpu_default_params", "pgpu_create", "pgpu_destroy", "pgpu_last_error", "pgpu_abi_version",
+    "pgpu_knn", "pgpu_knn_sorted", "pgpu_periodic_mesh", "pgpu_compute_mesh", "pgpu_download_mesh",
+    "pgpu_mesh_sizes", "pgpu_upload_mesh", "pgpu_set_prim", "pgpu_get_prim", "pgpu_dt_cfl",
+    "pgpu_hydro_step", "pgpu_sim_init", "pgpu_sim_step", "pgpu_sim_step_host", "pgpu_sim_get",
+    "pgpu_sim_set", "pgpu_sim_stats", "pgpu_enable_timing", "pgpu_stage_times", "pgpu_stream",
+]
+
+
+class Params(C.Structure):
+    _fields_ = [("dim", C.c_int), ("k", C.c_int), ("boundary", C.c_int), ("flux_mode", C.c_int),
+                ("buff", C.c_double), ("gamma", C.c_double), ("device", C.c_int), ("verbose", C.c_int)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("n_hydro", C.c_int64), ("n_ext", C.c_int64), ("num_faces", C.c_int64),
+                ("failed_cells", C.c_int64), ("box_faces", C.c_int64), ("unpaired_faces", C.c_int64),
+                ("knn_candidates", C.c_int64), ("last_dt", C.c_double), ("total_mass", C.c_double),
+                ("total_energy", C.c_double), ("total_mom", C.c_double * 3), ("cert_k_max", C.c_int32),
+                ("n_grid", C.c_int32)]
+
+
+_LIB = None
+vp = C.c_void_p
+i64 = C.c_int64
+dbl = C.c_double
+
+
+def load(path: str = LIB_PATH):
+    """Loads the library (build it with ``python -m proteusgpu_b200.build``)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise RuntimeError(f"{path} is missing: build it with `python -m proteusgpu_b200.build` "
+                           "(there is no CPU fallback)")
+    L = C.CDLL(path)
+    L.pgpu_default_params.argtypes = [C.POINTER(Params)]
+    L.pgpu_default_params.restype = None
+    L.pgpu_create.argtypes = [C.POINTER(Params), C.POINTER(vp)]
+    L.pgpu_destroy.argtypes = [vp]
+    L.pgpu_destroy.restype = None
+    L.pgpu_last_error.argtypes = [vp]
+    L.pgpu_last_error.restype = C.c_char_p
+    L.pgpu_abi_version.restype = C.c_int
+    L.pgpu_knn.argtypes = [vp, vp, i64, vp]
+    L.pgpu_knn_sorted.argtypes = [vp, vp, vp, vp]
+    L.pgpu_periodic_mesh.argtypes = [vp, vp, i64, vp, vp]
+    L.pgpu_compute_mesh.argtypes = [vp, vp, i64, vp]
+    L.pgpu_download_mesh.argtypes = [vp] + [vp] * 11
+    L.pgpu_mesh_sizes.argtypes = [vp, vp, vp, vp]
+    L.pgpu_upload_mesh.argtypes = [vp, i64, i64, i64] + [vp] * 7
+    L.pgpu_set_prim.argtypes = [vp, vp, vp, vp, i64]
+    L.pgpu_get_prim.argtypes = [vp, vp, vp, vp]
+    L.pgpu_dt_cfl.argtypes = [vp, dbl, vp]
+    L.pgpu_hydro_step.argtypes = [vp, dbl]
+    L.pgpu_sim_init.argtypes = [vp, vp, vp, vp, vp, vp, i64]
+    L.pgpu_sim_step.argtypes = [vp, dbl, dbl, vp]
+    L.pgpu_sim_step_host.argtypes = [vp, dbl, dbl, vp, vp, vp, vp, vp]
+    L.pgpu_sim_get.argtypes = [vp, vp, vp, vp, vp]
+    L.pgpu_sim_set.argtypes = [vp, vp, vp, vp, vp]
+    L.pgpu_sim_stats.argtypes = [vp, C.POINTER(Stats)]
+    L.pgpu_enable_timing.argtypes = [vp, C.c_int]
+    L.pgpu_stage_times.argtypes = [vp, vp]
+    L.pgpu_stream.argtypes = [vp]
+    L.pgpu_stream.restype = vp
+    for name in EXPORTED:
+        getattr(L, name)  # raises AttributeError if a declared symbol is missing
+    _LIB = L
+    return L
+
+
+class PGPUError(RuntimeError):
+    pass
+
+
+def check(ctx, rc: int, what: str):
+    if rc != 0:
+        msg = ""
+        if ctx:
+            m = load().pgpu_last_error(ctx)
+            msg = m.decode() if m else ""
+        raise PGPUError(f"{what} failed ({rc}: {ERRORS.get(rc, '?')}) {msg}")

@@ -1,0 +1,227 @@
+"""Host-side mirror of the reference's knn:: / voronoi:: / hydro:: interface.
+
+Each method forwards to one C ABI entry point of libproteus_gpu.so; the
+reference function it stands for is named in its docstring.  Arrays are numpy
+(float64 / uint32 / int32 / uint64), C-contiguous, in host memory.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import check
+
+STATUS_SUCCESS = 4
+STATUS_NOT_COMPUTED = 6
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _c64(a, dtype=np.float64):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+@dataclass
+class Mesh:
+    """A mesh in the reference's VMesh layout (src/voronoi/voronoi.h:22-41):
+    cells in input order (hydro ids first, then ghosts), faces CSR per cell.
+    seeds and normal are 3-vectors even in 2D; status, cert_k and centroid are
+    per-cell extras."""
+    dim: int
+    n_seeds: int
+    n_hydro: int
+    seeds: np.ndarray
+    volumes: np.ndarray
+    face_counts: np.ndarray
+    face_ptr: np.ndarray
+    neighbor: np.ndarray
+    normal: np.ndarray
+    area: np.ndarray
+    ghost_ids: np.ndarray
+    status: np.ndarray
+    cert_k: np.ndarray
+    centroid: np.ndarray
+
+    @property
+    def num_faces(self) -> int:
+        return int(len(self.neighbor))
+
+
+class Context:
+    """One device context: a CUDA stream plus the device buffers of one mesh/simulation.
+
+    dim, k: the reference's compile-time dimension and _K_ (Config.sh:4-34),
+    here runtime parameters.  boundary: "periodic" (reference) or "reflective".
+    flux: "reference" (stored inward normal, own face area, as riemann.cpp) or
+    "physical" (outward normal, face-pair-symmetric area)."""
+
+    def __init__(self, dim: int = 3, k: int = 190, boundary: str = "periodic", flux: str = "reference",
+                 buff: float = 0.04, gamma: float = 5.0 / 3.0, device: int = 0):
+        L = _lib.load()
+        p = _lib.Params()
+        L.pgpu_default_params(C.byref(p))
+        p.dim, p.k, p.buff, p.gamma, p.device = dim, k, buff, gamma, device
+        p.boundary = {"periodic": 0, "reflective": 1}[boundary]
+        p.flux_mode = {"reference": 0, "physical": 1}[flux]
+        h = C.c_void_p()
+        rc = L.pgpu_create(C.byref(p), C.byref(h))
+        if rc != 0:
+            raise _lib.PGPUError(f"pgpu_create failed ({rc}: {_lib.ERRORS.get(rc, '?')})")
+        self._h = h
+        self.dim, self.k, self.boundary, self.flux, self.buff, self.gamma = dim, k, boundary, flux, buff, gamma
+        self._L = L
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.pgpu_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        return int(self._L.pgpu_stream(self._h) or 0)
+
+    # ---------------------------------------------------------------- knn::
+    def knn(self, pts: np.ndarray) -> np.ndarray:
+        """knn::init + knn::solve (src/knn/knn.cpp:16-234): (n, k) neighbour ids in input ids,
+        ascending by (squared distance, id); UINT32_MAX where fewer than k exist."""
+        pts = _c64(pts)
+        n = len(pts)
+        out = np.zeros((n, self.k), np.uint32)
+        check(self._h, self._L.pgpu_knn(self._h, _ptr(pts), n, _ptr(out)), "pgpu_knn")
+        return out
+
+    def knn_sorted(self):
+        """knn::get_points / get_permutation (src/knn/knn.cpp:445-455) of the last knn():
+        (sorted points, perm sorted->input id, grid resolution)."""
+        n = C.c_int64()
+        self._L.pgpu_mesh_sizes(self._h, C.byref(n), None, None)
+        pts = np.zeros((n.value, self.dim))
+        perm = np.zeros(n.value, np.uint32)
+        g = C.c_int()
+        check(self._h, self._L.pgpu_knn_sorted(self._h, _ptr(pts), _ptr(perm), C.byref(g)), "pgpu_knn_sorted")
+        return pts, perm, g.value
+
+    # ------------------------------------------------------------ voronoi::
+    def compute_periodic_mesh(self, pts: np.ndarray, download: bool = True) -> Mesh | None:
+        """voronoi::compute_periodic_mesh (src/voronoi/periodic_mesh.cpp:44-184)."""
+        pts = _c64(pts)
+        ns, nf = C.c_int64(), C.c_int64()
+        check(self._h, self._L.pgpu_periodic_mesh(self._h, _ptr(pts), len(pts), C.byref(ns), C.byref(nf)),
+              "pgpu_periodic_mesh")
+        return self.download_mesh() if download else None
+
+    def compute_mesh(self, pts_unit: np.ndarray, download: bool = True) -> Mesh | None:
+        """voronoi::compute_mesh (src/voronoi/voronoi.cpp:103-151) on points in the unit box."""
+        pts = _c64(pts_unit)
+        nf = C.c_int64()
+        check(self._h, self._L.pgpu_compute_mesh(self._h, _ptr(pts), len(pts), C.byref(nf)), "pgpu_compute_mesh")
+        return self.download_mesh() if download else None
+
+    def mesh_sizes(self):
+        ns, nh, nf = C.c_int64(), C.c_int64(), C.c_int64()
+        self._L.pgpu_mesh_sizes(self._h, C.byref(ns), C.byref(nh), C.byref(nf))
+        return ns.value, nh.value, nf.value
+
+    def download_mesh(self) -> Mesh:
+        """The device mesh in VMesh layout (unpermute_vmesh, src/voronoi/voronoi.cpp:298-419)."""
+        n, nh, F = self.mesh_sizes()
+        m = Mesh(self.dim, n, nh, np.zeros((n, 3)), np.zeros(n), np.zeros(n, np.uint64), np.zeros(n, np.uint64),
+                 np.zeros(F, np.int32), np.zeros((F, 3)), np.zeros(F), np.zeros(n - nh, np.uint64),
+                 np.zeros(n, np.int32), np.zeros(n, np.int32), np.zeros((n, 3)))
+        check(self._h, self._L.pgpu_download_mesh(
+            self._h, _ptr(m.seeds), _ptr(m.volumes), _ptr(m.face_counts), _ptr(m.face_ptr), _ptr(m.neighbor),
+            _ptr(m.normal), _ptr(m.area), _ptr(m.ghost_ids), _ptr(m.status), _ptr(m.cert_k), _ptr(m.centroid)),
+            "pgpu_download_mesh")
+        return m
+
+    def upload_mesh(self, m) -> None:
+        """Makes a host VMesh (any object with the Mesh fields) the device mesh."""
+        F = len(m.neighbor)
+        check(self._h, self._L.pgpu_upload_mesh(
+            self._h, m.n_seeds, m.n_hydro, F, _ptr(_c64(m.volumes)), _ptr(_c64(m.face_counts, np.uint64)),
+            _ptr(_c64(m.face_ptr, np.uint64)), _ptr(_c64(m.neighbor, np.int32)), _ptr(_c64(m.normal)),
+            _ptr(_c64(m.area)), _ptr(_c64(m.ghost_ids, np.uint64) if len(m.ghost_ids) else None)),
+            "pgpu_upload_mesh")
+
+    # -------------------------------------------------------------- hydro::
+    def set_prim(self, rho, v, E) -> None:
+        """hydro::init (src/hydro/finite_volume_solver.cpp:8-31)."""
+        rho, v, E = _c64(rho), _c64(v), _c64(E)
+        check(self._h, self._L.pgpu_set_prim(self._h, _ptr(rho), _ptr(v), _ptr(E), len(rho)), "pgpu_set_prim")
+
+    def get_prim(self):
+        _, nh, _ = self.mesh_sizes()
+        rho, v, E = np.zeros(nh), np.zeros((nh, self.dim)), np.zeros(nh)
+        check(self._h, self._L.pgpu_get_prim(self._h, _ptr(rho), _ptr(v), _ptr(E)), "pgpu_get_prim")
+        return rho, v, E
+
+    def dt_cfl(self, cfl: float) -> float:
+        """hydro::dt_CFL (src/hydro/finite_volume_solver.cpp:151-186)."""
+        dt = C.c_double()
+        check(self._h, self._L.pgpu_dt_cfl(self._h, cfl, C.byref(dt)), "pgpu_dt_cfl")
+        return dt.value
+
+    def hydro_step(self, dt: float) -> None:
+        """hydro::hydro_step (src/hydro/finite_volume_solver.cpp:43-123)."""
+        check(self._h, self._L.pgpu_hydro_step(self._h, dt), "pgpu_hydro_step")
+
+    # ------------------------------------------------------- moving mesh
+    def sim_init(self, pos, rho, v, E, deposit=None) -> None:
+        pos, rho, v, E = _c64(pos), _c64(rho), _c64(v), _c64(E)
+        dep = None if deposit is None else _c64(deposit)
+        check(self._h, self._L.pgpu_sim_init(self._h, _ptr(pos), _ptr(rho), _ptr(v), _ptr(E), _ptr(dep), len(pos)),
+              "pgpu_sim_init")
+
+    def sim_step(self, cfl: float = 0.3, fixed_dt: float = 0.0, want_dt: bool = True) -> float | None:
+        dt = C.c_double()
+        check(self._h, self._L.pgpu_sim_step(self._h, cfl, fixed_dt, C.byref(dt) if want_dt else None),
+              "pgpu_sim_step")
+        return dt.value if want_dt else None
+
+    def sim_step_host(self, cfl, fixed_dt, pos, mass, mom, energy) -> float:
+        """One step with the state in (pinned or pageable) host arrays, updated in place."""
+        dt = C.c_double()
+        check(self._h, self._L.pgpu_sim_step_host(self._h, cfl, fixed_dt, _ptr(pos), _ptr(mass), _ptr(mom),
+                                                  _ptr(energy), C.byref(dt)), "pgpu_sim_step_host")
+        return dt.value
+
+    def sim_get(self):
+        _, nh, _ = self.mesh_sizes()
+        pos, mass, mom, en = np.zeros((nh, self.dim)), np.zeros(nh), np.zeros((nh, self.dim)), np.zeros(nh)
+        check(self._h, self._L.pgpu_sim_get(self._h, _ptr(pos), _ptr(mass), _ptr(mom), _ptr(en)), "pgpu_sim_get")
+        return pos, mass, mom, en
+
+    def sim_set(self, pos=None, mass=None, mom=None, energy=None) -> None:
+        arrs = [None if a is None else _c64(a) for a in (pos, mass, mom, energy)]
+        check(self._h, self._L.pgpu_sim_set(self._h, *[_ptr(a) for a in arrs]), "pgpu_sim_set")
+
+    def stats(self) -> dict:
+        s = _lib.Stats()
+        check(self._h, self._L.pgpu_sim_stats(self._h, C.byref(s)), "pgpu_sim_stats")
+        return {f: (list(getattr(s, f)) if f == "total_mom" else getattr(s, f)) for f, _ in s._fields_}
+
+    def enable_timing(self, on: bool = True) -> None:
+        check(self._h, self._L.pgpu_enable_timing(self._h, int(on)), "pgpu_enable_timing")
+
+    def stage_times(self):
+        """Device ms of the last mesh/step: ghosts, sort, knn, clip, hydro."""
+        a = (C.c_float * 5)()
+        check(self._h, self._L.pgpu_stage_times(self._h, a), "pgpu_stage_times")
+        return list(a)

@@ -1,0 +1,561 @@
+// The C ABI (include/proteus_gpu.h): argument checks, device memory, the order
+// of the stage launches, and host transfers.  No computation happens here.
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "pgpu_common.cuh"
+#include "pgpu_ctx.h"
+
+using pgpu::DevBuf;
+using pgpu::DevScalars;
+using pgpu::ensure;
+
+namespace pgpu {
+
+cudaError_t ensure_bytes(DevBuf& b, size_t bytes) {
+    if (b.p && b.bytes >= bytes) return cudaSuccess;
+    if (b.p) {
+        cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+    }
+    size_t want = bytes + bytes / 8 + 256;  // headroom so that small growth does not reallocate
+    cudaError_t e = cudaMalloc(&b.p, want);
+    if (e != cudaSuccess) {
+        b.p = nullptr;
+        return e;
+    }
+    b.bytes = want;
+    return cudaSuccess;
+}
+
+}  // namespace pgpu
+
+namespace {
+
+int fail(pgpu_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int fail_cuda(pgpu_ctx* c, cudaError_t e, const char* what) {
+    std::string m = std::string("CUDA error in ") + what + ": " + cudaGetErrorString(e);
+    return fail(c, PGPU_ECUDA, m);
+}
+
+#define CK(x)                                               \
+    do {                                                    \
+        cudaError_t _e = (x);                               \
+        if (_e != cudaSuccess) return fail_cuda(c, _e, #x); \
+    } while (0)
+
+void free_buf(DevBuf& b) {
+    if (b.p) cudaFree(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+}
+
+int check_ctx(pgpu_ctx* c) {
+    if (!c) return PGPU_EINVAL;
+    cudaError_t e = cudaSetDevice(c->prm.device);
+    if (e != cudaSuccess) return fail_cuda(c, e, "cudaSetDevice");
+    return PGPU_OK;
+}
+
+void mark(pgpu_ctx* c, int i) {
+    if (c->timing) cudaEventRecord(c->ev[i], c->stream);
+}
+
+DevScalars* scalars(pgpu_ctx* c) { return (DevScalars*)c->scalars.p; }
+
+int upload_points(pgpu_ctx* c, const double* pts, int64_t n) {
+    const int D = c->prm.dim;
+    cudaError_t e = cudaSuccess;
+    double* d = ensure<double>(c->pos, (size_t)n * D + 1, &e);
+    CK(e);
+    if (n > 0) CK(cudaMemcpyAsync(d, pts, (size_t)n * D * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    return PGPU_OK;
+}
+
+// ghosts (or plain copy), grid sort, query list, KNN, clip + extraction
+int build_mesh(pgpu_ctx* c, int64_t n, bool no_ghosts, bool all_cells) {
+    if (n < 0 || n >= (1ll << 27)) return fail(c, PGPU_ECAPACITY, "point count outside [0, 2^27)");
+    mark(c, 0);
+    CK(pgpu::launch_ghosts(c, (const double*)c->pos.p, n, no_ghosts));
+    if (c->n_ext >= (1ll << 31)) return fail(c, PGPU_ECAPACITY, "too many ghost points");
+    mark(c, 1);
+    CK(pgpu::launch_grid_sort(c));
+    CK(pgpu::launch_query_list(c, all_cells));
+    mark(c, 2);
+    CK(pgpu::launch_knn(c));
+    mark(c, 3);
+    CK(pgpu::launch_clip(c));
+    mark(c, 4);
+    c->have_mesh = true;
+    c->mesh_uploaded = false;
+    return PGPU_OK;
+}
+
+void collect_times(pgpu_ctx* c) {
+    if (!c->timing) return;
+    cudaEventSynchronize(c->ev[5]);
+    for (int i = 0; i < 5; i++) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
+}
+
+}  // namespace
+
+extern "C" {
+
+void pgpu_default_params(pgpu_params* p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->dim = 3;
+    p->k = 190;
+    p->boundary = PGPU_PERIODIC;
+    p->flux_mode = PGPU_FLUX_REFERENCE;
+    p->buff = 0.04;
+    p->gamma = 5.0 / 3.0;
+    p->device = 0;
+}
+
+int pgpu_abi_version(void) { return PGPU_ABI_VERSION; }
+
+int pgpu_create(const pgpu_params* p, pgpu_ctx** out) {
+    if (!p || !out) return PGPU_EINVAL;
+    *out = nullptr;
+    if (p->dim != 2 && p->dim != 3) return PGPU_EINVAL;
+    if (p->k < 1 || p->k > pgpu::MAX_K) return PGPU_EINVAL;
+    if (!(p->buff >= 0.0 && p->buff < 0.5)) return PGPU_EINVAL;
+    if (!(p->gamma > 1.0)) return PGPU_EINVAL;
+    if (p->boundary != PGPU_PERIODIC && p->boundary != PGPU_REFLECTIVE) return PGPU_EINVAL;
+    if (p->flux_mode != PGPU_FLUX_REFERENCE && p->flux_mode != PGPU_FLUX_PHYSICAL) return PGPU_EINVAL;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return PGPU_ECUDA;
+    if (p->device < 0 || p->device >= ndev) return PGPU_EINVAL;
+    pgpu_ctx* c = new pgpu_ctx();
+    c->prm = *p;
+    if (cudaSetDevice(p->device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return PGPU_ECUDA;
+    }
+    cudaError_t e = pgpu::ensure_bytes(c->scalars, sizeof(DevScalars));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->scalars.p, 0, sizeof(DevScalars), c->stream);
+    for (int i = 0; i < 6 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
+    if (e != cudaSuccess) {
+        pgpu_destroy(c);
+        return PGPU_ECUDA;
+    }
+    *out = c;
+    return PGPU_OK;
+}
+
+void pgpu_destroy(pgpu_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->prm.device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    DevBuf* bufs[] = {&c->pos,   &c->ext,     &c->gcnt,     &c->goff,   &c->ghost_src, &c->ghost_code, &c->bin_cnt,
+                      &c->bin_start, &c->bin_key, &c->spts, &c->perm,  &c->inv,       &c->qflag,      &c->qoff,
+                      &c->qs,    &c->knn,     &c->vol,      &c->fptr,   &c->fcnt,      &c->status,     &c->certk,
+                      &c->centroid, &c->f_nb, &c->f_own,    &c->f_geo,  &c->scan_tmp,  &c->scalars,    &c->rho,
+                      &c->vel,   &c->energy,  &c->rho2,     &c->vel2,   &c->energy2,   &c->mass,       &c->mom,
+                      &c->en,    &c->w4,      &c->we,       &c->red_tmp, &c->dl_ptr,   &c->dl_a,       &c->dl_b,
+                      &c->dl_c};
+    for (DevBuf* b : bufs) free_buf(*b);
+    for (int i = 0; i < 6; i++)
+        if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* pgpu_last_error(const pgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+void* pgpu_stream(pgpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int pgpu_enable_timing(pgpu_ctx* c, int on) {
+    if (!c) return PGPU_EINVAL;
+    c->timing = on != 0;
+    return PGPU_OK;
+}
+
+int pgpu_stage_times(pgpu_ctx* c, float* ms5) {
+    if (!c || !ms5) return PGPU_EINVAL;
+    collect_times(c);
+    for (int i = 0; i < 5; i++) ms5[i] = c->stage_ms[i];
+    return PGPU_OK;
+}
+
+// ------------------------------------------------------------------ KNN
+int pgpu_knn(pgpu_ctx* c, const double* pts, int64_t n, uint32_t* out) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if ((!pts && n > 0) || n < 0) return fail(c, PGPU_EINVAL, "pgpu_knn: bad points");
+    if ((r = upload_points(c, pts, n))) return r;
+    mark(c, 0);
+    CK(pgpu::launch_ghosts(c, (const double*)c->pos.p, n, true));
+    mark(c, 1);
+    CK(pgpu::launch_grid_sort(c));
+    CK(pgpu::launch_query_list(c, true));
+    mark(c, 2);
+    CK(pgpu::launch_knn(c));
+    mark(c, 3);
+    mark(c, 4);
+    c->have_mesh = false;
+    c->have_sim = false;
+    if (out && n > 0) {
+        cudaError_t e = cudaSuccess;
+        uint32_t* rows = ensure<uint32_t>(c->dl_a, (size_t)n * c->prm.k + 1, &e);
+        CK(e);
+        CK(pgpu::launch_knn_rows(c, rows));
+        CK(cudaMemcpyAsync(out, rows, (size_t)n * c->prm.k * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    }
+    mark(c, 5);
+    CK(cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+int pgpu_knn_sorted(pgpu_ctx* c, double* sorted_pts, uint32_t* perm, int* n_grid) {
+    int r = check_ctx(c);
+    if (r) return r;
+    const int64_t n = c->n_ext;
+    cudaError_t e = cudaSuccess;
+    if (sorted_pts && n > 0) {
+        double* tmp = ensure<double>(c->dl_b, (size_t)n * c->prm.dim + 1, &e);
+        CK(e);
+        CK(pgpu::launch_unpack_points(c, c->spts.p, n, tmp));
+        CK(cudaMemcpyAsync(sorted_pts, tmp, (size_t)n * c->prm.dim * sizeof(double), cudaMemcpyDeviceToHost,
+                           c->stream));
+    }
+    if (perm && n > 0) CK(cudaMemcpyAsync(perm, c->perm.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (n_grid) *n_grid = c->grid_G;
+    CK(cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+// ------------------------------------------------------------------ mesh
+int pgpu_periodic_mesh(pgpu_ctx* c, const double* pts, int64_t n, int64_t* n_seeds, int64_t* num_faces) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if ((!pts && n > 0) || n < 0) return fail(c, PGPU_EINVAL, "pgpu_periodic_mesh: bad points");
+    if ((r = upload_points(c, pts, n))) return r;
+    if ((r = build_mesh(c, n, false, true))) return r;
+    mark(c, 5);
+    c->have_sim = false;
+    if (n_seeds) *n_seeds = c->n_ext;
+    if (num_faces) *num_faces = c->num_faces;
+    return PGPU_OK;
+}
+
+int pgpu_compute_mesh(pgpu_ctx* c, const double* pts, int64_t n, int64_t* num_faces) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if ((!pts && n > 0) || n < 0) return fail(c, PGPU_EINVAL, "pgpu_compute_mesh: bad points");
+    if ((r = upload_points(c, pts, n))) return r;
+    if ((r = build_mesh(c, n, true, true))) return r;
+    mark(c, 5);
+    c->have_sim = false;
+    if (num_faces) *num_faces = c->num_faces;
+    return PGPU_OK;
+}
+
+int pgpu_mesh_sizes(pgpu_ctx* c, int64_t* n_seeds, int64_t* n_hydro, int64_t* num_faces) {
+    if (!c) return PGPU_EINVAL;
+    if (n_seeds) *n_seeds = c->n_ext;
+    if (n_hydro) *n_hydro = c->n_hydro;
+    if (num_faces) *num_faces = c->num_faces;
+    return c->have_mesh ? PGPU_OK : PGPU_ESTATE;
+}
+
+int pgpu_download_mesh(pgpu_ctx* c, double* seeds, double* volumes, uint64_t* face_counts, uint64_t* face_ptr,
+                       int32_t* neighbor, double* normal, double* area, uint64_t* ghost_ids, int32_t* status,
+                       int32_t* cert_k, double* centroid) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_mesh) return fail(c, PGPU_ESTATE, "pgpu_download_mesh: no mesh");
+    const int64_t n = c->n_ext, F = c->num_faces, ng = c->n_ext - c->n_hydro;
+    cudaError_t e = cudaSuccess;
+    uint32_t* nptr = ensure<uint32_t>(c->dl_ptr, n + 1, &e);
+    int32_t* nb = ensure<int32_t>(c->dl_a, F + 1, &e);
+    double* nrm = ensure<double>(c->dl_b, 3 * F + 3, &e);
+    double* ar = ensure<double>(c->dl_c, F + 1, &e);
+    CK(e);
+    CK(pgpu::launch_mesh_compact(c, nptr, nb, nrm, ar));
+    std::vector<uint32_t> hptr(n + 1), hcnt(n + 1);
+    CK(cudaMemcpyAsync(hptr.data(), nptr, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(hcnt.data(), c->fcnt.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (neighbor && F) CK(cudaMemcpyAsync(neighbor, nb, F * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (normal && F) CK(cudaMemcpyAsync(normal, nrm, 3 * F * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (area && F) CK(cudaMemcpyAsync(area, ar, F * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (volumes && n) CK(cudaMemcpyAsync(volumes, c->vol.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (cert_k && n) CK(cudaMemcpyAsync(cert_k, c->certk.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (status && n) CK(cudaMemcpyAsync(status, c->status.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (centroid && n)
+        CK(cudaMemcpyAsync(centroid, c->centroid.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    std::vector<uint32_t> gsrc(ng > 0 ? ng : 1);
+    if (ghost_ids && ng > 0)
+        CK(cudaMemcpyAsync(gsrc.data(), c->ghost_src.p, ng * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (seeds && n && !c->mesh_uploaded) {
+        DevBuf tmp;
+        CK(pgpu::ensure_bytes(tmp, 3 * n * sizeof(double) + 16));
+        CK(pgpu::launch_seeds(c, (double*)tmp.p, c->unit_scale == 1.0));
+        CK(cudaMemcpyAsync(seeds, tmp.p, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        free_buf(tmp);
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    for (int64_t i = 0; i < n; i++) {
+        if (face_counts) face_counts[i] = hcnt[i];
+        if (face_ptr) face_ptr[i] = hptr[i];
+    }
+    if (ghost_ids)
+        for (int64_t g = 0; g < ng; g++) ghost_ids[g] = gsrc[g];
+    if (status && !c->all_cells)
+        for (int64_t i = c->n_hydro; i < n; i++) status[i] = PGPU_NOT_COMPUTED;
+    return PGPU_OK;
+}
+
+int pgpu_upload_mesh(pgpu_ctx* c, int64_t n_seeds, int64_t n_hydro, int64_t num_faces, const double* volumes,
+                     const uint64_t* face_counts, const uint64_t* face_ptr, const int32_t* neighbor,
+                     const double* normal, const double* area, const uint64_t* ghost_ids) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (n_seeds < 0 || n_hydro < 0 || n_hydro > n_seeds || num_faces < 0 || num_faces >= (1ll << 32) ||
+        n_hydro >= (1ll << 27) || !volumes || !face_counts || !face_ptr ||
+        (num_faces > 0 && (!neighbor || !normal || !area)) || (n_seeds > n_hydro && !ghost_ids))
+        return fail(c, PGPU_EINVAL, "pgpu_upload_mesh: bad arguments");
+    std::vector<uint32_t> fp(n_seeds + 1), fc(n_seeds + 1), own(num_faces + 1), gs(n_seeds - n_hydro + 1);
+    std::vector<double4> geo(num_faces + 1);
+    for (int64_t i = 0; i < n_seeds; i++) {
+        if (face_ptr[i] + face_counts[i] > (uint64_t)num_faces)
+            return fail(c, PGPU_EINVAL, "pgpu_upload_mesh: face range out of bounds");
+        fp[i] = (uint32_t)face_ptr[i];
+        fc[i] = (uint32_t)face_counts[i];
+    }
+    for (int64_t g = 0; g < n_seeds - n_hydro; g++) {
+        if (ghost_ids[g] >= (uint64_t)n_hydro) return fail(c, PGPU_EINVAL, "pgpu_upload_mesh: bad ghost id");
+        gs[g] = (uint32_t)ghost_ids[g];
+    }
+    for (int64_t f = 0; f < num_faces; f++) {
+        const int32_t nb = neighbor[f];
+        if (nb >= n_seeds) return fail(c, PGPU_EINVAL, "pgpu_upload_mesh: neighbour out of range");
+        own[f] = nb < 0 ? pgpu::BOX_FACE : (nb < n_hydro ? (uint32_t)nb : gs[nb - n_hydro]);
+        geo[f] = make_double4(normal[3 * f], normal[3 * f + 1], normal[3 * f + 2], area[f]);
+    }
+    cudaError_t e = cudaSuccess;
+    ensure<double>(c->vol, n_seeds + 1, &e);
+    ensure<uint32_t>(c->fptr, n_seeds + 1, &e);
+    ensure<uint32_t>(c->fcnt, n_seeds + 1, &e);
+    ensure<int32_t>(c->f_nb, num_faces + 1, &e);
+    ensure<uint32_t>(c->f_own, num_faces + 1, &e);
+    ensure<double4>(c->f_geo, num_faces + 1, &e);
+    ensure<uint32_t>(c->ghost_src, n_seeds - n_hydro + 1, &e);
+    ensure<int>(c->status, n_seeds + 1, &e);
+    ensure<int>(c->certk, n_seeds + 1, &e);
+    ensure<double>(c->centroid, 3 * n_seeds + 3, &e);
+    CK(e);
+    CK(cudaMemcpyAsync(c->vol.p, volumes, n_seeds * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->fptr.p, fp.data(), n_seeds * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->fcnt.p, fc.data(), n_seeds * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+    if (num_faces) {
+        CK(cudaMemcpyAsync(c->f_nb.p, neighbor, num_faces * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->f_own.p, own.data(), num_faces * sizeof(uint32_t), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->f_geo.p, geo.data(), num_faces * sizeof(double4), cudaMemcpyHostToDevice, c->stream));
+    }
+    if (n_seeds > n_hydro)
+        CK(cudaMemcpyAsync(c->ghost_src.p, gs.data(), (n_seeds - n_hydro) * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                           c->stream));
+    CK(cudaMemsetAsync(c->status.p, 0, n_seeds * sizeof(int), c->stream));
+    CK(cudaMemsetAsync(c->certk.p, 0, n_seeds * sizeof(int), c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->n_ext = n_seeds;
+    c->n_hydro = n_hydro;
+    c->num_faces = num_faces;
+    c->have_mesh = true;
+    c->mesh_uploaded = true;
+    c->all_cells = true;
+    c->have_sim = false;
+    return PGPU_OK;
+}
+
+// ------------------------------------------------------------------ hydro (reference semantics)
+int pgpu_set_prim(pgpu_ctx* c, const double* rho, const double* v, const double* E, int64_t n) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (n < 0 || (n > 0 && (!rho || !v || !E))) return fail(c, PGPU_EINVAL, "pgpu_set_prim: bad arguments");
+    const int D = c->prm.dim;
+    cudaError_t e = cudaSuccess;
+    ensure<double>(c->rho, n + 1, &e);
+    ensure<double>(c->vel, n * D + 1, &e);
+    ensure<double>(c->energy, n + 1, &e);
+    CK(e);
+    if (n) {
+        CK(cudaMemcpyAsync(c->rho.p, rho, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->vel.p, v, n * D * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(c->energy.p, E, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_prim = true;
+    if (!c->have_mesh) c->n_hydro = n;
+    else if (n != c->n_hydro) return fail(c, PGPU_EINVAL, "pgpu_set_prim: n differs from the mesh's n_hydro");
+    return PGPU_OK;
+}
+
+int pgpu_get_prim(pgpu_ctx* c, double* rho, double* v, double* E) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_prim) return fail(c, PGPU_ESTATE, "pgpu_get_prim: no primitives");
+    const int64_t n = c->n_hydro;
+    const int D = c->prm.dim;
+    if (n && rho) CK(cudaMemcpyAsync(rho, c->rho.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (n && v) CK(cudaMemcpyAsync(v, c->vel.p, n * D * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (n && E) CK(cudaMemcpyAsync(E, c->energy.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+int pgpu_dt_cfl(pgpu_ctx* c, double cfl, double* dt) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_mesh || !c->have_prim) return fail(c, PGPU_ESTATE, "pgpu_dt_cfl: needs a mesh and primitives");
+    if (!dt) return PGPU_EINVAL;
+    CK(pgpu::launch_dt_ref(c, cfl));
+    unsigned long long bits = 0;
+    CK(cudaMemcpyAsync(&bits, &scalars(c)->dt_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memcpy(dt, &bits, sizeof(double));
+    return PGPU_OK;
+}
+
+int pgpu_hydro_step(pgpu_ctx* c, double dt) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_mesh || !c->have_prim) return fail(c, PGPU_ESTATE, "pgpu_hydro_step: needs a mesh and primitives");
+    CK(cudaMemsetAsync(&scalars(c)->box_faces, 0, sizeof(unsigned int), c->stream));
+    CK(pgpu::launch_hydro_ref(c, dt));
+    unsigned int nbox = 0;
+    CK(cudaMemcpyAsync(&nbox, &scalars(c)->box_faces, sizeof(nbox), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (nbox) return fail(c, PGPU_EMESH, "pgpu_hydro_step: a hydro cell has a bounding-box face (ghost layer too thin)");
+    return PGPU_OK;
+}
+
+// ------------------------------------------------------------------ moving mesh
+int pgpu_sim_init(pgpu_ctx* c, const double* pos, const double* rho, const double* v, const double* E,
+                  const double* deposit, int64_t n) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (n <= 0 || !pos || !rho || !v || !E) return fail(c, PGPU_EINVAL, "pgpu_sim_init: bad arguments");
+    if ((r = upload_points(c, pos, n))) return r;
+    c->have_mesh = false;
+    if ((r = build_mesh(c, n, false, false))) return r;
+    c->have_mesh = true;
+    if ((r = pgpu_set_prim(c, rho, v, E, n))) return r;
+    const double* dep = nullptr;
+    cudaError_t e = cudaSuccess;
+    if (deposit) {
+        double* d = ensure<double>(c->dl_c, n + 1, &e);
+        CK(e);
+        CK(cudaMemcpyAsync(d, deposit, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        dep = d;
+    }
+    CK(pgpu::launch_cons_from_prim(c, dep));
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_sim = true;
+    return PGPU_OK;
+}
+
+int pgpu_sim_step(pgpu_ctx* c, double cfl, double fixed_dt, double* dt_out) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_sim) return fail(c, PGPU_ESTATE, "pgpu_sim_step: call pgpu_sim_init first");
+    if ((r = build_mesh(c, c->n_hydro, false, false))) return r;
+    CK(pgpu::launch_prim_dt(c, cfl, fixed_dt));
+    CK(pgpu::launch_flux_update(c, fixed_dt));
+    mark(c, 5);
+    if (dt_out) {
+        unsigned long long bits = 0;
+        CK(cudaMemcpyAsync(&bits, &scalars(c)->dt_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (fixed_dt > 0)
+            *dt_out = fixed_dt;
+        else
+            std::memcpy(dt_out, &bits, sizeof(double));
+    }
+    return PGPU_OK;
+}
+
+int pgpu_sim_set(pgpu_ctx* c, const double* pos, const double* mass, const double* mom, const double* energy) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_sim) return fail(c, PGPU_ESTATE, "pgpu_sim_set: no simulation");
+    const int64_t n = c->n_hydro;
+    const int D = c->prm.dim;
+    if (pos) CK(cudaMemcpyAsync(c->pos.p, pos, n * D * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (mass) CK(cudaMemcpyAsync(c->mass.p, mass, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (mom) CK(cudaMemcpyAsync(c->mom.p, mom, n * D * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (energy) CK(cudaMemcpyAsync(c->en.p, energy, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    return PGPU_OK;
+}
+
+int pgpu_sim_get(pgpu_ctx* c, double* pos, double* mass, double* mom, double* energy) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_sim) return fail(c, PGPU_ESTATE, "pgpu_sim_get: no simulation");
+    const int64_t n = c->n_hydro;
+    const int D = c->prm.dim;
+    if (pos) CK(cudaMemcpyAsync(pos, c->pos.p, n * D * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (mass) CK(cudaMemcpyAsync(mass, c->mass.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (mom) CK(cudaMemcpyAsync(mom, c->mom.p, n * D * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (energy) CK(cudaMemcpyAsync(energy, c->en.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+int pgpu_sim_step_host(pgpu_ctx* c, double cfl, double fixed_dt, double* pos, double* mass, double* mom,
+                       double* energy, double* dt_out) {
+    int r = pgpu_sim_set(c, pos, mass, mom, energy);
+    if (r) return r;
+    if ((r = pgpu_sim_step(c, cfl, fixed_dt, nullptr))) return r;
+    if ((r = pgpu_sim_get(c, pos, mass, mom, energy))) return r;
+    if (dt_out) {
+        unsigned long long bits = 0;
+        CK(cudaMemcpyAsync(&bits, &scalars(c)->dt_bits, sizeof(bits), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        if (fixed_dt > 0)
+            *dt_out = fixed_dt;
+        else
+            std::memcpy(dt_out, &bits, sizeof(double));
+    }
+    return PGPU_OK;
+}
+
+int pgpu_sim_stats(pgpu_ctx* c, pgpu_stats* out) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!out) return PGPU_EINVAL;
+    std::memset(out, 0, sizeof(*out));
+    if (c->have_sim) CK(pgpu::launch_sums(c));
+    DevScalars h;
+    CK(cudaMemcpyAsync(&h, c->scalars.p, sizeof(h), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    out->n_hydro = c->n_hydro;
+    out->n_ext = c->n_ext;
+    out->num_faces = c->num_faces;
+    out->failed_cells = h.failed;
+    out->box_faces = h.box_faces;
+    out->unpaired_faces = h.unpaired;
+    out->knn_candidates = (int64_t)h.knn_cand;
+    std::memcpy(&out->last_dt, &h.dt_bits, sizeof(double));
+    out->total_mass = h.sums[0];
+    out->total_mom[0] = h.sums[1];
+    out->total_mom[1] = h.sums[2];
+    out->total_mom[2] = h.sums[3];
+    out->total_energy = h.sums[4];
+    out->cert_k_max = h.cert_k_max;
+    out->n_grid = c->grid_G;
+    return PGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,756 @@
+// Voronoi cells by half-space clipping with the security-radius certificate,
+// fused with the extraction of faces, areas, volumes and centroids
+// (replaces cpu_compute_cell + ConvexCell + extract_cell_to_vmesh,
+// src/voronoi/voronoi.cpp:201-241, src/voronoi/cell.cpp:42-669; the method is
+// Ray, Sokolov, Lefebvre, Levy, "Meshless Voronoi on the GPU", ACM TOG 2018).
+//
+// One warp per cell.  The cell lives in shared memory in dual form: planes
+// (a, b, c, d) and vertices as plane triples (pairs in 2D), consistently
+// oriented.  Per clipping plane:
+//   1. every lane tests its vertices against the plane with the reference's
+//      determinant predicate and error bound (cell.cpp:175-221);
+//   2. the cavity boundary is the set of directed edges of removed vertices
+//      whose reverse edge belongs to no removed vertex (3D: a 64x64 edge bit
+//      matrix in shared memory; 2D: the two lines used once), checked to be a
+//      single cycle; one new vertex (plane, x, y) per boundary edge x -> y,
+//      which is the vertex the reference's boundary walk (cell.cpp:224-364)
+//      creates for that edge;
+//   3. kept vertices are compacted in order and new ones appended, each with
+//      its squared distance to the seed cached for the certificate
+//      (cell.cpp:369-384), whose maximum is a warp reduction.
+// Predicates, vertex coordinates and plane equations use the reference's
+// expansions without FMA, so every decision, and the mesh topology, equal the
+// reference's.  Vertex order inside a cell differs, which changes face-area
+// and volume rounding only (3D); 2D edge lengths are bit-identical.
+//
+// Extraction: faces are the planes with >= D vertices, in plane order (box
+// planes first, then neighbours in clipping order).  Each lane builds one
+// face polygon by following the triangle orientation around its plane, and
+// sums the fan area and the divergence-theorem volume as cell.cpp:582-631
+// does.  A cell's faces are written contiguously at a slot reserved with one
+// atomic add; placement varies run to run, contents do not.
+#include <math_constants.h>
+
+#include "pgpu_common.cuh"
+#include "pgpu_ctx.h"
+
+namespace pgpu {
+namespace {
+
+constexpr int CLIP_WARPS = 4;
+constexpr unsigned FULL = 0xffffffffu;
+constexpr int FACE_MAX_V = 32;  // vertices per face polygon handled by one lane
+
+struct WarpCell {
+    double4 hp[MAX_P];
+    int vid[MAX_P];
+    uint32_t tri[MAX_T];
+    double vd2[MAX_T];
+    double fvol[MAX_P];      // per-face volume contribution (3D) for an ordered sum
+    double fcen[MAX_P][3];   // per-face centroid moment (3D)
+    union {
+        struct {
+            unsigned long long emask[MAX_P];
+            unsigned char nxt[MAX_P];
+        } b;
+        double vpos[MAX_T][3];
+    } u;
+};
+
+__device__ __forceinline__ uint32_t tri_a(uint32_t t) { return t & 255u; }
+__device__ __forceinline__ uint32_t tri_b(uint32_t t) { return (t >> 8) & 255u; }
+__device__ __forceinline__ uint32_t tri_c(uint32_t t) { return (t >> 16) & 255u; }
+__device__ __forceinline__ uint32_t pack3(uint32_t a, uint32_t b, uint32_t c) { return a | (b << 8) | (c << 16); }
+
+// compute_vertex_point with the perspective divide (cell.cpp:388-411)
+template <int D>
+__device__ __forceinline__ void vertex_pos(const double4* hp, uint32_t t, double& x, double& y, double& z) {
+    const double4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)];
+    if (D == 2) {
+        double rx = -det2(p1.w, p1.y, p2.w, p2.y);
+        double ry = -det2(p1.x, p1.w, p2.x, p2.w);
+        double rw = det2(p1.x, p1.y, p2.x, p2.y);
+        x = rx / rw;
+        y = ry / rw;
+        z = 0.0;
+    } else {
+        const double4 p3 = hp[tri_c(t)];
+        double rx = -det3(p1.w, p1.y, p1.z, p2.w, p2.y, p2.z, p3.w, p3.y, p3.z);
+        double ry = -det3(p1.x, p1.w, p1.z, p2.x, p2.w, p2.z, p3.x, p3.w, p3.z);
+        double rz = -det3(p1.x, p1.y, p1.w, p2.x, p2.y, p2.w, p3.x, p3.y, p3.w);
+        double rw = det3(p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z);
+        x = rx / rw;
+        y = ry / rw;
+        z = rz / rw;
+    }
+}
+
+// squared distance to the seed as is_security_radius_reached computes it
+__device__ __forceinline__ double seed_d2(double x, double y, double z, double sx, double sy, double sz) {
+    double dx = x - sx, dy = y - sy, dz = z - sz;
+    return dx * dx + dy * dy + dz * dz;
+}
+
+__device__ __forceinline__ double fmax3(double a, double b, double c) {
+    double m = a > b ? a : b;
+    return m > c ? m : c;
+}
+
+// vert_is_in_conflict (cell.cpp:175-221): returns det > 0, sets *near when |det| < eps
+template <int D>
+__device__ __forceinline__ bool in_conflict(const double4* hp, uint32_t t, const double4& e, bool* near) {
+    const double4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)];
+    double det, eps;
+    if (D == 2) {
+        det = det3(p1.x, p2.x, e.x, p1.y, p2.y, e.y, p1.w, p2.w, e.w);
+        double maxx = fmax3(fabs(p1.x), fabs(p2.x), fabs(e.x));
+        double maxy = fmax3(fabs(p1.y), fabs(p2.y), fabs(e.y));
+        double maxw = fmax3(fabs(p1.w), fabs(p2.w), fabs(e.w));
+        double max_max = fmax3(maxx, maxy, maxw);
+        eps = 1e-14 * maxx * maxy * maxw;
+        eps *= max_max;
+    } else {
+        const double4 p3 = hp[tri_c(t)];
+        det = det4(p1.x, p2.x, p3.x, e.x, p1.y, p2.y, p3.y, e.y, p1.z, p2.z, p3.z, e.z, p1.w, p2.w, p3.w, e.w);
+        double maxx = fmax3(fmax3(fabs(p1.x), fabs(p2.x), fabs(p3.x)), fabs(e.x), 0.0);
+        double maxy = fmax3(fmax3(fabs(p1.y), fabs(p2.y), fabs(p3.y)), fabs(e.y), 0.0);
+        double maxz = fmax3(fmax3(fabs(p1.z), fabs(p2.z), fabs(p3.z)), fabs(e.z), 0.0);
+        eps = 1e-14 * maxx * maxy * maxz;
+        double max_max = fmax3(maxx, maxy, maxz);
+        eps *= (max_max * max_max);
+    }
+    if (fabs(det) < eps) *near = true;
+    return det > 0.0;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+
+// std::max semantics of the reference's running maximum are irrelevant here:
+// squared distances are finite and non-negative.
+__device__ __forceinline__ double max_vd2(const WarpCell& W, int n, int lane, const uint32_t* keep_mask) {
+    double m = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        int i = lane + 32 * j;
+        if (i < n && (keep_mask == nullptr || ((keep_mask[j] >> lane) & 1u))) m = fmax(m, W.vd2[i]);
+    }
+    return warp_max(m);
+}
+
+struct ClipParams {
+    const uint32_t* qs;
+    const uint32_t* perm;
+    const void* spts;
+    const void* ext;
+    const uint32_t* knn;
+    const uint32_t* ghost_src;
+    const uint32_t* ghost_code;
+    int64_t nq;
+    int64_t n_hydro;
+    int K;
+    double vscale, ascale, scale;  // unit box -> physical
+    double* vol;
+    uint32_t* fptr;
+    uint32_t* fcnt;
+    int* status;
+    int* certk;
+    double* centroid;  // 3 per cell
+    int32_t* f_nb;
+    uint32_t* f_own;
+    double4* f_geo;
+    unsigned long long* face_counter;
+    unsigned int* overflow;
+    unsigned long long face_cap;
+};
+
+template <int D>
+__global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
+    using PT = typename PointOf<D>::type;
+    __shared__ WarpCell cells[CLIP_WARPS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t t = (int64_t)blockIdx.x * CLIP_WARPS + w;
+    if (t >= P.nq) return;  // warp-uniform
+    WarpCell& W = cells[w];
+    const PT* spts = (const PT*)P.spts;
+    const PT* ext = (const PT*)P.ext;
+    const uint32_t s = P.qs[t];
+    const uint32_t e = P.perm[s];
+    const PT sp = spts[s];
+    const double sx = sp.x, sy = sp.y, sz = pz(sp);
+    const int K = P.K;
+    const uint32_t* kl = P.knn + (size_t)t * K;
+
+    // ---- ConvexCell::ConvexCell (cell.cpp:42-104): bounding box [-1e-14, 1 + 1e-14]^D
+    const double beps = 1e-14;
+    const double xmin = -beps, xmax = 1.0 + beps;
+    if (lane < 2 * D) {
+        double4 pl;
+        switch (lane) {
+            case 0: pl = make_double4(1.0, 0.0, 0.0, -xmin); break;
+            case 1: pl = make_double4(-1.0, 0.0, 0.0, xmax); break;
+            case 2: pl = make_double4(0.0, 1.0, 0.0, -xmin); break;
+            case 3: pl = make_double4(0.0, -1.0, 0.0, xmax); break;
+            case 4: pl = make_double4(0.0, 0.0, 1.0, -xmin); break;
+            default: pl = make_double4(0.0, 0.0, -1.0, xmax); break;
+        }
+        W.hp[lane] = pl;
+        W.vid[lane] = -1;
+    }
+    if (D == 3) {
+        W.u.b.emask[lane] = 0ull;
+        W.u.b.emask[lane + 32] = 0ull;
+    }
+    const int ntri0 = D == 2 ? 4 : 8;
+    if (lane < ntri0) {
+        uint32_t tv;
+        if (D == 2) {
+            const uint32_t t2[4] = {pack3(2, 0, 0), pack3(1, 2, 0), pack3(3, 1, 0), pack3(0, 3, 0)};
+            tv = t2[lane & 3];
+        } else {
+            const uint32_t t3[8] = {pack3(2, 5, 0), pack3(5, 3, 0), pack3(1, 5, 2), pack3(5, 1, 3),
+                                    pack3(4, 2, 0), pack3(4, 0, 3), pack3(2, 4, 1), pack3(4, 3, 1)};
+            tv = t3[lane & 7];
+        }
+        W.tri[lane] = tv;
+    }
+    __syncwarp();
+    if (lane < ntri0) {
+        double x, y, z;
+        vertex_pos<D>(W.hp, W.tri[lane], x, y, z);
+        W.vd2[lane] = seed_d2(x, y, z, sx, sy, sz);
+    }
+    __syncwarp();
+    int nb_v = 2 * D, nb_t = ntri0;
+    int status = ST_SUCCESS, certk = 0;
+    double v_dist = max_vd2(W, nb_t, lane, nullptr);
+    double fail_vdist = 0.0;
+
+    for (int k = 0; k < K; k++) {
+        const uint32_t z = kl[k];
+        if (z == NO_NEIGHBOR) break;
+        const PT B = ext[z];
+        const double bx = B.x, by = B.y, bz = pz(B);
+        const double d2B = seed_d2(bx, by, bz, sx, sy, sz);  // (B - seed)^2 as cell.cpp:381-382
+        if (nb_v >= MAX_P) {  // new_halfplane (cell.cpp:159-162)
+            status = ST_VERTEX_OVERFLOW;
+            fail_vdist = v_dist;
+            break;
+        }
+        // new_halfplane: bisector plane (cell.cpp:164-168)
+        const double dx = sx - bx, dy = sy - by, dz = sz - bz;
+        const double ax = sx + bx, ay = sy + by, az = sz + bz;
+        const double dot = ax * dx + ay * dy + az * dz;
+        const double4 eq = make_double4(dx, dy, dz, -dot / 2.0);
+        const int cur = nb_v;
+        if (lane == 0) W.hp[cur] = eq;
+
+        // 1. conflicts
+        uint32_t cm[3];
+        bool near = false;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            int i = lane + 32 * j;
+            bool cf = false;
+            if (i < nb_t) cf = in_conflict<D>(W.hp, W.tri[i], eq, &near);
+            cm[j] = __ballot_sync(FULL, cf);
+        }
+        const int nb_r = __popc(cm[0]) + __popc(cm[1]) + __popc(cm[2]);
+        const uint32_t km[3] = {~cm[0], ~cm[1], ~cm[2]};
+        if (__any_sync(FULL, near)) {  // needs_exact_predicates: the reference keeps only the kept vertices
+            status = ST_NEEDS_EXACT_PREDICATES;
+            fail_vdist = max_vd2(W, nb_t, lane, km);
+            break;
+        }
+        if (nb_r == 0) {  // plane does not cut the cell: dropped (cell.cpp:133-136)
+            if (d2B > 4 * v_dist) {
+                certk = k + 1;
+                break;
+            }
+            continue;
+        }
+        __syncwarp();  // hp[cur] visible
+
+        // 2. cavity boundary
+        const int kept = nb_t - nb_r;
+        int n_new = 0;
+        bool bad = false;
+        uint32_t my_new[9];
+        int my_new_pos[9];
+        int my_new_cnt = 0;
+        if (D == 2) {
+            uint32_t lo = 0, hi = 0;  // XOR of the lines of removed vertices
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                int i = lane + 32 * j;
+                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
+                    uint32_t tv = W.tri[i];
+                    uint32_t a = tri_a(tv), b = tri_b(tv);
+                    if (a < 32) lo ^= 1u << a; else hi ^= 1u << (a - 32);
+                    if (b < 32) lo ^= 1u << b; else hi ^= 1u << (b - 32);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                lo ^= __shfl_xor_sync(FULL, lo, o);
+                hi ^= __shfl_xor_sync(FULL, hi, o);
+            }
+            unsigned long long xm = (unsigned long long)lo | ((unsigned long long)hi << 32);
+            if (__popcll(xm) < 2) {
+                bad = true;
+            } else {
+                int b0 = __ffsll((long long)xm) - 1;
+                unsigned long long x2 = xm & (xm - 1);
+                int b1 = __ffsll((long long)x2) - 1;
+                n_new = 2;
+                if (lane < 2) {
+                    int j = lane == 0 ? b0 : b1;
+                    const double4 hi_ = W.hp[cur], hj = W.hp[j];
+                    double rw = det2(hi_.x, hi_.y, hj.x, hj.y);  // new_vertex orientation (cell.cpp:351-359)
+                    my_new[0] = rw > 0 ? pack3(j, cur, 0) : pack3(cur, j, 0);
+                    my_new_pos[0] = lane;
+                    my_new_cnt = 1;
+                }
+            }
+        } else {
+            unsigned long long* em = W.u.b.emask;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                int i = lane + 32 * j;
+                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
+                    uint32_t tv = W.tri[i];
+                    uint32_t a = tri_a(tv), b = tri_b(tv), c = tri_c(tv);
+                    atomicOr(&em[a], 1ull << b);
+                    atomicOr(&em[b], 1ull << c);
+                    atomicOr(&em[c], 1ull << a);
+                }
+            }
+            __syncwarp();
+            unsigned long long src = 0ull;
+            int base = 0;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                int i = lane + 32 * j;
+                bool rem = i < nb_t && ((cm[j] >> lane) & 1u);
+                uint32_t tv = rem ? W.tri[i] : 0u;
+                uint32_t v3[3] = {tri_a(tv), tri_b(tv), tri_c(tv)};
+#pragma unroll
+                for (int ed = 0; ed < 3; ed++) {
+                    uint32_t x = v3[ed], y = v3[(ed + 1) % 3];
+                    bool isb = rem && !((em[y] >> x) & 1ull);
+                    unsigned bal = __ballot_sync(FULL, isb);
+                    if (isb) {
+                        my_new[my_new_cnt] = pack3(cur, x, y);
+                        my_new_pos[my_new_cnt] = base + __popc(bal & ((1u << lane) - 1u));
+                        my_new_cnt++;
+                        src |= 1ull << x;
+                        W.u.b.nxt[x] = (unsigned char)y;
+                    }
+                    base += __popc(bal);
+                }
+            }
+            n_new = base;
+            // OR-reduce the source planes; a simple cycle visits each source once
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) src |= __shfl_xor_sync(FULL, src, o);
+            __syncwarp();
+            bool ok = __popcll(src) == n_new && n_new >= 3;
+            if (ok && lane == 0) {
+                int x0 = __ffsll((long long)src) - 1, x = x0;
+                for (int st = 1; st <= n_new; st++) {
+                    x = W.u.b.nxt[x];
+                    if (!((src >> x) & 1ull) || (x == x0 && st < n_new)) {
+                        ok = false;
+                        break;
+                    }
+                }
+                if (x != x0) ok = false;
+            }
+            ok = __shfl_sync(FULL, ok ? 1 : 0, 0) != 0;
+            bad = !ok;
+            // clear the edge rows of removed vertices
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                int i = lane + 32 * j;
+                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
+                    uint32_t tv = W.tri[i];
+                    em[tri_a(tv)] = 0ull;
+                    em[tri_b(tv)] = 0ull;
+                    em[tri_c(tv)] = 0ull;
+                }
+            }
+            __syncwarp();
+        }
+        if (bad) {
+            status = ST_INCONSISTENT_BOUNDARY;
+            fail_vdist = max_vd2(W, nb_t, lane, km);
+            break;
+        }
+        // 3. new vertices and their certificate distances
+        double nd2[9];
+        double newmax = 0.0;
+        for (int q = 0; q < my_new_cnt; q++) {
+            double x, y, zz;
+            vertex_pos<D>(W.hp, my_new[q], x, y, zz);
+            nd2[q] = seed_d2(x, y, zz, sx, sy, sz);
+            newmax = fmax(newmax, nd2[q]);
+        }
+        if (kept + n_new >= MAX_T) {  // new_vertex overflow (cell.cpp:347-350)
+            status = ST_TRIANGLE_OVERFLOW;
+            fail_vdist = fmax(max_vd2(W, nb_t, lane, km), warp_max(newmax));
+            break;
+        }
+        // compaction: kept vertices in order, then the new ones
+        uint32_t kt[3];
+        double kd[3];
+        int kp[3];
+        int before = 0;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int i = lane + 32 * j;
+            const int nvalid = nb_t - 32 * j;
+            const uint32_t vm = nvalid >= 32 ? FULL : (nvalid > 0 ? ((1u << nvalid) - 1u) : 0u);
+            const uint32_t kmj = km[j] & vm;
+            const bool keep = (kmj >> lane) & 1u;
+            kt[j] = keep ? W.tri[i] : 0u;
+            kd[j] = keep ? W.vd2[i] : 0.0;
+            kp[j] = keep ? before + __popc(kmj & ((1u << lane) - 1u)) : -1;
+            before += __popc(kmj);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            if (kp[j] >= 0) {
+                W.tri[kp[j]] = kt[j];
+                W.vd2[kp[j]] = kd[j];
+            }
+        for (int q = 0; q < my_new_cnt; q++) {
+            W.tri[kept + my_new_pos[q]] = my_new[q];
+            W.vd2[kept + my_new_pos[q]] = nd2[q];
+        }
+        if (lane == 0) W.vid[cur] = (int)z;
+        nb_v++;
+        nb_t = kept + n_new;
+        __syncwarp();
+        v_dist = max_vd2(W, nb_t, lane, nullptr);
+        if (d2B > 4 * v_dist) {  // security radius reached (voronoi.cpp:224)
+            certk = k + 1;
+            break;
+        }
+    }
+    // final certificate with the K-th neighbour (voronoi.cpp:231-233)
+    {
+        const double vdf = status == ST_SUCCESS ? v_dist : fail_vdist;
+        const uint32_t zK = kl[K - 1];
+        if (zK == NO_NEIGHBOR) {
+            status = ST_SECURITY_RADIUS_NOT_REACHED;
+        } else {
+            const PT BK = ext[zK];
+            if (!(seed_d2(BK.x, BK.y, pz(BK), sx, sy, sz) > 4 * vdf)) status = ST_SECURITY_RADIUS_NOT_REACHED;
+        }
+    }
+    if (status != ST_SUCCESS) {
+        if (lane == 0) {
+            P.vol[e] = 0.0;
+            P.fptr[e] = 0;
+            P.fcnt[e] = 0;
+            P.status[e] = status;
+            P.certk[e] = 0;
+            P.centroid[3 * (size_t)e] = P.centroid[3 * (size_t)e + 1] = P.centroid[3 * (size_t)e + 2] = 0.0;
+        }
+        return;
+    }
+
+    // ---- extraction (cell.cpp:416-669)
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        int i = lane + 32 * j;
+        if (i < nb_t) vertex_pos<D>(W.hp, W.tri[i], W.u.vpos[i][0], W.u.vpos[i][1], W.u.vpos[i][2]);
+    }
+    __syncwarp();
+
+    double cell_vol = 0.0, cen[3] = {0.0, 0.0, 0.0};
+    if (D == 2) {
+        // compute_cell_area_2d (cell.cpp:475-498): vertices ordered by angle about their mean
+        double cx = 0, cy = 0;
+        for (int i = 0; i < nb_t; i++) cx += W.u.vpos[i][0], cy += W.u.vpos[i][1];
+        cx /= nb_t;
+        cy /= nb_t;
+        // rank of each vertex by angle; lane-parallel, then lane 0 sums in order
+        __shared__ unsigned char order_s[CLIP_WARPS][MAX_T];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            int i = lane + 32 * j;
+            if (i < nb_t) W.vd2[i] = atan2(W.u.vpos[i][1] - cy, W.u.vpos[i][0] - cx);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            int i = lane + 32 * j;
+            if (i < nb_t) {
+                const double ai = W.vd2[i];
+                int rank = 0;
+                for (int q = 0; q < nb_t; q++) {
+                    const double aq = W.vd2[q];
+                    rank += (aq < ai || (aq == ai && q < i)) ? 1 : 0;
+                }
+                order_s[w][rank] = (unsigned char)i;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            double a = 0, mx = 0, my = 0, sa = 0;
+            for (int i = 0; i < nb_t; i++) {
+                int j = (i + 1) % nb_t;
+                const double* pp = W.u.vpos[order_s[w][i]];
+                const double* qq = W.u.vpos[order_s[w][j]];
+                a += pp[0] * qq[1];
+                a -= qq[0] * pp[1];
+                double cr = (pp[0] - cx) * (qq[1] - cy) - (qq[0] - cx) * (pp[1] - cy);
+                mx += (pp[0] + qq[0] - 2 * cx) * cr;
+                my += (pp[1] + qq[1] - 2 * cy) * cr;
+                sa += cr;
+            }
+            cell_vol = fabs(a) / 2.0;
+            cen[0] = cx + mx / (3.0 * sa);
+            cen[1] = cy + my / (3.0 * sa);
+        }
+    }
+
+    // faces: lane handles planes p = lane and p = lane + 32
+    bool valid[2] = {false, false};
+    double area[2] = {0.0, 0.0};
+#pragma unroll
+    for (int pass = 0; pass < 2; pass++) {
+        const int p = lane + 32 * pass;
+        if (p >= nb_v) continue;
+        if (D == 2) {
+            int cnt = 0, v0 = -1, v1 = -1;
+            for (int i = 0; i < nb_t; i++) {
+                uint32_t tv = W.tri[i];
+                if ((int)tri_a(tv) == p || (int)tri_b(tv) == p) {
+                    if (cnt == 0) v0 = i; else if (cnt == 1) v1 = i;
+                    cnt++;
+                }
+            }
+            if (cnt >= 2) {
+                double ddx = W.u.vpos[v1][0] - W.u.vpos[v0][0];
+                double ddy = W.u.vpos[v1][1] - W.u.vpos[v0][1];
+                area[pass] = sqrt(ddx * ddx + ddy * ddy);
+                valid[pass] = true;
+            }
+        } else {
+            unsigned char fa[FACE_MAX_V], fb[FACE_MAX_V], fi[FACE_MAX_V];
+            int cnt = 0;
+            bool over = false;
+            for (int i = 0; i < nb_t; i++) {
+                uint32_t tv = W.tri[i];
+                uint32_t a = tri_a(tv), b = tri_b(tv), c = tri_c(tv);
+                uint32_t x, y;
+                if ((int)a == p) x = b, y = c;
+                else if ((int)b == p) x = c, y = a;
+                else if ((int)c == p) x = a, y = b;
+                else continue;
+                if (cnt < FACE_MAX_V) {
+                    fa[cnt] = (unsigned char)x;
+                    fb[cnt] = (unsigned char)y;
+                    fi[cnt] = (unsigned char)i;
+                } else {
+                    over = true;
+                }
+                cnt++;
+            }
+            double fv = 0.0, fc0 = 0.0, fc1 = 0.0, fc2 = 0.0;
+            if (cnt >= 3 && !over) {
+                // Walk the polygon: after vertex (p, a, b) comes (p, b, c).  Fan
+                // triangles (v0, v_{i-1}, v_i) give the area and, with the seed,
+                // the signed volume and first moment (cell.cpp:611-627).
+                const double* v0 = W.u.vpos[fi[0]];
+                const double a0 = v0[0] - sx, a1 = v0[1] - sy, a2 = v0[2] - sz;
+                int curv = 0;
+                double meas = 0.0;
+                bool ok = true;
+                for (int st = 1; st < cnt; st++) {
+                    int nx = -1;
+                    for (int q = 1; q < cnt; q++)
+                        if (fa[q] == fb[curv]) {
+                            nx = q;
+                            break;
+                        }
+                    if (nx < 0) {
+                        ok = false;
+                        break;
+                    }
+                    if (st >= 2) {
+                        const double* vi = W.u.vpos[fi[curv]];
+                        const double* vj = W.u.vpos[fi[nx]];
+                        double e1x = vi[0] - v0[0], e1y = vi[1] - v0[1], e1z = vi[2] - v0[2];
+                        double e2x = vj[0] - v0[0], e2y = vj[1] - v0[1], e2z = vj[2] - v0[2];
+                        double crx = e1y * e2z - e1z * e2y;
+                        double cry = e1z * e2x - e1x * e2z;
+                        double crz = e1x * e2y - e1y * e2x;
+                        meas += 0.5 * sqrt(crx * crx + cry * cry + crz * crz);
+                        double b0 = vi[0] - sx, b1 = vi[1] - sy, b2 = vi[2] - sz;
+                        double c0 = vj[0] - sx, c1 = vj[1] - sy, c2 = vj[2] - sz;
+                        double x0 = b1 * c2 - b2 * c1;
+                        double x1 = b2 * c0 - b0 * c2;
+                        double x2 = b0 * c1 - b1 * c0;
+                        double tv = (a0 * x0 + a1 * x1 + a2 * x2) / 6.0;
+                        fv += tv;
+                        fc0 += tv * (a0 + b0 + c0) * 0.25;
+                        fc1 += tv * (a1 + b1 + c1) * 0.25;
+                        fc2 += tv * (a2 + b2 + c2) * 0.25;
+                    }
+                    curv = nx;
+                }
+                if (ok && fb[curv] != fa[0]) ok = false;  // the walk must close on v0
+                if (ok) {
+                    valid[pass] = true;
+                    area[pass] = meas;
+                }
+            }
+            W.fvol[p] = valid[pass] ? fv : 0.0;
+            W.fcen[p][0] = valid[pass] ? fc0 : 0.0;
+            W.fcen[p][1] = valid[pass] ? fc1 : 0.0;
+            W.fcen[p][2] = valid[pass] ? fc2 : 0.0;
+        }
+    }
+    const uint32_t vb0 = __ballot_sync(FULL, valid[0]);
+    const uint32_t vb1 = __ballot_sync(FULL, valid[1]);
+    const int nf = __popc(vb0) + __popc(vb1);
+    __syncwarp();
+    if (D == 3 && lane == 0) {
+        for (int p = 0; p < nb_v; p++) {  // plane order, as the reference accumulates
+            cell_vol += W.fvol[p];
+            cen[0] += W.fcen[p][0];
+            cen[1] += W.fcen[p][1];
+            cen[2] += W.fcen[p][2];
+        }
+        const double sv = cell_vol;
+        cell_vol = fabs(sv);
+        cen[0] = sx + cen[0] / sv;
+        cen[1] = sy + cen[1] / sv;
+        cen[2] = sz + cen[2] / sv;
+    }
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(P.face_counter, (unsigned long long)nf);
+    base = __shfl_sync(FULL, base, 0);
+    const bool fits = base + (unsigned long long)nf <= P.face_cap;
+    if (!fits) {
+        if (lane == 0) atomicOr(P.overflow, 1u);
+    } else {
+#pragma unroll
+        for (int pass = 0; pass < 2; pass++) {
+            if (!valid[pass]) continue;
+            const int p = lane + 32 * pass;
+            const uint32_t vb = pass == 0 ? vb0 : vb1;
+            const int idx = (pass == 0 ? 0 : __popc(vb0)) + __popc(vb & ((1u << lane) - 1u));
+            const size_t f = base + idx;
+            const double4 pe = W.hp[p];
+            const double nlen = sqrt(pe.x * pe.x + pe.y * pe.y + pe.z * pe.z);  // compute_face_normal
+            const int nbr = W.vid[p];
+            P.f_nb[f] = nbr;
+            uint32_t own = BOX_FACE;
+            if (nbr >= 0) {
+                if ((int64_t)nbr < P.n_hydro)
+                    own = pack_owner((uint32_t)nbr, 0);
+                else
+                    own = pack_owner(P.ghost_src[nbr - P.n_hydro], P.ghost_code[nbr - P.n_hydro]);
+            }
+            P.f_own[f] = own;
+            P.f_geo[f] = make_double4(pe.x / nlen, pe.y / nlen, pe.z / nlen, P.ascale * area[pass]);
+        }
+    }
+    if (lane == 0) {
+        P.vol[e] = P.vscale * cell_vol;
+        P.fptr[e] = fits ? (uint32_t)base : 0u;
+        P.fcnt[e] = fits ? (uint32_t)nf : 0u;
+        P.status[e] = ST_SUCCESS;
+        P.certk[e] = certk;
+        P.centroid[3 * (size_t)e] = (cen[0] - 0.5) * P.scale + 0.5;
+        P.centroid[3 * (size_t)e + 1] = (cen[1] - 0.5) * P.scale + 0.5;
+        P.centroid[3 * (size_t)e + 2] = D == 3 ? (cen[2] - 0.5) * P.scale + 0.5 : 0.0;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_clip(pgpu_ctx* c) {
+    const int D = c->prm.dim;
+    cudaError_t e = cudaSuccess;
+    const int64_t n = c->n_ext;
+    ensure<double>(c->vol, n + 1, &e);
+    ensure<uint32_t>(c->fptr, n + 1, &e);
+    ensure<uint32_t>(c->fcnt, n + 1, &e);
+    ensure<int>(c->status, n + 1, &e);
+    ensure<int>(c->certk, n + 1, &e);
+    ensure<double>(c->centroid, 3 * n + 3, &e);
+    if (e) return e;
+    if (!c->all_cells && c->n_ext > c->n_hydro) {
+        // ghost cells are not computed in the per-step path
+        if ((e = cudaMemsetAsync(c->fcnt.p, 0, (n + 1) * sizeof(uint32_t), c->stream))) return e;
+        if ((e = cudaMemsetAsync(c->vol.p, 0, (n + 1) * sizeof(double), c->stream))) return e;
+    }
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    for (int attempt = 0; attempt < 3; attempt++) {
+        size_t want = c->face_cap;
+        if (want < (size_t)c->n_query * (D == 2 ? 8 : 20) + 1024) want = (size_t)c->n_query * (D == 2 ? 8 : 20) + 1024;
+        if (attempt > 0) want = want * 2;
+        ensure<int32_t>(c->f_nb, want, &e);
+        ensure<uint32_t>(c->f_own, want, &e);
+        ensure<double4>(c->f_geo, want, &e);
+        if (e) return e;
+        c->face_cap = want;
+        if ((e = cudaMemsetAsync(&sc->face_count, 0, sizeof(unsigned long long), c->stream))) return e;
+        if ((e = cudaMemsetAsync(&sc->overflow, 0, sizeof(unsigned int), c->stream))) return e;
+        ClipParams P;
+        P.qs = (const uint32_t*)c->qs.p;
+        P.perm = (const uint32_t*)c->perm.p;
+        P.spts = c->spts.p;
+        P.ext = c->ext.p;
+        P.knn = (const uint32_t*)c->knn.p;
+        P.ghost_src = (const uint32_t*)c->ghost_src.p;
+        P.ghost_code = (const uint32_t*)c->ghost_code.p;
+        P.nq = c->n_query;
+        P.n_hydro = c->n_hydro;
+        P.K = c->prm.k;
+        P.scale = c->unit_scale;
+        P.vscale = D == 2 ? P.scale * P.scale : P.scale * P.scale * P.scale;
+        P.ascale = D == 2 ? P.scale : P.scale * P.scale;
+        P.vol = (double*)c->vol.p;
+        P.fptr = (uint32_t*)c->fptr.p;
+        P.fcnt = (uint32_t*)c->fcnt.p;
+        P.status = (int*)c->status.p;
+        P.certk = (int*)c->certk.p;
+        P.centroid = (double*)c->centroid.p;
+        P.f_nb = (int32_t*)c->f_nb.p;
+        P.f_own = (uint32_t*)c->f_own.p;
+        P.f_geo = (double4*)c->f_geo.p;
+        P.face_counter = &sc->face_count;
+        P.overflow = &sc->overflow;
+        P.face_cap = c->face_cap;
+        if (c->n_query > 0) {
+            const unsigned blocks = (unsigned)((c->n_query + CLIP_WARPS - 1) / CLIP_WARPS);
+            if (D == 2)
+                k_clip<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+            else
+                k_clip<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+        }
+        if ((e = cudaGetLastError())) return e;
+        unsigned long long fc = 0;
+        unsigned int of = 0;
+        if ((e = cudaMemcpyAsync(&fc, &sc->face_count, sizeof(fc), cudaMemcpyDeviceToHost, c->stream))) return e;
+        if ((e = cudaMemcpyAsync(&of, &sc->overflow, sizeof(of), cudaMemcpyDeviceToHost, c->stream))) return e;
+        if ((e = cudaStreamSynchronize(c->stream))) return e;
+        c->num_faces = (int64_t)fc;
+        if (!of) return cudaSuccess;
+        c->face_cap = (size_t)fc + 1024;  // retry with room for all faces
+    }
+    return cudaErrorMemoryAllocation;
+}
+
+}  // namespace pgpu

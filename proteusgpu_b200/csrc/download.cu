@@ -1,0 +1,108 @@
+// Device -> reference layout conversions, run only when a caller asks for host
+// copies (the drop-in entry points and the tests).
+//
+// k_gather_faces replaces voronoi::unpermute_vmesh (src/voronoi/voronoi.cpp:298-419):
+// the extraction writes each cell's faces contiguously at a reserved slot; this
+// rebuilds the reference's CSR layout (cells in input order, face_ptr = prefix
+// sum of face_counts).  Neighbour ids are already input ids.
+#include "pgpu_common.cuh"
+#include "pgpu_ctx.h"
+
+namespace pgpu {
+namespace {
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+__global__ void k_gather_faces(const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fcnt,
+                               const uint32_t* __restrict__ new_ptr, const int32_t* __restrict__ f_nb,
+                               const double4* __restrict__ f_geo, int64_t n, int32_t* __restrict__ nb_out,
+                               double* __restrict__ nrm_out, double* __restrict__ area_out) {
+    // one warp per cell
+    const int64_t e = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (e >= n) return;
+    const uint32_t src = fptr[e], cnt = fcnt[e], dst = new_ptr[e];
+    for (uint32_t q = lane; q < cnt; q += 32) {
+        const double4 g = f_geo[src + q];
+        nb_out[dst + q] = f_nb[src + q];
+        nrm_out[3 * (size_t)(dst + q)] = g.x;
+        nrm_out[3 * (size_t)(dst + q) + 1] = g.y;
+        nrm_out[3 * (size_t)(dst + q) + 2] = g.z;
+        area_out[dst + q] = g.w;
+    }
+}
+
+// VMesh seeds: the unit-box point scaled back, (s - 0.5) * scale + 0.5
+// (periodic_mesh.cpp:146-166); 3 doubles per cell, z = 0 in 2D.  As in the
+// reference, only extracted cells carry their seed (cell.cpp:418-420); the
+// others hold the scaled-back zero.
+template <int D>
+__global__ void k_seeds(const typename PointOf<D>::type* __restrict__ ext, const int* __restrict__ status,
+                        int64_t n, double scale, int no_scale, double* __restrict__ out) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const typename PointOf<D>::type p = ext[e];
+    const bool ok = status[e] == ST_SUCCESS;
+    double c[3] = {ok ? p.x : 0.0, ok ? p.y : 0.0, ok ? pz(p) : 0.0};
+    for (int a = 0; a < 3; a++) out[3 * e + a] = (a < D && !no_scale) ? (c[a] - 0.5) * scale + 0.5 : c[a];
+}
+
+__global__ void k_knn_rows(const uint32_t* __restrict__ knn, const uint32_t* __restrict__ qs,
+                           const uint32_t* __restrict__ perm, int64_t nq, int K, uint32_t* __restrict__ out) {
+    const int64_t t = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (t >= nq) return;
+    const uint32_t q = perm[qs[t]];
+    for (int j = lane; j < K; j += 32) out[(size_t)q * K + j] = knn[(size_t)t * K + j];
+}
+
+template <int D>
+__global__ void k_unpack_points(const typename PointOf<D>::type* __restrict__ p, int64_t n, double* __restrict__ out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i * D] = p[i].x;
+    out[i * D + 1] = p[i].y;
+    if (D == 3) out[i * D + 2] = pz(p[i]);
+}
+
+}  // namespace
+
+cudaError_t launch_mesh_compact(pgpu_ctx* c, uint32_t* new_ptr, int32_t* nb_out, double* nrm_out, double* area_out) {
+    const int64_t n = c->n_ext;
+    cudaError_t e = exclusive_scan_u32((const uint32_t*)c->fcnt.p, new_ptr, n, c->scan_tmp, c->stream);
+    if (e) return e;
+    if (n > 0)
+        k_gather_faces<<<nblk(n * 32, 256), 256, 0, c->stream>>>(
+            (const uint32_t*)c->fptr.p, (const uint32_t*)c->fcnt.p, new_ptr, (const int32_t*)c->f_nb.p,
+            (const double4*)c->f_geo.p, n, nb_out, nrm_out, area_out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_seeds(pgpu_ctx* c, double* out, bool no_scale) {
+    const int64_t n = c->n_ext;
+    if (n <= 0) return cudaSuccess;
+    if (c->prm.dim == 2)
+        k_seeds<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, (const int*)c->status.p, n, c->unit_scale, no_scale, out);
+    else
+        k_seeds<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, (const int*)c->status.p, n, c->unit_scale, no_scale, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_knn_rows(pgpu_ctx* c, uint32_t* out) {
+    const int64_t nq = c->n_query;
+    if (nq <= 0) return cudaSuccess;
+    k_knn_rows<<<nblk(nq * 32, 256), 256, 0, c->stream>>>((const uint32_t*)c->knn.p, (const uint32_t*)c->qs.p,
+                                                           (const uint32_t*)c->perm.p, nq, c->prm.k, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unpack_points(pgpu_ctx* c, const void* pts, int64_t n, double* out) {
+    if (n <= 0) return cudaSuccess;
+    if (c->prm.dim == 2)
+        k_unpack_points<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)pts, n, out);
+    else
+        k_unpack_points<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)pts, n, out);
+    return cudaGetLastError();
+}
+
+}  // namespace pgpu

@@ -1,0 +1,430 @@
+// Hydro on the device mesh.
+//
+// Reference semantics (src/hydro/finite_volume_solver.cpp:43-186):
+//   k_dt_ref    hydro::dt_CFL   min over cells of CFL R_i / (c_i + |v_i|)
+//   k_hydro_ref hydro::hydro_step: per cell, sum over its faces of the HLL flux
+//               (riemann.cpp:7-45) times the face area, then
+//               rho' = rho - dt/V F_rho, v' = (rho v - dt/V F_m) / rho',
+//               E' = E - dt/V F_E, written to a second buffer.
+// Moving-mesh form (extension; the reference never moves its mesh):
+//   k_prim_dt     primitives from the conserved mass, momentum and energy on
+//                 the new mesh, and the CFL step in the same pass;
+//   k_flux_update HLL fluxes with the conserved update and the drift of the
+//                 generating point, one thread per cell gathering its faces
+//                 (no atomics).  In PGPU_FLUX_PHYSICAL mode the normal is the
+//                 outward one and the area is the one the lower hydro id
+//                 computed for that face, so each face's flux cancels exactly
+//                 between its two cells.
+// All arithmetic is FP64 without FMA, operation for operation the reference's,
+// so a flux computed from the same inputs is bit-identical.
+#include <math_constants.h>
+
+#include "pgpu_common.cuh"
+#include "pgpu_ctx.h"
+
+namespace pgpu {
+namespace {
+
+constexpr int HT = 256;  // threads per block
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+__device__ __forceinline__ double block_min(double v) {
+    __shared__ double sm[HT / 32];
+    for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        v = threadIdx.x < HT / 32 ? sm[threadIdx.x] : CUDART_INF;
+        for (int o = 16; o > 0; o >>= 1) v = fmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    }
+    return v;
+}
+
+template <int D>
+__device__ __forceinline__ double dt_cell(const Prim& s, double V, double cfl, double gamma) {
+    double P = pressure<D>(s, gamma);
+    double c = sqrt(gamma * P / s.rho);
+    double R, va;
+    if (D == 2) {
+        R = sqrt(V / CUDART_PI);
+        va = sqrt(s.vx * s.vx + s.vy * s.vy);
+    } else {
+        R = cbrt(3.0 * V / (4.0 * CUDART_PI));
+        va = sqrt(s.vx * s.vx + s.vy * s.vy + s.vz * s.vz);
+    }
+    return cfl * (R / (c + va));
+}
+
+template <int D>
+__device__ __forceinline__ Prim load_prim(const double* rho, const double* v, const double* E, int64_t i) {
+    Prim s;
+    s.rho = rho[i];
+    s.vx = v[i * D];
+    s.vy = v[i * D + 1];
+    s.vz = D == 3 ? v[i * D + 2] : 0.0;
+    s.E = E[i];
+    return s;
+}
+
+// ---- reference hydro::dt_CFL
+template <int D>
+__global__ void k_dt_ref(const double* __restrict__ rho, const double* __restrict__ v, const double* __restrict__ E,
+                         const double* __restrict__ vol, int64_t n, double cfl, double gamma,
+                         unsigned long long* __restrict__ dt_bits) {
+    int64_t i = (int64_t)blockIdx.x * HT + threadIdx.x;
+    double d = 1e100;
+    if (i < n) d = dt_cell<D>(load_prim<D>(rho, v, E, i), vol[i], cfl, gamma);
+    d = block_min(d);
+    if (threadIdx.x == 0) atomicMin(dt_bits, dbits(d));
+}
+
+// ---- reference hydro::hydro_step on primitives (rho, v, E) -> (rho2, v2, E2)
+template <int D, bool PHYSICAL>
+__global__ void k_hydro_ref(const double* __restrict__ rho, const double* __restrict__ v,
+                            const double* __restrict__ E, const double* __restrict__ vol,
+                            const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fcnt,
+                            const uint32_t* __restrict__ f_own, const double4* __restrict__ f_geo, int64_t n,
+                            double dt, double gamma, double* __restrict__ rho2, double* __restrict__ v2,
+                            double* __restrict__ E2, unsigned int* __restrict__ box_faces) {
+    int64_t i = (int64_t)blockIdx.x * HT + threadIdx.x;
+    if (i >= n) return;
+    const Prim si = load_prim<D>(rho, v, E, i);
+    double tr = 0, tx = 0, ty = 0, tz = 0, te = 0;
+    const uint32_t fp = fptr[i], nf = fcnt[i];
+    unsigned nbox = 0;
+    for (uint32_t q = 0; q < nf; q++) {
+        const uint32_t own = f_own[fp + q];
+        const double4 g = f_geo[fp + q];
+        int64_t h = i;
+        if (own == BOX_FACE) nbox++;
+        else h = own & OWNER_MASK;
+        const Prim sj = load_prim<D>(rho, v, E, h);
+        const Flux fl = PHYSICAL ? hll<D>(si, sj, -g.x, -g.y, -g.z, gamma) : hll<D>(si, sj, g.x, g.y, g.z, gamma);
+        const double A = g.w;
+        tr += fl.rho * A;
+        tx += fl.mx * A;
+        ty += fl.my * A;
+        if (D == 3) tz += fl.mz * A;
+        te += fl.E * A;
+    }
+    if (nbox) atomicAdd(box_faces, nbox);
+    const double V = vol[i];
+    const double frac = dt / V;
+    const double nr = si.rho - frac * tr;
+    const double inv = 1.0 / nr;
+    rho2[i] = nr;
+    v2[i * D] = (si.rho * si.vx - frac * tx) * inv;
+    v2[i * D + 1] = (si.rho * si.vy - frac * ty) * inv;
+    if (D == 3) v2[i * D + 2] = (si.rho * si.vz - frac * tz) * inv;
+    E2[i] = si.E - frac * te;
+}
+
+// ---- moving mesh: conserved variables from primitives on the first mesh
+template <int D>
+__global__ void k_cons_from_prim(const double* __restrict__ rho, const double* __restrict__ v,
+                                 const double* __restrict__ E, const double* __restrict__ dep,
+                                 const double* __restrict__ vol, int64_t n, double* __restrict__ mass,
+                                 double* __restrict__ mom, double* __restrict__ en) {
+    int64_t i = (int64_t)blockIdx.x * HT + threadIdx.x;
+    if (i >= n) return;
+    const double V = vol[i];
+    mass[i] = rho[i] * V;
+#pragma unroll
+    for (int a = 0; a < D; a++) mom[i * D + a] = (rho[i] * v[i * D + a]) * V;
+    double e = E[i] * V;
+    if (dep) e = e + dep[i];
+    en[i] = e;
+}
+
+// ---- moving mesh: primitives + CFL step (+ failed-cell and cert-K statistics)
+template <int D>
+__global__ void k_prim_dt(const double* __restrict__ mass, const double* __restrict__ mom,
+                          const double* __restrict__ en, const double* __restrict__ vol,
+                          const int* __restrict__ status, const int* __restrict__ certk, int64_t n, double cfl,
+                          double gamma, double4* __restrict__ w4, double* __restrict__ we,
+                          DevScalars* __restrict__ sc) {
+    int64_t i = (int64_t)blockIdx.x * HT + threadIdx.x;
+    double d = 1e100;
+    if (i < n) {
+        const double V = vol[i];
+        const double m = mass[i];
+        Prim s;
+        s.rho = m / V;
+        s.vx = mom[i * D] / m;
+        s.vy = mom[i * D + 1] / m;
+        s.vz = D == 3 ? mom[i * D + 2] / m : 0.0;
+        s.E = en[i] / V;
+        w4[i] = make_double4(s.rho, s.vx, s.vy, s.vz);
+        we[i] = s.E;
+        d = dt_cell<D>(s, V, cfl, gamma);
+        if (status[i] != ST_SUCCESS) atomicAdd(&sc->failed, 1u);
+        else atomicMax(&sc->cert_k_max, certk[i]);
+    }
+    d = block_min(d);
+    if (threadIdx.x == 0) atomicMin(&sc->dt_bits, dbits(d));
+}
+
+template <int D, bool PHYSICAL, bool MIRROR>
+__global__ void k_flux_update(const double4* __restrict__ w4, const double* __restrict__ we,
+                              const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fcnt,
+                              const uint32_t* __restrict__ f_own, const double4* __restrict__ f_geo, int64_t n,
+                              double gamma, double fixed_dt, double* __restrict__ mass, double* __restrict__ mom,
+                              double* __restrict__ en, double* __restrict__ pos, DevScalars* __restrict__ sc) {
+    int64_t i = (int64_t)blockIdx.x * HT + threadIdx.x;
+    if (i >= n) return;
+    const double dt = fixed_dt > 0 ? fixed_dt : __longlong_as_double((long long)sc->dt_bits);
+    const double4 wi = w4[i];
+    const Prim si = {wi.x, wi.y, wi.z, wi.w, we[i]};
+    double tr = 0, tx = 0, ty = 0, tz = 0, te = 0;
+    const uint32_t fp = fptr[i], nf = fcnt[i];
+    unsigned nbox = 0, nunp = 0;
+    for (uint32_t q = 0; q < nf; q++) {
+        const uint32_t own = f_own[fp + q];
+        const double4 g = f_geo[fp + q];
+        uint32_t h = (uint32_t)i;
+        uint32_t code = 0;
+        double A = g.w;
+        if (own == BOX_FACE) {
+            nbox++;
+        } else {
+            h = own & OWNER_MASK;
+            code = own >> OWNER_BITS;
+            if (PHYSICAL && h < (uint32_t)i) {
+                // the lower hydro id's value of this face's area
+                const uint32_t want = pack_owner((uint32_t)i, reverse_code(code, D, !MIRROR));
+                const uint32_t hp = fptr[h], hn = fcnt[h];
+                bool found = false;
+                for (uint32_t r = 0; r < hn; r++)
+                    if (f_own[hp + r] == want) {
+                        A = f_geo[hp + r].w;
+                        found = true;
+                        break;
+                    }
+                if (!found) nunp++;
+            }
+        }
+        const double4 wj4 = w4[h];
+        Prim sj = {wj4.x, wj4.y, wj4.z, wj4.w, we[h]};
+        if (MIRROR && code) {
+            uint32_t cd = code;
+            if (cd % 3) sj.vx = -sj.vx;
+            cd /= 3;
+            if (cd % 3) sj.vy = -sj.vy;
+            cd /= 3;
+            if (D == 3 && (cd % 3)) sj.vz = -sj.vz;
+        }
+        const Flux fl = PHYSICAL ? hll<D>(si, sj, -g.x, -g.y, -g.z, gamma) : hll<D>(si, sj, g.x, g.y, g.z, gamma);
+        tr += fl.rho * A;
+        tx += fl.mx * A;
+        ty += fl.my * A;
+        if (D == 3) tz += fl.mz * A;
+        te += fl.E * A;
+    }
+    if (nbox) atomicAdd(&sc->box_faces, nbox);
+    if (nunp) atomicAdd(&sc->unpaired, nunp);
+    mass[i] = mass[i] - dt * tr;
+    mom[i * D] = mom[i * D] - dt * tx;
+    mom[i * D + 1] = mom[i * D + 1] - dt * ty;
+    if (D == 3) mom[i * D + 2] = mom[i * D + 2] - dt * tz;
+    en[i] = en[i] - dt * te;
+    // drift with the cell's velocity at the start of the step, then wrap or reflect
+    const double vv[3] = {si.vx, si.vy, si.vz};
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        double p = pos[i * D + a] + vv[a] * dt;
+        if (!MIRROR) {
+            if (p < 0.0) p += 1.0;
+            if (p >= 1.0) p -= 1.0;
+        } else {
+            if (p < 0.0) p = -p;
+            if (p >= 1.0) p = 2.0 - p;
+            if (p >= 1.0) p = 0x1.fffffffffffffp-1;
+        }
+        pos[i * D + a] = p;
+    }
+}
+
+// Deterministic sums (mass, momentum, energy) over hydro cells: fixed block
+// partials, then one ordered pass.
+template <int D>
+__global__ void k_partial_sums(const double* __restrict__ mass, const double* __restrict__ mom,
+                               const double* __restrict__ en, int64_t n, double* __restrict__ part) {
+    __shared__ double sm[5][HT];
+    int64_t i = (int64_t)blockIdx.x * HT + threadIdx.x;
+    double v[5] = {0, 0, 0, 0, 0};
+    if (i < n) {
+        v[0] = mass[i];
+        for (int a = 0; a < D; a++) v[1 + a] = mom[i * D + a];
+        v[4] = en[i];
+    }
+    for (int k = 0; k < 5; k++) sm[k][threadIdx.x] = v[k];
+    __syncthreads();
+    for (int s = HT / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s)
+            for (int k = 0; k < 5; k++) sm[k][threadIdx.x] += sm[k][threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 5; k++) part[blockIdx.x * 5 + k] = sm[k][0];
+}
+
+__global__ void k_final_sums(const double* __restrict__ part, int64_t nb, double* __restrict__ out) {
+    if (threadIdx.x >= 5) return;
+    double s = 0;
+    for (int64_t b = 0; b < nb; b++) s += part[b * 5 + threadIdx.x];
+    out[threadIdx.x] = s;
+}
+
+}  // namespace
+
+cudaError_t launch_dt_ref(pgpu_ctx* c, double cfl) {
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    const unsigned long long init = 0x54B249AD2594C37Dull;  // bit pattern of 1e100
+    cudaError_t e = cudaMemcpyAsync(&sc->dt_bits, &init, sizeof(init), cudaMemcpyHostToDevice, c->stream);
+    if (e) return e;
+    const int64_t n = c->n_hydro;
+    if (n > 0) {
+        if (c->prm.dim == 2)
+            k_dt_ref<2><<<nblk(n, HT), HT, 0, c->stream>>>((const double*)c->rho.p, (const double*)c->vel.p,
+                                                            (const double*)c->energy.p, (const double*)c->vol.p, n,
+                                                            cfl, c->prm.gamma, &sc->dt_bits);
+        else
+            k_dt_ref<3><<<nblk(n, HT), HT, 0, c->stream>>>((const double*)c->rho.p, (const double*)c->vel.p,
+                                                            (const double*)c->energy.p, (const double*)c->vol.p, n,
+                                                            cfl, c->prm.gamma, &sc->dt_bits);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hydro_ref(pgpu_ctx* c, double dt) {
+    cudaError_t e = cudaSuccess;
+    const int D = c->prm.dim;
+    const int64_t n = c->n_hydro;
+    double* r2 = ensure<double>(c->rho2, n + 1, &e);
+    double* v2 = ensure<double>(c->vel2, n * D + 1, &e);
+    double* e2 = ensure<double>(c->energy2, n + 1, &e);
+    if (e) return e;
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    const bool phys = c->prm.flux_mode == PGPU_FLUX_PHYSICAL;
+    if (n > 0) {
+#define PGPU_HREF(DD, PH)                                                                                         \
+    k_hydro_ref<DD, PH><<<nblk(n, HT), HT, 0, c->stream>>>(                                                      \
+        (const double*)c->rho.p, (const double*)c->vel.p, (const double*)c->energy.p, (const double*)c->vol.p, \
+        (const uint32_t*)c->fptr.p, (const uint32_t*)c->fcnt.p, (const uint32_t*)c->f_own.p,                   \
+        (const double4*)c->f_geo.p, n, dt, c->prm.gamma, r2, v2, e2, &sc->box_faces)
+        if (D == 2) {
+            if (phys) PGPU_HREF(2, true); else PGPU_HREF(2, false);
+        } else {
+            if (phys) PGPU_HREF(3, true); else PGPU_HREF(3, false);
+        }
+#undef PGPU_HREF
+    }
+    if ((e = cudaGetLastError())) return e;
+    std::swap(c->rho, c->rho2);
+    std::swap(c->vel, c->vel2);
+    std::swap(c->energy, c->energy2);
+    return cudaSuccess;
+}
+
+cudaError_t launch_cons_from_prim(pgpu_ctx* c, const double* dep) {
+    cudaError_t e = cudaSuccess;
+    const int D = c->prm.dim;
+    const int64_t n = c->n_hydro;
+    ensure<double>(c->mass, n + 1, &e);
+    ensure<double>(c->mom, n * D + 1, &e);
+    ensure<double>(c->en, n + 1, &e);
+    if (e) return e;
+    if (n > 0) {
+        if (D == 2)
+            k_cons_from_prim<2><<<nblk(n, HT), HT, 0, c->stream>>>(
+                (const double*)c->rho.p, (const double*)c->vel.p, (const double*)c->energy.p, dep,
+                (const double*)c->vol.p, n, (double*)c->mass.p, (double*)c->mom.p, (double*)c->en.p);
+        else
+            k_cons_from_prim<3><<<nblk(n, HT), HT, 0, c->stream>>>(
+                (const double*)c->rho.p, (const double*)c->vel.p, (const double*)c->energy.p, dep,
+                (const double*)c->vol.p, n, (double*)c->mass.p, (double*)c->mom.p, (double*)c->en.p);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_prim_dt(pgpu_ctx* c, double cfl, double fixed_dt) {
+    cudaError_t e = cudaSuccess;
+    const int64_t n = c->n_hydro;
+    double4* w4 = ensure<double4>(c->w4, n + 1, &e);
+    double* we = ensure<double>(c->we, n + 1, &e);
+    if (e) return e;
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    // reset the per-step statistics and the dt accumulator (1e100 as the reference's start value)
+    DevScalars init{};
+    init.dt_bits = 0x54B249AD2594C37Dull;
+    if ((e = cudaMemcpyAsync(&sc->dt_bits, &init.dt_bits, sizeof(init.dt_bits), cudaMemcpyHostToDevice, c->stream)))
+        return e;
+    if ((e = cudaMemsetAsync(&sc->overflow, 0, offsetof(DevScalars, dt) - offsetof(DevScalars, overflow),
+                             c->stream)))
+        return e;
+    (void)fixed_dt;
+    if (n > 0) {
+        if (c->prm.dim == 2)
+            k_prim_dt<2><<<nblk(n, HT), HT, 0, c->stream>>>((const double*)c->mass.p, (const double*)c->mom.p,
+                                                            (const double*)c->en.p, (const double*)c->vol.p,
+                                                            (const int*)c->status.p, (const int*)c->certk.p, n, cfl,
+                                                            c->prm.gamma, w4, we, sc);
+        else
+            k_prim_dt<3><<<nblk(n, HT), HT, 0, c->stream>>>((const double*)c->mass.p, (const double*)c->mom.p,
+                                                            (const double*)c->en.p, (const double*)c->vol.p,
+                                                            (const int*)c->status.p, (const int*)c->certk.p, n, cfl,
+                                                            c->prm.gamma, w4, we, sc);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_flux_update(pgpu_ctx* c, double fixed_dt) {
+    const int D = c->prm.dim;
+    const int64_t n = c->n_hydro;
+    if (n <= 0) return cudaSuccess;
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    const bool phys = c->prm.flux_mode == PGPU_FLUX_PHYSICAL;
+    const bool mir = c->prm.boundary == PGPU_REFLECTIVE;
+#define PGPU_FLUX(DD, PH, MI)                                                                                     \
+    k_flux_update<DD, PH, MI><<<nblk(n, HT), HT, 0, c->stream>>>(                                                \
+        (const double4*)c->w4.p, (const double*)c->we.p, (const uint32_t*)c->fptr.p, (const uint32_t*)c->fcnt.p, \
+        (const uint32_t*)c->f_own.p, (const double4*)c->f_geo.p, n, c->prm.gamma, fixed_dt, (double*)c->mass.p,  \
+        (double*)c->mom.p, (double*)c->en.p, (double*)c->pos.p, sc)
+    if (D == 2) {
+        if (phys) {
+            if (mir) PGPU_FLUX(2, true, true); else PGPU_FLUX(2, true, false);
+        } else {
+            if (mir) PGPU_FLUX(2, false, true); else PGPU_FLUX(2, false, false);
+        }
+    } else {
+        if (phys) {
+            if (mir) PGPU_FLUX(3, true, true); else PGPU_FLUX(3, true, false);
+        } else {
+            if (mir) PGPU_FLUX(3, false, true); else PGPU_FLUX(3, false, false);
+        }
+    }
+#undef PGPU_FLUX
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sums(pgpu_ctx* c) {
+    cudaError_t e = cudaSuccess;
+    const int64_t n = c->n_hydro;
+    const int64_t nb = (n + HT - 1) / HT;
+    double* part = ensure<double>(c->red_tmp, 5 * (nb + 1), &e);
+    if (e) return e;
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    if (n > 0) {
+        if (c->prm.dim == 2)
+            k_partial_sums<2><<<(unsigned)nb, HT, 0, c->stream>>>((const double*)c->mass.p, (const double*)c->mom.p,
+                                                                  (const double*)c->en.p, n, part);
+        else
+            k_partial_sums<3><<<(unsigned)nb, HT, 0, c->stream>>>((const double*)c->mass.p, (const double*)c->mom.p,
+                                                                  (const double*)c->en.p, n, part);
+        k_final_sums<<<1, 32, 0, c->stream>>>(part, nb, sc->sums);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace pgpu

@@ -1,0 +1,264 @@
+// Mesh inputs on the device: ghost layer + unit-box scaling, Morton-ordered
+// grid sort, and the list of cells to compute.
+//
+// Ghosts restate src/voronoi/periodic_mesh.cpp:63-126: for every hydro point,
+// the 8 (2D) or 26 (3D) boundary regions are tested in the reference's order,
+// which numbers the ghosts (ghost ids appear as face neighbours).  A count
+// pass, a prefix sum and a write pass place each point's ghosts after all hydro
+// points, exactly where the reference's serial append puts them.
+//
+// The grid sort replaces knn::sort_points_into_grid (src/knn/knn.cpp:119-154):
+// points are binned on a uniform grid whose bins are numbered in Morton order,
+// so that spatially close bins are close in memory; a histogram, a prefix sum
+// and a scatter produce the sorted points and the sorted -> extended-id map.
+#include "pgpu_common.cuh"
+#include "pgpu_ctx.h"
+
+namespace pgpu {
+namespace {
+
+// Shift vectors of the ghost regions in the order of periodic_mesh.cpp:71-79
+// (2D) and :83-110 (3D); a +1 shift selects the open interval (0, buff) on that
+// axis, -1 selects (1 - buff, 1), 0 selects (0, 1).
+__constant__ int8_t c_reg2[8][2] = {{1, 0}, {0, -1}, {-1, 0}, {0, 1}, {1, 1}, {1, -1}, {-1, -1}, {-1, 1}};
+__constant__ int8_t c_reg3[26][3] = {
+    {0, 0, 1},  {1, 0, 0},   {0, -1, 0},  {-1, 0, 0}, {0, 1, 0},  {0, 0, -1}, {0, 1, 1},   {1, 0, 1},   {0, -1, 1},
+    {-1, 0, 1}, {1, 1, 0},   {1, -1, 0},  {-1, -1, 0}, {-1, 1, 0}, {1, 0, -1}, {0, -1, -1}, {-1, 0, -1}, {0, 1, -1},
+    {1, 1, 1},  {1, -1, 1},  {-1, -1, 1}, {-1, 1, 1}, {1, 1, -1}, {1, -1, -1}, {-1, -1, -1}, {-1, 1, -1}};
+
+template <int D>
+__device__ __forceinline__ int shift_of(int r, int a) {
+    return D == 2 ? c_reg2[r][a] : c_reg3[r][a];
+}
+
+template <int D>
+__device__ __forceinline__ bool in_region(const double* p, int r, double buff) {
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        int s = shift_of<D>(r, a);
+        double lo = s > 0 ? 0. : (s < 0 ? 1. - buff : 0.);
+        double hi = s > 0 ? 0. + buff : 1.;
+        if (!(p[a] > lo && p[a] < hi)) return false;
+    }
+    return true;
+}
+
+template <int D>
+__global__ void k_ghost_count(const double* __restrict__ pos, int64_t n, double buff, uint32_t* __restrict__ cnt) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double p[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) p[a] = pos[i * D + a];
+    constexpr int NR = D == 2 ? 8 : 26;
+    uint32_t c = 0;
+    for (int r = 0; r < NR; r++) c += in_region<D>(p, r, buff) ? 1u : 0u;
+    cnt[i] = c;
+}
+
+template <int D>
+__global__ void k_ghost_write(const double* __restrict__ pos, int64_t n, double buff, double scale, int mirror,
+                              int no_ghosts, const uint32_t* __restrict__ goff,
+                              typename PointOf<D>::type* __restrict__ ext, uint32_t* __restrict__ gsrc,
+                              uint32_t* __restrict__ gcode) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double p[D];
+#pragma unroll
+    for (int a = 0; a < D; a++) p[a] = pos[i * D + a];
+    if (no_ghosts) {  // compute_mesh: points are used as given
+        ext[i] = make_pt<D>(p[0], p[1], D == 3 ? p[D - 1] : 0.0);
+        return;
+    }
+    // scale into [0,1]^D: scale * (x - 0.5) + 0.5 (periodic_mesh.cpp:119-126)
+    double q[3] = {0, 0, 0};
+#pragma unroll
+    for (int a = 0; a < D; a++) q[a] = scale * (p[a] - 0.5) + 0.5;
+    ext[i] = make_pt<D>(q[0], q[1], q[2]);
+    constexpr int NR = D == 2 ? 8 : 26;
+    uint32_t k = goff[i];
+    for (int r = 0; r < NR; r++) {
+        if (!in_region<D>(p, r, buff)) continue;
+        double g[3] = {0, 0, 0};
+        uint32_t code = 0, mul = 1;
+#pragma unroll
+        for (int a = 0; a < D; a++) {
+            int s = shift_of<D>(r, a);
+            if (!mirror)
+                g[a] = p[a] + (double)s;  // add_ghost (periodic_mesh.cpp:28-33)
+            else
+                g[a] = s > 0 ? -p[a] : (s < 0 ? 2.0 - p[a] : p[a]);
+            code += (s == 0 ? 0u : (s > 0 ? 1u : 2u)) * mul;
+            mul *= 3;
+        }
+#pragma unroll
+        for (int a = 0; a < D; a++) g[a] = scale * (g[a] - 0.5) + 0.5;
+        ext[n + k] = make_pt<D>(g[0], g[1], g[2]);
+        gsrc[k] = (uint32_t)i;
+        gcode[k] = code;
+        k++;
+    }
+}
+
+template <int D>
+__global__ void k_bin_count(const typename PointOf<D>::type* __restrict__ ext, int64_t n, int G,
+                            uint32_t* __restrict__ key, uint32_t* __restrict__ cnt) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    typename PointOf<D>::type p = ext[e];
+    uint32_t k = morton<D>(bin_coord(p.x, G), bin_coord(p.y, G), D == 3 ? bin_coord(pz(p), G) : 0);
+    key[e] = k;
+    atomicAdd(&cnt[k], 1u);
+}
+
+template <int D>
+__global__ void k_bin_scatter(const typename PointOf<D>::type* __restrict__ ext, int64_t n,
+                              const uint32_t* __restrict__ key, const uint32_t* __restrict__ start,
+                              uint32_t* __restrict__ fill, typename PointOf<D>::type* __restrict__ spts,
+                              uint32_t* __restrict__ perm, uint32_t* __restrict__ inv) {
+    int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    uint32_t k = key[e];
+    uint32_t s = start[k] + atomicAdd(&fill[k], 1u);
+    spts[s] = ext[e];
+    perm[s] = (uint32_t)e;
+    inv[e] = s;
+}
+
+__global__ void k_query_flags(const uint32_t* __restrict__ perm, int64_t n_ext, int64_t n_hydro,
+                              uint32_t* __restrict__ flag) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_ext) return;
+    flag[s] = perm[s] < (uint32_t)n_hydro ? 1u : 0u;
+}
+
+__global__ void k_query_compact(const uint32_t* __restrict__ flag, const uint32_t* __restrict__ off, int64_t n_ext,
+                                uint32_t* __restrict__ qs) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_ext) return;
+    if (flag[s]) qs[off[s]] = (uint32_t)s;
+}
+
+__global__ void k_iota(uint32_t* __restrict__ q, int64_t n) {
+    int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) q[s] = (uint32_t)s;
+}
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+}  // namespace
+
+cudaError_t launch_ghosts(pgpu_ctx* c, const double* pos_dev, int64_t n, bool no_ghosts) {
+    const int D = c->prm.dim;
+    cudaError_t e = cudaSuccess;
+    const double buff = c->prm.buff;
+    const double scale = 1. / (1. + (2 * buff));
+    int64_t ng = 0;
+    if (!no_ghosts) {
+        uint32_t* cnt = ensure<uint32_t>(c->gcnt, n + 1, &e);
+        uint32_t* off = ensure<uint32_t>(c->goff, n + 1, &e);
+        if (e) return e;
+        if (n > 0) {
+            if (D == 2)
+                k_ghost_count<2><<<nblk(n, 256), 256, 0, c->stream>>>(pos_dev, n, buff, cnt);
+            else
+                k_ghost_count<3><<<nblk(n, 256), 256, 0, c->stream>>>(pos_dev, n, buff, cnt);
+        }
+        if ((e = exclusive_scan_u32(cnt, off, n, c->scan_tmp, c->stream))) return e;
+        uint32_t total = 0;
+        if ((e = cudaMemcpyAsync(&total, off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream))) return e;
+        if ((e = cudaStreamSynchronize(c->stream))) return e;
+        ng = total;
+    }
+    c->n_hydro = n;
+    c->n_ext = n + ng;
+    const size_t pt_bytes = D == 2 ? 16 : 32;
+    if ((e = ensure_bytes(c->ext, (size_t)(c->n_ext + 1) * pt_bytes))) return e;
+    ensure<uint32_t>(c->ghost_src, ng + 1, &e);
+    ensure<uint32_t>(c->ghost_code, ng + 1, &e);
+    if (e) return e;
+    if (n > 0) {
+        const uint32_t* off = (const uint32_t*)c->goff.p;
+        if (D == 2)
+            k_ghost_write<2><<<nblk(n, 256), 256, 0, c->stream>>>(
+                pos_dev, n, buff, scale, c->prm.boundary == PGPU_REFLECTIVE, no_ghosts, off, (double2*)c->ext.p,
+                (uint32_t*)c->ghost_src.p, (uint32_t*)c->ghost_code.p);
+        else
+            k_ghost_write<3><<<nblk(n, 256), 256, 0, c->stream>>>(
+                pos_dev, n, buff, scale, c->prm.boundary == PGPU_REFLECTIVE, no_ghosts, off, (double4*)c->ext.p,
+                (uint32_t*)c->ghost_src.p, (uint32_t*)c->ghost_code.p);
+    }
+    c->unit_scale = no_ghosts ? 1.0 : 1. + (2 * buff);
+    return cudaGetLastError();
+}
+
+// Grid resolution: about GRID_PPB points per bin.
+static int grid_resolution(int64_t n, int D) {
+    const double ppb = D == 2 ? 2.0 : 2.0;
+    double g = D == 2 ? sqrt((double)n / ppb) : cbrt((double)n / ppb);
+    int G = (int)(g + 0.5);
+    if (G < 1) G = 1;
+    const int gmax = D == 2 ? 32768 : 1024;
+    return G > gmax ? gmax : G;
+}
+
+cudaError_t launch_grid_sort(pgpu_ctx* c) {
+    const int D = c->prm.dim;
+    const int64_t n = c->n_ext;
+    cudaError_t e = cudaSuccess;
+    int G = grid_resolution(n, D);
+    int64_t P = 1;
+    while (P < G) P <<= 1;
+    int64_t M = D == 2 ? P * P : P * P * P;
+    c->grid_G = G;
+    c->morton_slots = M;
+    uint32_t* cnt = ensure<uint32_t>(c->bin_cnt, M + 1, &e);
+    uint32_t* start = ensure<uint32_t>(c->bin_start, M + 1, &e);
+    uint32_t* key = ensure<uint32_t>(c->bin_key, n + 1, &e);
+    const size_t pt_bytes = D == 2 ? 16 : 32;
+    if (e || (e = ensure_bytes(c->spts, (size_t)(n + 1) * pt_bytes))) return e;
+    uint32_t* perm = ensure<uint32_t>(c->perm, n + 1, &e);
+    uint32_t* inv = ensure<uint32_t>(c->inv, n + 1, &e);
+    if (e) return e;
+    if ((e = cudaMemsetAsync(cnt, 0, (M + 1) * sizeof(uint32_t), c->stream))) return e;
+    if (n > 0) {
+        if (D == 2)
+            k_bin_count<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, G, key, cnt);
+        else
+            k_bin_count<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, G, key, cnt);
+    }
+    if ((e = exclusive_scan_u32(cnt, start, M, c->scan_tmp, c->stream))) return e;
+    if ((e = cudaMemsetAsync(cnt, 0, (M + 1) * sizeof(uint32_t), c->stream))) return e;
+    if (n > 0) {
+        if (D == 2)
+            k_bin_scatter<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, key, start, cnt,
+                                                                  (double2*)c->spts.p, perm, inv);
+        else
+            k_bin_scatter<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, key, start, cnt,
+                                                                  (double4*)c->spts.p, perm, inv);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_query_list(pgpu_ctx* c, bool all_cells) {
+    cudaError_t e = cudaSuccess;
+    const int64_t n = c->n_ext;
+    uint32_t* qs = ensure<uint32_t>(c->qs, n + 1, &e);
+    if (e) return e;
+    c->all_cells = all_cells;
+    if (all_cells || c->n_hydro == n) {
+        c->n_query = n;
+        if (n > 0) k_iota<<<nblk(n, 256), 256, 0, c->stream>>>(qs, n);
+        return cudaGetLastError();
+    }
+    uint32_t* flag = ensure<uint32_t>(c->qflag, n + 1, &e);
+    uint32_t* off = ensure<uint32_t>(c->qoff, n + 1, &e);
+    if (e) return e;
+    k_query_flags<<<nblk(n, 256), 256, 0, c->stream>>>((const uint32_t*)c->perm.p, n, c->n_hydro, flag);
+    if ((e = exclusive_scan_u32(flag, off, n, c->scan_tmp, c->stream))) return e;
+    k_query_compact<<<nblk(n, 256), 256, 0, c->stream>>>(flag, off, n, qs);
+    c->n_query = c->n_hydro;
+    return cudaGetLastError();
+}
+
+}  // namespace pgpu
