@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Benchmark of the per-timestep mesh-and-flux path (one JSON line on stdout).
+
+A step is one full moving-mesh step of the 3D Sedov-Taylor workload
+(1,048,576 uniform points, K = 190, FP64): ghost layer, Morton grid sort, KNN,
+clipping with the security-radius certificate, extraction, CFL time step,
+HLL flux + conserved update + drift.  The metric is hydro cell-updates per
+second (one hydro cell advanced one full step).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun: every rank advances its own replica of the workload
+(weak scaling, no data-path collective); the timed region is bracketed by a
+barrier + synchronize on every rank and the maximum over ranks is reported.
+``--impl reference`` times the reference's own CPU implementation (compiled
+from its sources into oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Voronoi cell-updates/s per B200: learned-K+FP32 vs plain GPU, at matched L1 err"
+UNIT = "cell-updates/s"
+
+# Workloads.  sedov3d_1m is the configuration the metric is quoted on for one GPU
+# (3D Sedov, plain method); the others are smaller cases (profiling, smoke).
+CONFIGS = {
+    "sedov3d_1m": dict(dim=3, n=1_048_576, seed=2, k=190, buff=0.04, boundary="periodic", cfl=0.3),
+    "sedov3d_256k": dict(dim=3, n=262_144, seed=2, k=190, buff=0.04 * 4 ** (1 / 3), boundary="periodic", cfl=0.3),
+    "sod2d_10k": dict(dim=2, n=10_000, seed=1, k=16, buff=0.04, boundary="reflective", cfl=0.3),
+}
+
+# Algorithmic work per unit ("Roofline"): counted with the oracle's
+# instrumented restatement of the reference's search and clipping on the same
+# distributions (3D uniform K=190; 2D jittered lattice K=16).
+#   KNN: candidates per query x flops per squared distance (3D: 8, 2D: 5)
+#   clip: predicates per cell x 45 (det4x4) + vertices created per cell x 59   (3D)
+#         predicates per cell x 14 (det3x3) + vertices created per cell x 11   (2D)
+#   hydro (flux+update+drift): compulsory HBM bytes per cell-update
+WORK = {
+    3: dict(knn_flop_per_query=969.6 * 8, clip_flop_per_cell=924.7 * 45 + 70.8 * 59, hydro_bytes_per_cell=683),
+    2: dict(knn_flop_per_query=73.5 * 5, clip_flop_per_cell=34.3 * 14 + 12.0 * 11, hydro_bytes_per_cell=272),
+}
+STAGES = ["ghosts", "sort", "knn", "clip", "hydro"]
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="sedov3d_1m")
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
+    ap.add_argument("--skip-e2e", action="store_true", help="omit the end-to-end leg")
+    return ap.parse_args()
+
+
+def make_ic(cfg):
+    from proteusgpu_b200 import ics
+    if cfg["dim"] == 3:
+        return ics.sedov_3d(n=cfg["n"], seed=cfg["seed"])
+    return ics.sod_2d(n_side=int(round(cfg["n"] ** 0.5)), seed=cfg["seed"])
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str | None):
+        self.gpu_id, self.proc, self.lines = gpu_id, None, []
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.gpu_id:
+            cmd += ["-i", self.gpu_id]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 6:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[2:6]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU reference
+def cpu_reference_step_rate(steps: int, n_sample: int = 20000, nthreads: int | None = None):
+    """Cell-updates/s of the reference's own CPU code (oracle/_ref, compiled from its sources) on a
+    bounded sample of the 3D Sedov workload: per step compute_periodic_mesh (KNN + clipping + extraction)
+    + dt_CFL + hydro_step; ghost layer widened so that it spans the same number of cells as buff = 0.04
+    does at 1,048,576 points.  Falls back to the C restatement (oracle/liboracle.so) if _ref is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from proteusgpu_b200 import ics
+    nthreads = nthreads or os.cpu_count() or 1
+    ic = ics.sedov_3d(n=n_sample, seed=2)
+    buff = 0.04 * (1_048_576 / n_sample) ** (1 / 3)
+    kind = "reference"
+    try:
+        import refbuild as rb
+        rb.load(3, 190)
+    except (FileNotFoundError, OSError):
+        kind = "port"
+    times = []
+    x = ic.pos.copy()
+    rho, vel, E = ic.rho.copy(), ic.vel.copy(), ic.energy.copy()
+    for s in range(steps):
+        t0 = time.perf_counter()
+        if kind == "reference":
+            m = rb.periodic_mesh(x, 190, buff=buff, gamma=ic.gamma, keep_handle=True, nthreads=nthreads)
+            if s == 0:
+                E = E + ic.deposit / np.where(m.volumes[:n_sample] > 0, m.volumes[:n_sample], 1.0)
+            dt = rb.dt_cfl(3, 190, m.handle, 0.3, rho, vel, E, ic.gamma)
+            rho, vel, E = rb.hydro_step(3, 190, m.handle, dt, rho, vel, E, ic.gamma)
+            rb.free_handle(3, 190, m.handle)
+        else:
+            import oracle as om
+            m = om.build_mesh(x, 190, buff=buff)
+            if s == 0:
+                E = E + ic.deposit / np.where(m.volumes[:n_sample] > 0, m.volumes[:n_sample], 1.0)
+            dt = om.dt_cfl(m, 0.3, ic.gamma, rho, vel, E)
+            rho, vel, E, _ = om.hydro_step_ref(m, dt, ic.gamma, rho, vel, E)
+        times.append(time.perf_counter() - t0)
+    t = float(np.mean(times))
+    sample = (f"3D Sedov, {n_sample} uniform points (seed 2), K=190, buff {buff:.3f}, {steps} step(s) of "
+              "compute_periodic_mesh + dt_CFL + hydro_step")
+    return n_sample / t, kind, nthreads, sample, t
+
+
+# ---------------------------------------------------------------- our arm
+def run_ours(args, rank, world, local_rank):
+    import torch
+    from proteusgpu_b200 import Context, _lib
+    cfg = CONFIGS[args.config]
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    ic = make_ic(cfg)
+    ctx = Context(dim=cfg["dim"], k=cfg["k"], buff=cfg["buff"], boundary=cfg["boundary"], flux="physical",
+                  gamma=ic.gamma, device=local_rank)
+    ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+    for _ in range(max(args.warmup, 0)):
+        ctx.sim_step(cfg["cfl"], want_dt=False)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    L = _lib.load()
+    # per-stage device times (CUDA events on the context's stream), one step, outside the timed region
+    ctx.enable_timing(True)
+    ctx.sim_step(cfg["cfl"], want_dt=False)
+    stage = ctx.stage_times()
+    ctx.enable_timing(False)
+    stats = ctx.stats()
+
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = L.pgpu_launch_count()
+    with ClockSampler(uuid) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.sim_step(cfg["cfl"], want_dt=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = L.pgpu_launch_count() - l0
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        dist.barrier()
+    n = ic.n
+    value = n * args.steps * world / (ms / 1e3)
+
+    # end to end: the same step through the C ABI with the state in pinned host memory,
+    # copied to the device before and back after every step
+    e2e = None
+    if not args.skip_e2e:
+        D = cfg["dim"]
+        x, m_, p_, e_ = ctx.sim_get()
+        hp = [torch.from_numpy(a).pin_memory() for a in (x, m_, p_, e_)]
+        hn = [t.numpy() for t in hp]
+        ke = max(1, min(args.steps, 5))
+        ctx.sim_step_host(cfg["cfl"], 0.0, *hn)  # warm the path
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            ctx.sim_step_host(cfg["cfl"], 0.0, *hn)
+        torch.cuda.synchronize()
+        e_ms = (time.perf_counter() - t0) * 1e3
+        if dist:
+            t = torch.tensor([e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+        nbytes = int(sum(a.nbytes for a in hn))
+        e2e = {"value": n * ke * world / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
+               "d2h_bytes_per_step": nbytes, "steps": ke,
+               "path": "pgpu_sim_step_host (C ABI), pinned host state in/out every step"}
+
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        ctx.close()
+        return None
+
+    # roofline of the dominant stage
+    D = cfg["dim"]
+    W = WORK[D]
+    knn_ms, clip_ms, hydro_ms = stage[2], stage[3], stage[4]
+    dom = STAGES[int(np.argmax(stage))]
+    fp64 = C_double = None
+    import ctypes
+    C_double = ctypes.c_double()
+    L.pgpu_fp64_peak(local_rank, ctypes.c_float(200.0), ctypes.byref(C_double))
+    fp64 = C_double.value
+    hbm, hbm_src = measured_peaks()
+    n_query = stats["n_hydro"]
+    if dom == "knn":
+        ach = n_query * W["knn_flop_per_query"] / (knn_ms * 1e-3) / 1e12
+        roof = {"kernel": "k_knn", "bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
+                "frac": ach / fp64, "traffic": None,
+                "peak_source": "FP64 FMA rate measured in this run (pgpu_fp64_peak)",
+                "work": f"{W['knn_flop_per_query']:.0f} algorithmic flop per query x {n_query} queries"}
+    elif dom == "clip":
+        ach = n_query * W["clip_flop_per_cell"] / (clip_ms * 1e-3) / 1e12
+        roof = {"kernel": "k_clip", "bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
+                "frac": ach / fp64, "traffic": None,
+                "peak_source": "FP64 FMA rate measured in this run (pgpu_fp64_peak)",
+                "work": f"{W['clip_flop_per_cell']:.0f} algorithmic flop per cell x {n_query} cells"}
+    else:
+        ach = n_query * W["hydro_bytes_per_cell"] / (stage[STAGES.index(dom)] * 1e-3) / 1e9
+        roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                "traffic": None, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})"}
+    hyd = n_query * W["hydro_bytes_per_cell"] / (hydro_ms * 1e-3) / 1e9
+    roof_hydro = {"kernel": "k_prim_dt + k_flux_update", "bound": "hbm", "achieved": hyd, "peak": hbm,
+                  "unit": "GB/s", "frac": hyd / hbm, "traffic": None,
+                  "work": f"{W['hydro_bytes_per_cell']} compulsory bytes per cell-update"}
+
+    cpu = None
+    if not args.skip_cpu and world == 1:
+        v, kind, cores, sample, t_step = cpu_reference_step_rate(steps=2)
+        cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
+               "s_per_step": t_step}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.config}: 3D Sedov-Taylor blast, {cfg['n']} uniform points (seed "
+                               f"{cfg['seed']}), K={cfg['k']}, plain FP64 method, moving mesh, "
+                               f"{cfg['boundary']} box" if D == 3 else args.config,
+                   "n_points": cfg["n"], "k": cfg["k"], "buff": cfg["buff"], "form": "plain",
+                   "flux": "physical (outward normal, pair-symmetric area)",
+                   "l2": "inputs larger than L2: per-step KNN lists alone are "
+                         f"{stats['n_hydro'] * cfg['k'] * 4 / 2 ** 20:.0f} MiB",
+                   "parallelism": f"replicas x{world}"},
+        "roofline": roof, "roofline_hydro": roof_hydro,
+        "stages_ms": dict(zip(STAGES, stage)),
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "mesh": {"n_ext": stats["n_ext"], "faces": stats["num_faces"], "cert_k_max": stats["cert_k_max"],
+                 "failed_cells": stats["failed_cells"], "knn_candidates_per_query":
+                     stats["knn_candidates"] / max(stats["n_hydro"], 1)},
+    }
+    ctx.close()
+    return out
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return None
+    steps, warm = max(args.steps, 1), max(args.warmup, 0)
+    v_all = []
+    kind = cores = sample = None
+    if warm:
+        cpu_reference_step_rate(steps=1)
+    for _ in range(steps):
+        v, kind, cores, sample, _t = cpu_reference_step_rate(steps=1)
+        v_all.append(v)
+    v = float(np.mean(v_all))
+    cfg = CONFIGS[args.config]
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": warm, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"{args.config} (bounded sample on the host cores)", "n_points": cfg["n"],
+                       "k": cfg["k"]},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        out = run_reference(args, rank)
+    else:
+        out = run_ours(args, rank, world, local_rank)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -46,6 +46,11 @@ extern "C" {
 #define PGPU_FLUX_REFERENCE 0 /* stored (inward) normal, each cell's own face area: riemann.cpp:7-45 as is */
 #define PGPU_FLUX_PHYSICAL 1  /* outward normal, face-pair-symmetric area: conservative to round-off */
 
+/* plane-vertex predicate near zero (|det| below the reference's error bound, cell.cpp:187-218) */
+#define PGPU_PRED_REFERENCE 0 /* as the reference: the cell fails with NEEDS_EXACT_PREDICATES */
+#define PGPU_PRED_ROBUST 1    /* the vertex is kept (treated as not cut); needed for mirror walls,
+                                 whose symmetric point sets make exact degeneracies */
+
 /* cell status codes: the reference's Status enum, src/global/allvars.h:13-20 */
 #define PGPU_TRIANGLE_OVERFLOW 0
 #define PGPU_VERTEX_OVERFLOW 1
@@ -66,6 +71,9 @@ typedef struct {
     double gamma;     /* adiabatic index, the reference's global `_gamma_` (allvars.cpp:14) */
     int device;       /* CUDA device ordinal */
     int verbose;      /* 0 = silent */
+    int predicates;   /* PGPU_PRED_REFERENCE or PGPU_PRED_ROBUST */
+    int k_fallback;   /* moving-mesh steps only: hydro cells whose certificate does not close
+                         within k neighbours are recomputed with this budget (0 = off; k < k_fallback <= 256) */
 } pgpu_params;
 
 /* Fills p with the reference's defaults: dim 3, K 190, periodic, reference flux,
@@ -169,6 +177,8 @@ typedef struct {
     double total_mass, total_energy, total_mom[3]; /* deterministic sums over hydro cells */
     int32_t cert_k_max;
     int32_t n_grid;
+    int64_t refit_cells;        /* cells recomputed with k_fallback in the last step */
+    int64_t uncertified_cells;  /* hydro cells still without a certificate after it */
 } pgpu_stats;
 
 /* Statistics of the last step (synchronises the stream). */
@@ -182,6 +192,21 @@ int pgpu_stage_times(pgpu_ctx *ctx, float *ms5);
 /* The CUDA stream of the context (a cudaStream_t), for callers that time or
  * order work around it. */
 void *pgpu_stream(pgpu_ctx *ctx);
+
+/* hydro::riemann_hll (src/hydro/riemann.cpp:7-45) for one face, on the host,
+ * with the same arithmetic as the device kernels: L and R are (rho, vx, vy, vz, E)
+ * (vz ignored in 2D), normal is the face normal as stored (3 doubles), flux
+ * receives (rho, mx, my, mz, E) in the lab frame. */
+int pgpu_riemann_hll(int dim, double gamma, const double *L, const double *R, const double *normal, double *flux);
+
+/* Number of kernels launched by this library in this process so far (diagnostics). */
+int64_t pgpu_launch_count(void);
+
+/* Diagnostics, no reference counterpart: runs a dependent-chain FP64 FMA
+ * kernel on the device for about `ms` milliseconds and returns the achieved
+ * FP64 rate in TFLOP/s (the FP64 pipe peak that the KNN and clipping kernels
+ * are measured against). */
+int pgpu_fp64_peak(int device, float ms, double *tflops);
 
 #ifdef __cplusplus
 }

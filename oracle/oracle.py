@@ -70,6 +70,10 @@ def lib():
         L.om_symmetric_area.argtypes = [C.POINTER(_Mesh), _dp]
         L.om_symmetric_area.restype = C.c_long
         L.om_num_regions.argtypes = [C.c_int]
+        L.om_get_counters.argtypes = [_lp]
+        L.om_set_predicate_mode.argtypes = [C.c_int]
+        L.om_set_fallback_k.argtypes = [C.c_int]
+        L.om_set_boundary_mode.argtypes = [C.c_int]
         _LIB = L
     return _LIB
 
@@ -111,8 +115,8 @@ class Mesh:
 
 
 def _arr(ptr, n, dtype):
-    if n <= 0:
-        return np.zeros(0, dtype)
+    if n <= 0 or not ptr:
+        return np.zeros(max(n, 0), dtype)
     return np.ctypeslib.as_array(ptr, shape=(n,)).astype(dtype, copy=True)
 
 
@@ -156,10 +160,18 @@ def cells(ext_unit: np.ndarray, n_hydro: int, knn_lists: np.ndarray, n_compute: 
 
 
 def build_mesh(pts: np.ndarray, k: int, buff: float = 0.04, boundary: int = PERIODIC,
-               hydro_only: bool = False) -> Mesh:
+               hydro_only: bool = False, robust: bool = False, k_fallback: int = 0) -> Mesh:
+    """The whole mesh build.  robust / k_fallback: the moving-mesh extensions (om.h)."""
     pts = np.ascontiguousarray(pts, np.float64)
     m = _Mesh()
-    lib().om_build_mesh(pts.shape[1], boundary, buff, k, pts.ravel(), len(pts), int(hydro_only), C.byref(m))
+    L = lib()
+    L.om_set_predicate_mode(1 if robust else 0)
+    L.om_set_fallback_k(k_fallback)
+    try:
+        L.om_build_mesh(pts.shape[1], boundary, buff, k, pts.ravel(), len(pts), int(hydro_only), C.byref(m))
+    finally:
+        L.om_set_predicate_mode(0)
+        L.om_set_fallback_k(0)
     return _wrap(m)
 
 
@@ -181,6 +193,17 @@ def symmetric_area(mesh: Mesh):
     out = np.zeros(max(mesh.num_faces, 1))
     unp = lib().om_symmetric_area(C.byref(mesh._c), out)
     return out[: mesh.num_faces], unp
+
+
+def reset_counters():
+    lib().om_reset_counters()
+
+
+def counters() -> dict:
+    """Work counters since the last reset: KNN candidates, clip predicates, vertices created, cells."""
+    out = np.zeros(4, np.int64)
+    lib().om_get_counters(out)
+    return dict(zip(("knn_candidates", "predicates", "new_vertices", "cells"), out.tolist()))
 
 
 def prim_to_cons(mesh: Mesh, rho, vel, energy, deposit=None):

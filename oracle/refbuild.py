@@ -26,12 +26,28 @@ _up = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _LIBS: dict = {}
 
 
-def lib_path(dim: int, k: int) -> str:
-    return os.path.join(REF_DIR, f"libref_{dim}d_k{k}.so")
+# Libraries with the same extern "C" surface: the reference build (oracle/_ref) and
+# the drop-in translation units linked with the same driver (proteusgpu_b200/dropin).
+DROPIN_DIR = os.path.join(os.path.dirname(HERE), "proteusgpu_b200", "dropin", "_build")
+_PREFIX = {"ref": (REF_DIR, "libref"), "dropin": (DROPIN_DIR, "libdropin")}
+_FLAVOR = "ref"
 
 
-def available(dim: int, k: int) -> bool:
-    return os.path.exists(lib_path(dim, k))
+def use(flavor: str):
+    """Selects which library the functions below call: "ref" (the reference build) or
+    "dropin" (the drop-in units over the GPU path).  Returns the previous choice."""
+    global _FLAVOR
+    prev, _FLAVOR = _FLAVOR, flavor
+    return prev
+
+
+def lib_path(dim: int, k: int, flavor: str | None = None) -> str:
+    d, p = _PREFIX[flavor or _FLAVOR]
+    return os.path.join(d, f"{p}_{dim}d_k{k}.so")
+
+
+def available(dim: int, k: int, flavor: str | None = None) -> bool:
+    return os.path.exists(lib_path(dim, k, flavor))
 
 
 def _bind(lib):
@@ -59,13 +75,13 @@ def _bind(lib):
 
 
 def load(dim: int, k: int):
-    key = (dim, k)
-    if key not in _LIBS:
-        path = lib_path(dim, k)
+    path = lib_path(dim, k)
+    if path not in _LIBS:
         if not os.path.exists(path):
-            raise FileNotFoundError(f"reference build {path} missing (run `make -C oracle ref`)")
-        _LIBS[key] = _bind(C.CDLL(path, mode=os.RTLD_LOCAL))
-    return _LIBS[key]
+            raise FileNotFoundError(f"library {path} missing (run `make -C oracle ref` or "
+                                    "`make -C proteusgpu_b200/dropin`)")
+        _LIBS[path] = _bind(C.CDLL(path, mode=os.RTLD_LOCAL))
+    return _LIBS[path]
 
 
 @dataclass

@@ -87,6 +87,12 @@ void om_region_shift(int dim, int r, int *shift3);
 long om_ghosts(int dim, int boundary, double buff, const double *pts, long n,
                double *ext, long *ghost_src, int *ghost_code);
 
+/* ---- work counters (instrumentation for the roofline's algorithmic counts) ----
+ * [0] KNN candidate distance evaluations, [1] clip plane-vertex predicates,
+ * [2] vertices created, [3] cells clipped. */
+void om_reset_counters(void);
+void om_get_counters(long *out4);
+
 /* ---- KNN --------------------------------------------------------------- */
 
 /* Exact K nearest neighbours of every point of `pts` (n x dim, unit box),
@@ -110,6 +116,19 @@ int om_build_mesh(int dim, int boundary, double buff, int K, const double *pts, 
                   int hydro_only, om_mesh *mesh);
 
 void om_mesh_free(om_mesh *mesh);
+
+/* Test hook: 0 = the reference's boundary walk (default), 1 = the set-based
+ * cavity boundary that the CUDA kernel uses. */
+void om_set_boundary_mode(int mode);
+
+/* Extensions used by the moving-mesh workloads (both default to the reference's
+ * behaviour, 0):
+ *   predicate mode 1 keeps a vertex whose plane predicate is within the
+ *   reference's error bound of zero instead of failing the cell;
+ *   fallback K > K recomputes, in hydro-only builds, the hydro cells whose
+ *   certificate did not close within K with the larger budget. */
+void om_set_predicate_mode(int mode);
+void om_set_fallback_k(int k);
 
 /* ---- hydro ------------------------------------------------------------- */
 

@@ -21,6 +21,14 @@
 
 #define END_OF_LIST 255
 
+/* Predicate mode (extension): 0 = the reference's (a near-zero determinant
+ * fails the cell), 1 = robust (the vertex is kept, i.e. not cut, and a vertex
+ * with w = 0 blocks the security-radius certificate). */
+int om_predicate_mode = 0;
+void om_set_predicate_mode(int m) { om_predicate_mode = m; }
+
+extern long om_counters_g[4];
+
 typedef struct {
     int dim;
     const double *pts;
@@ -32,6 +40,7 @@ typedef struct {
     int vid[OM_MAX_P];
     unsigned char tri[OM_MAX_T][3];
     unsigned char bnext[OM_MAX_P];
+    long n_pred, n_newv;
 } cell_t;
 
 /* ---- the reference's determinant expansions (allvars.h:168-195) ---- */
@@ -132,7 +141,12 @@ static int security_reached(const cell_t *c, const double *nb) {
         vertex_point(c, c->tri[i], pc);
         for (int k = 0; k < 4; k++) d[k] = pc[k] - c->seed[k];
         double d2 = dot3(d, d);
-        v_dist = (d2 < v_dist) ? v_dist : d2; /* std::max(d2, v_dist) */
+        if (om_predicate_mode == 1) {
+            /* robust mode: a vertex without a position (w = 0) blocks the certificate */
+            v_dist = (d2 != d2 || v_dist != v_dist) ? d2 + v_dist : (d2 > v_dist ? d2 : v_dist);
+        } else {
+            v_dist = (d2 < v_dist) ? v_dist : d2; /* std::max(d2, v_dist) */
+        }
     }
     double d[4];
     for (int k = 0; k < 4; k++) d[k] = nb[k] - c->seed[k];
@@ -162,7 +176,10 @@ static int in_conflict(cell_t *c, const unsigned char *v, const double *e) {
         double max_max = fmax3(maxx, maxy, maxz);
         eps *= (max_max * max_max);
     }
-    if (fabs(det) < eps) c->status = OM_NEEDS_EXACT_PREDICATES;
+    if (fabs(det) < eps) {
+        if (om_predicate_mode == 1) return 0;
+        c->status = OM_NEEDS_EXACT_PREDICATES;
+    }
     return det > 0.0;
 }
 
@@ -237,6 +254,48 @@ static void boundary_3d(cell_t *c) {
     }
 }
 
+/* Alternative cavity boundary used to cross-check the CUDA kernel's method
+ * (not the reference's): the boundary is the set of directed edges x -> y of
+ * removed vertices whose reverse edge belongs to no removed vertex; it must form
+ * one cycle.  Selected by om_set_boundary_mode(1). */
+int om_boundary_mode = 0;
+void om_set_boundary_mode(int m) { om_boundary_mode = m; }
+
+static void boundary_3d_set(cell_t *c) {
+    unsigned long long em[OM_MAX_P];
+    memset(em, 0, sizeof(em));
+    for (int i = 0; i < OM_MAX_P; i++) c->bnext[i] = END_OF_LIST;
+    c->first = END_OF_LIST;
+    for (int r = 0; r < c->nb_r; r++) {
+        unsigned char *T = c->tri[c->nb_t + r];
+        for (int e = 0; e < 3; e++) em[T[e]] |= 1ull << T[(e + 1) % 3];
+    }
+    unsigned long long src = 0;
+    int n = 0;
+    for (int r = 0; r < c->nb_r; r++) {
+        unsigned char *T = c->tri[c->nb_t + r];
+        for (int e = 0; e < 3; e++) {
+            int x = T[e], y = T[(e + 1) % 3];
+            if (!((em[y] >> x) & 1ull)) {
+                if ((src >> x) & 1ull) { c->status = OM_INCONSISTENT_BOUNDARY; return; }
+                src |= 1ull << x;
+                c->bnext[x] = (unsigned char)y;
+                n++;
+            }
+        }
+    }
+    if (n < 3) { c->status = OM_INCONSISTENT_BOUNDARY; return; }
+    int x0 = __builtin_ctzll(src), x = x0;
+    for (int st = 1; st <= n; st++) {
+        x = c->bnext[x];
+        if (!((src >> x) & 1ull) || (x == x0 && st < n)) { c->status = OM_INCONSISTENT_BOUNDARY; return; }
+    }
+    if (x != x0) { c->status = OM_INCONSISTENT_BOUNDARY; return; }
+    c->first = x0;
+    c->nb_t += 0;
+    c->nb_r = 0;
+}
+
 /* new_vertex (cell.cpp:346-364) */
 static void new_vertex(cell_t *c, int i, int j, int k) {
     if (c->nb_t + 1 >= OM_MAX_T) {
@@ -259,6 +318,7 @@ static void new_vertex(cell_t *c, int i, int j, int k) {
         c->tri[c->nb_t][2] = (unsigned char)k;
     }
     c->nb_t++;
+    c->n_newv++;
 }
 
 /* clip_by_plane + new_halfplane (cell.cpp:110-172) */
@@ -280,6 +340,7 @@ static void clip(cell_t *c, long vid) {
     c->nb_v++;
 
     const double *eqn = c->hp[cur];
+    c->n_pred += c->nb_t;
     c->nb_r = 0;
     int i = 0;
     while (i < c->nb_t) {
@@ -301,6 +362,8 @@ static void clip(cell_t *c, long vid) {
     }
     if (c->dim == 2)
         boundary_2d(c);
+    else if (om_boundary_mode == 1)
+        boundary_3d_set(c);
     else
         boundary_3d(c);
     if (c->status != OM_SUCCESS) return;
@@ -483,6 +546,7 @@ static void one_cell(int dim, const double *ext, long i, const uint32_t *knn, in
                      int *cert_k) {
     cell_t c;
     cell_init(&c, dim, ext, i);
+    c.n_pred = c.n_newv = 0;
     *cert_k = 0;
     for (int v = 0; v < K; v++) {
         uint32_t z = knn[(long)K * i + v];
@@ -505,6 +569,12 @@ static void one_cell(int dim, const double *ext, long i, const uint32_t *knn, in
         if (!security_reached(&c, nb)) c.status = OM_SECURITY_RADIUS_NOT_REACHED;
     }
     *status = c.status;
+#pragma omp atomic
+    om_counters_g[1] += c.n_pred;
+#pragma omp atomic
+    om_counters_g[2] += c.n_newv;
+#pragma omp atomic
+    om_counters_g[3] += 1;
     o->nf = 0;
     o->volume = 0;
     o->centroid[0] = o->centroid[1] = o->centroid[2] = 0;
@@ -592,6 +662,53 @@ void om_mesh_free(om_mesh *m) {
     memset(m, 0, sizeof(*m));
 }
 
+int om_fallback_k = 0;
+void om_set_fallback_k(int k) { om_fallback_k = k; }
+
+/* m <- per cell: b's result where m's hydro cell was SECURITY_RADIUS_NOT_REACHED, else m's */
+static void merge_refit(om_mesh *m, const om_mesh *b, long n_hydro) {
+    long F = 0;
+    for (long i = 0; i < m->n_seeds; i++) {
+        const om_mesh *s = (i < n_hydro && m->status[i] == OM_SECURITY_RADIUS_NOT_REACHED) ? b : m;
+        F += s->face_counts[i];
+    }
+    int *nb = (int *)malloc((F + 1) * sizeof(int));
+    double *nr = (double *)malloc((F + 1) * 3 * sizeof(double));
+    double *ar = (double *)malloc((F + 1) * sizeof(double));
+    long *fp = (long *)malloc((m->n_seeds + 1) * sizeof(long));
+    long *fc = (long *)malloc((m->n_seeds + 1) * sizeof(long));
+    long f = 0;
+    for (long i = 0; i < m->n_seeds; i++) {
+        const int use_b = i < n_hydro && m->status[i] == OM_SECURITY_RADIUS_NOT_REACHED;
+        const om_mesh *s = use_b ? b : m;
+        fp[i] = f;
+        fc[i] = s->face_counts[i];
+        for (long q = 0; q < s->face_counts[i]; q++, f++) {
+            long g = s->face_ptr[i] + q;
+            nb[f] = s->neighbor[g];
+            for (int k = 0; k < 3; k++) nr[3 * f + k] = s->normal[3 * g + k];
+            ar[f] = s->area[g];
+        }
+        if (use_b) {
+            m->volumes[i] = b->volumes[i];
+            m->status[i] = b->status[i];
+            m->cert_k[i] = b->cert_k[i];
+            for (int k = 0; k < 3; k++) m->centroid[3 * i + k] = b->centroid[3 * i + k], m->seeds[3 * i + k] = b->seeds[3 * i + k];
+        }
+    }
+    free(m->neighbor);
+    free(m->normal);
+    free(m->area);
+    free(m->face_ptr);
+    free(m->face_counts);
+    m->neighbor = nb;
+    m->normal = nr;
+    m->area = ar;
+    m->face_ptr = fp;
+    m->face_counts = fc;
+    m->num_faces = F;
+}
+
 int om_build_mesh(int dim, int boundary, double buff, int K, const double *pts, long n, int hydro_only,
                   om_mesh *m) {
     const int nreg = om_num_regions(dim);
@@ -603,6 +720,22 @@ int om_build_mesh(int dim, int boundary, double buff, int K, const double *pts, 
     om_knn(dim, ext, ntot, K, knn);
     om_cells(dim, ext, ntot, n, knn, K, hydro_only ? n : ntot, m);
     free(knn);
+    if (hydro_only && om_fallback_k > K) {
+        /* extension: hydro cells whose certificate did not close within K are
+           recomputed with the fallback budget (the other cells keep their K result) */
+        long nunc = 0;
+        for (long i = 0; i < n; i++) nunc += m->status[i] == OM_SECURITY_RADIUS_NOT_REACHED;
+        if (nunc) {
+            const int K2 = om_fallback_k;
+            uint32_t *knn2 = (uint32_t *)malloc((size_t)ntot * K2 * sizeof(uint32_t));
+            om_knn(dim, ext, ntot, K2, knn2);
+            om_mesh b;
+            om_cells(dim, ext, ntot, n, knn2, K2, n, &b);
+            free(knn2);
+            merge_refit(m, &b, n);
+            om_mesh_free(&b);
+        }
+    }
     free(ext);
     m->ghost_ids = (long *)malloc((ntot - n + 1) * sizeof(long));
     m->ghost_code = (int *)malloc((ntot - n + 1) * sizeof(int));

@@ -26,6 +26,16 @@
 #include <stdlib.h>
 #include <string.h>
 
+long om_counters_g[4];  /* see om_get_counters */
+
+void om_reset_counters(void) {
+    for (int i = 0; i < 4; i++) om_counters_g[i] = 0;
+}
+
+void om_get_counters(long *out4) {
+    for (int i = 0; i < 4; i++) out4[i] = om_counters_g[i];
+}
+
 static int n_grid_for(long n, int dim) {
     int g = (int)round(pow((double)(n / 3.1f), (double)(1.0f / (float)dim)));
     return g < 1 ? 1 : g;
@@ -84,7 +94,8 @@ int om_knn(int dim, const double *pts, long n, int K, uint32_t *out) {
         free(fill);
     }
 
-#pragma omp parallel
+    long total_cand = 0;
+#pragma omp parallel reduction(+ : total_cand)
     {
         double *bd = (double *)malloc(K * sizeof(double));
         uint32_t *bi = (uint32_t *)malloc(K * sizeof(uint32_t));
@@ -116,6 +127,7 @@ int om_knn(int dim, const double *pts, long n, int K, uint32_t *out) {
                             for (long s = start[b]; s < start[b + 1]; s++) {
                                 long j = order[s];
                                 if (j == q) continue;
+                                total_cand++;
                                 topk_insert(bd, bi, &cnt, K, dist2(p, pts + j * dim, dim), (uint32_t)j);
                             }
                         }
@@ -127,6 +139,7 @@ int om_knn(int dim, const double *pts, long n, int K, uint32_t *out) {
         free(bd);
         free(bi);
     }
+    om_counters_g[0] += total_cand;
     free(start);
     free(order);
     free(bin);

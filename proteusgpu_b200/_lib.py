@@ -24,12 +24,14 @@ EXPORTED = [
     "pgpu_mesh_sizes", "pgpu_upload_mesh", "pgpu_set_prim", "pgpu_get_prim", "pgpu_dt_cfl",
     "pgpu_hydro_step", "pgpu_sim_init", "pgpu_sim_step", "pgpu_sim_step_host", "pgpu_sim_get",
     "pgpu_sim_set", "pgpu_sim_stats", "pgpu_enable_timing", "pgpu_stage_times", "pgpu_stream",
+    "pgpu_launch_count", "pgpu_fp64_peak", "pgpu_riemann_hll",
 ]
 
 
 class Params(C.Structure):
     _fields_ = [("dim", C.c_int), ("k", C.c_int), ("boundary", C.c_int), ("flux_mode", C.c_int),
-                ("buff", C.c_double), ("gamma", C.c_double), ("device", C.c_int), ("verbose", C.c_int)]
+                ("buff", C.c_double), ("gamma", C.c_double), ("device", C.c_int), ("verbose", C.c_int),
+                ("predicates", C.c_int), ("k_fallback", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -37,7 +39,7 @@ class Stats(C.Structure):
                 ("failed_cells", C.c_int64), ("box_faces", C.c_int64), ("unpaired_faces", C.c_int64),
                 ("knn_candidates", C.c_int64), ("last_dt", C.c_double), ("total_mass", C.c_double),
                 ("total_energy", C.c_double), ("total_mom", C.c_double * 3), ("cert_k_max", C.c_int32),
-                ("n_grid", C.c_int32)]
+                ("n_grid", C.c_int32), ("refit_cells", C.c_int64), ("uncertified_cells", C.c_int64)]
 
 
 _LIB = None
@@ -84,6 +86,9 @@ def load(path: str = LIB_PATH):
     L.pgpu_stage_times.argtypes = [vp, vp]
     L.pgpu_stream.argtypes = [vp]
     L.pgpu_stream.restype = vp
+    L.pgpu_launch_count.restype = C.c_int64
+    L.pgpu_fp64_peak.argtypes = [C.c_int, C.c_float, vp]
+    L.pgpu_riemann_hll.argtypes = [C.c_int, dbl, vp, vp, vp, vp]
     for name in EXPORTED:
         getattr(L, name)  # raises AttributeError if a declared symbol is missing
     _LIB = L

@@ -18,7 +18,7 @@ OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libproteus_gpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # per-file extra flags; files not listed get the FP64 parity flags
-FAST_MATH_FILES: set[str] = set()
+FAST_MATH_FILES: set[str] = {"diag.cu"}
 
 
 def nvcc() -> str:

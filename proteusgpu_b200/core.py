@@ -58,16 +58,22 @@ class Context:
     dim, k: the reference's compile-time dimension and _K_ (Config.sh:4-34),
     here runtime parameters.  boundary: "periodic" (reference) or "reflective".
     flux: "reference" (stored inward normal, own face area, as riemann.cpp) or
-    "physical" (outward normal, face-pair-symmetric area)."""
+    "physical" (outward normal, face-pair-symmetric area).  predicates:
+    "reference" (a near-degenerate predicate fails the cell, cell.cpp:216-218) or
+    "robust" (the vertex is kept).  k_fallback: moving-mesh steps recompute cells
+    whose certificate does not close within k neighbours with this budget."""
 
     def __init__(self, dim: int = 3, k: int = 190, boundary: str = "periodic", flux: str = "reference",
-                 buff: float = 0.04, gamma: float = 5.0 / 3.0, device: int = 0):
+                 buff: float = 0.04, gamma: float = 5.0 / 3.0, device: int = 0, predicates: str = "reference",
+                 k_fallback: int = 0):
         L = _lib.load()
         p = _lib.Params()
         L.pgpu_default_params(C.byref(p))
         p.dim, p.k, p.buff, p.gamma, p.device = dim, k, buff, gamma, device
         p.boundary = {"periodic": 0, "reflective": 1}[boundary]
         p.flux_mode = {"reference": 0, "physical": 1}[flux]
+        p.predicates = {"reference": 0, "robust": 1}[predicates]
+        p.k_fallback = k_fallback
         h = C.c_void_p()
         rc = L.pgpu_create(C.byref(p), C.byref(h))
         if rc != 0:

@@ -1,5 +1,6 @@
 // The C ABI (include/proteus_gpu.h): argument checks, device memory, the order
 // of the stage launches, and host transfers.  No computation happens here.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -13,6 +14,9 @@ using pgpu::DevScalars;
 using pgpu::ensure;
 
 namespace pgpu {
+
+static std::atomic<long long> g_launches{0};
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 cudaError_t ensure_bytes(DevBuf& b, size_t bytes) {
     if (b.p && b.bytes >= bytes) return cudaSuccess;
@@ -92,6 +96,10 @@ int build_mesh(pgpu_ctx* c, int64_t n, bool no_ghosts, bool all_cells) {
     CK(pgpu::launch_knn(c));
     mark(c, 3);
     CK(pgpu::launch_clip(c));
+    if (!all_cells && c->prm.k_fallback > c->prm.k && c->n_uncertified > 0) {
+        // cells whose certificate did not close within k: KNN and clipping again with the fallback budget
+        CK(pgpu::launch_fallback(c));
+    }
     mark(c, 4);
     c->have_mesh = true;
     c->mesh_uploaded = false;
@@ -131,6 +139,8 @@ int pgpu_create(const pgpu_params* p, pgpu_ctx** out) {
     if (!(p->gamma > 1.0)) return PGPU_EINVAL;
     if (p->boundary != PGPU_PERIODIC && p->boundary != PGPU_REFLECTIVE) return PGPU_EINVAL;
     if (p->flux_mode != PGPU_FLUX_REFERENCE && p->flux_mode != PGPU_FLUX_PHYSICAL) return PGPU_EINVAL;
+    if (p->predicates != PGPU_PRED_REFERENCE && p->predicates != PGPU_PRED_ROBUST) return PGPU_EINVAL;
+    if (p->k_fallback != 0 && (p->k_fallback <= p->k || p->k_fallback > pgpu::MAX_K)) return PGPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return PGPU_ECUDA;
     if (p->device < 0 || p->device >= ndev) return PGPU_EINVAL;
@@ -156,7 +166,7 @@ void pgpu_destroy(pgpu_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->prm.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf* bufs[] = {&c->pos,   &c->ext,     &c->gcnt,     &c->goff,   &c->ghost_src, &c->ghost_code, &c->bin_cnt,
+    DevBuf* bufs[] = {&c->fb_qs, &c->fb_knn, &c->pos,   &c->ext,     &c->gcnt,     &c->goff,   &c->ghost_src, &c->ghost_code, &c->bin_cnt,
                       &c->bin_start, &c->bin_key, &c->spts, &c->perm,  &c->inv,       &c->qflag,      &c->qoff,
                       &c->qs,    &c->knn,     &c->vol,      &c->fptr,   &c->fcnt,      &c->status,     &c->certk,
                       &c->centroid, &c->f_nb, &c->f_own,    &c->f_geo,  &c->scan_tmp,  &c->scalars,    &c->rho,
@@ -173,6 +183,22 @@ void pgpu_destroy(pgpu_ctx* c) {
 const char* pgpu_last_error(const pgpu_ctx* c) { return c ? c->err.c_str() : "null context"; }
 
 void* pgpu_stream(pgpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int64_t pgpu_launch_count(void) { return (int64_t)pgpu::g_launches.load(); }
+
+int pgpu_riemann_hll(int dim, double gamma, const double* L, const double* R, const double* normal, double* flux) {
+    if ((dim != 2 && dim != 3) || !L || !R || !normal || !flux) return PGPU_EINVAL;
+    const pgpu::Prim l = {L[0], L[1], L[2], dim == 3 ? L[3] : 0.0, L[4]};
+    const pgpu::Prim r = {R[0], R[1], R[2], dim == 3 ? R[3] : 0.0, R[4]};
+    const pgpu::Flux f = dim == 2 ? pgpu::hll<2>(l, r, normal[0], normal[1], normal[2], gamma)
+                                  : pgpu::hll<3>(l, r, normal[0], normal[1], normal[2], gamma);
+    flux[0] = f.rho;
+    flux[1] = f.mx;
+    flux[2] = f.my;
+    flux[3] = f.mz;
+    flux[4] = f.E;
+    return PGPU_OK;
+}
 
 int pgpu_enable_timing(pgpu_ctx* c, int on) {
     if (!c) return PGPU_EINVAL;
@@ -555,6 +581,8 @@ int pgpu_sim_stats(pgpu_ctx* c, pgpu_stats* out) {
     out->total_energy = h.sums[4];
     out->cert_k_max = h.cert_k_max;
     out->n_grid = c->grid_G;
+    out->refit_cells = c->n_refit;
+    out->uncertified_cells = c->n_uncertified;
     return PGPU_OK;
 }
 

@@ -96,9 +96,11 @@ __device__ __forceinline__ double fmax3(double a, double b, double c) {
     return m > c ? m : c;
 }
 
-// vert_is_in_conflict (cell.cpp:175-221): returns det > 0, sets *near when |det| < eps
+// vert_is_in_conflict (cell.cpp:175-221): returns det > 0, sets *near when |det| < eps.
+// In robust mode a near-zero determinant keeps the vertex (not cut) instead.
 template <int D>
-__device__ __forceinline__ bool in_conflict(const double4* hp, uint32_t t, const double4& e, bool* near) {
+__device__ __forceinline__ bool in_conflict(const double4* hp, uint32_t t, const double4& e, bool* near,
+                                            bool robust) {
     const double4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)];
     double det, eps;
     if (D == 2) {
@@ -119,24 +121,31 @@ __device__ __forceinline__ bool in_conflict(const double4* hp, uint32_t t, const
         double max_max = fmax3(maxx, maxy, maxz);
         eps *= (max_max * max_max);
     }
-    if (fabs(det) < eps) *near = true;
+    if (fabs(det) < eps) {
+        if (robust) return false;
+        *near = true;
+    }
     return det > 0.0;
 }
 
+// Maximum that propagates NaN: a vertex with w = 0 (three planes sharing a line,
+// which mirror-symmetric point sets produce) has no position, and a cell holding
+// one must not pass the certificate.  The reference's running std::max
+// (cell.cpp:377) keeps or drops such a NaN depending on vertex order.
+__device__ __forceinline__ double nan_max(double a, double b) { return (a != a || b != b) ? (a + b) : fmax(a, b); }
+
 __device__ __forceinline__ double warp_max(double v) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(FULL, v, o));
+    for (int o = 16; o > 0; o >>= 1) v = nan_max(v, __shfl_xor_sync(FULL, v, o));
     return v;
 }
 
-// std::max semantics of the reference's running maximum are irrelevant here:
-// squared distances are finite and non-negative.
 __device__ __forceinline__ double max_vd2(const WarpCell& W, int n, int lane, const uint32_t* keep_mask) {
     double m = 0.0;
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         int i = lane + 32 * j;
-        if (i < n && (keep_mask == nullptr || ((keep_mask[j] >> lane) & 1u))) m = fmax(m, W.vd2[i]);
+        if (i < n && (keep_mask == nullptr || ((keep_mask[j] >> lane) & 1u))) m = nan_max(m, W.vd2[i]);
     }
     return warp_max(m);
 }
@@ -152,6 +161,8 @@ struct ClipParams {
     int64_t nq;
     int64_t n_hydro;
     int K;
+    int robust;
+    unsigned int* uncertified;  // hydro cells ending with SECURITY_RADIUS_NOT_REACHED
     double vscale, ascale, scale;  // unit box -> physical
     double* vol;
     uint32_t* fptr;
@@ -255,7 +266,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
         for (int j = 0; j < 3; j++) {
             int i = lane + 32 * j;
             bool cf = false;
-            if (i < nb_t) cf = in_conflict<D>(W.hp, W.tri[i], eq, &near);
+            if (i < nb_t) cf = in_conflict<D>(W.hp, W.tri[i], eq, &near, P.robust);
             cm[j] = __ballot_sync(FULL, cf);
         }
         const int nb_r = __popc(cm[0]) + __popc(cm[1]) + __popc(cm[2]);
@@ -396,11 +407,11 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
             double x, y, zz;
             vertex_pos<D>(W.hp, my_new[q], x, y, zz);
             nd2[q] = seed_d2(x, y, zz, sx, sy, sz);
-            newmax = fmax(newmax, nd2[q]);
+            newmax = nan_max(newmax, nd2[q]);
         }
         if (kept + n_new >= MAX_T) {  // new_vertex overflow (cell.cpp:347-350)
             status = ST_TRIANGLE_OVERFLOW;
-            fail_vdist = fmax(max_vd2(W, nb_t, lane, km), warp_max(newmax));
+            fail_vdist = nan_max(max_vd2(W, nb_t, lane, km), warp_max(newmax));
             break;
         }
         // compaction: kept vertices in order, then the new ones
@@ -454,6 +465,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
     }
     if (status != ST_SUCCESS) {
         if (lane == 0) {
+            if (status == ST_SECURITY_RADIUS_NOT_REACHED && (int64_t)e < P.n_hydro) atomicAdd(P.uncertified, 1u);
             P.vol[e] = 0.0;
             P.fptr[e] = 0;
             P.fcnt[e] = 0;
@@ -679,6 +691,88 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
 
 }  // namespace
 
+namespace {
+
+inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
+
+__global__ void k_mark_not_computed(int* __restrict__ status, int* __restrict__ certk, int64_t from, int64_t to) {
+    int64_t e = from + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= to) return;
+    status[e] = ST_NOT_COMPUTED;
+    certk[e] = 0;
+}
+
+__global__ void k_flag_uncertified(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ perm,
+                                   const int* __restrict__ status, int64_t nq, int64_t n_hydro,
+                                   uint32_t* __restrict__ flag) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nq) return;
+    const uint32_t e = perm[qs[t]];
+    flag[t] = (e < (uint32_t)n_hydro && status[e] == ST_SECURITY_RADIUS_NOT_REACHED) ? 1u : 0u;
+}
+
+__global__ void k_compact_list(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ flag,
+                               const uint32_t* __restrict__ off, int64_t nq, uint32_t* __restrict__ out) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nq) return;
+    if (flag[t]) out[off[t]] = qs[t];
+}
+
+// One clipping pass over the query list qs[0, nq) with K-neighbour lists `knn`.
+// reset: start a fresh face array (else faces are appended to the current one).
+cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const uint32_t* knn, bool reset,
+                      unsigned long long* fc, unsigned* overflow, unsigned* uncert) {
+    const int D = c->prm.dim;
+    cudaError_t e = cudaSuccess;
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    if (reset && (e = cudaMemsetAsync(&sc->face_count, 0, sizeof(unsigned long long), c->stream))) return e;
+    if ((e = cudaMemsetAsync(&sc->overflow, 0, sizeof(unsigned int), c->stream))) return e;
+    if ((e = cudaMemsetAsync(&sc->uncertified, 0, sizeof(unsigned int), c->stream))) return e;
+    ClipParams P;
+    P.qs = qs;
+    P.perm = (const uint32_t*)c->perm.p;
+    P.spts = c->spts.p;
+    P.ext = c->ext.p;
+    P.knn = knn;
+    P.ghost_src = (const uint32_t*)c->ghost_src.p;
+    P.ghost_code = (const uint32_t*)c->ghost_code.p;
+    P.nq = nq;
+    P.n_hydro = c->n_hydro;
+    P.K = K;
+    P.robust = c->prm.predicates == PGPU_PRED_ROBUST;
+    P.uncertified = &sc->uncertified;
+    P.scale = c->unit_scale;
+    P.vscale = D == 2 ? P.scale * P.scale : P.scale * P.scale * P.scale;
+    P.ascale = D == 2 ? P.scale : P.scale * P.scale;
+    P.vol = (double*)c->vol.p;
+    P.fptr = (uint32_t*)c->fptr.p;
+    P.fcnt = (uint32_t*)c->fcnt.p;
+    P.status = (int*)c->status.p;
+    P.certk = (int*)c->certk.p;
+    P.centroid = (double*)c->centroid.p;
+    P.f_nb = (int32_t*)c->f_nb.p;
+    P.f_own = (uint32_t*)c->f_own.p;
+    P.f_geo = (double4*)c->f_geo.p;
+    P.face_counter = &sc->face_count;
+    P.overflow = &sc->overflow;
+    P.face_cap = c->face_cap;
+    if (nq > 0) {
+        const unsigned blocks = (unsigned)((nq + CLIP_WARPS - 1) / CLIP_WARPS);
+        if (D == 2)
+            k_clip<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+        else
+            k_clip<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+        count_launches(1);
+    }
+    if ((e = cudaGetLastError())) return e;
+    if ((e = cudaMemcpyAsync(fc, &sc->face_count, sizeof(*fc), cudaMemcpyDeviceToHost, c->stream))) return e;
+    if ((e = cudaMemcpyAsync(overflow, &sc->overflow, sizeof(*overflow), cudaMemcpyDeviceToHost, c->stream))) return e;
+    if ((e = cudaMemcpyAsync(uncert, &sc->uncertified, sizeof(*uncert), cudaMemcpyDeviceToHost, c->stream))) return e;
+    return cudaStreamSynchronize(c->stream);
+}
+
+}  // namespace
+
 cudaError_t launch_clip(pgpu_ctx* c) {
     const int D = c->prm.dim;
     cudaError_t e = cudaSuccess;
@@ -694,63 +788,61 @@ cudaError_t launch_clip(pgpu_ctx* c) {
         // ghost cells are not computed in the per-step path
         if ((e = cudaMemsetAsync(c->fcnt.p, 0, (n + 1) * sizeof(uint32_t), c->stream))) return e;
         if ((e = cudaMemsetAsync(c->vol.p, 0, (n + 1) * sizeof(double), c->stream))) return e;
+        k_mark_not_computed<<<nblk(n - c->n_hydro, 256), 256, 0, c->stream>>>((int*)c->status.p, (int*)c->certk.p,
+                                                                              c->n_hydro, n);
+        count_launches(1);
     }
-    DevScalars* sc = (DevScalars*)c->scalars.p;
     for (int attempt = 0; attempt < 3; attempt++) {
         size_t want = c->face_cap;
-        if (want < (size_t)c->n_query * (D == 2 ? 8 : 20) + 1024) want = (size_t)c->n_query * (D == 2 ? 8 : 20) + 1024;
-        if (attempt > 0) want = want * 2;
+        const size_t est = (size_t)c->n_query * (D == 2 ? 8 : 20) + 1024;
+        if (want < est) want = est;
         ensure<int32_t>(c->f_nb, want, &e);
         ensure<uint32_t>(c->f_own, want, &e);
         ensure<double4>(c->f_geo, want, &e);
         if (e) return e;
         c->face_cap = want;
-        if ((e = cudaMemsetAsync(&sc->face_count, 0, sizeof(unsigned long long), c->stream))) return e;
-        if ((e = cudaMemsetAsync(&sc->overflow, 0, sizeof(unsigned int), c->stream))) return e;
-        ClipParams P;
-        P.qs = (const uint32_t*)c->qs.p;
-        P.perm = (const uint32_t*)c->perm.p;
-        P.spts = c->spts.p;
-        P.ext = c->ext.p;
-        P.knn = (const uint32_t*)c->knn.p;
-        P.ghost_src = (const uint32_t*)c->ghost_src.p;
-        P.ghost_code = (const uint32_t*)c->ghost_code.p;
-        P.nq = c->n_query;
-        P.n_hydro = c->n_hydro;
-        P.K = c->prm.k;
-        P.scale = c->unit_scale;
-        P.vscale = D == 2 ? P.scale * P.scale : P.scale * P.scale * P.scale;
-        P.ascale = D == 2 ? P.scale : P.scale * P.scale;
-        P.vol = (double*)c->vol.p;
-        P.fptr = (uint32_t*)c->fptr.p;
-        P.fcnt = (uint32_t*)c->fcnt.p;
-        P.status = (int*)c->status.p;
-        P.certk = (int*)c->certk.p;
-        P.centroid = (double*)c->centroid.p;
-        P.f_nb = (int32_t*)c->f_nb.p;
-        P.f_own = (uint32_t*)c->f_own.p;
-        P.f_geo = (double4*)c->f_geo.p;
-        P.face_counter = &sc->face_count;
-        P.overflow = &sc->overflow;
-        P.face_cap = c->face_cap;
-        if (c->n_query > 0) {
-            const unsigned blocks = (unsigned)((c->n_query + CLIP_WARPS - 1) / CLIP_WARPS);
-            if (D == 2)
-                k_clip<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
-            else
-                k_clip<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
-        }
-        if ((e = cudaGetLastError())) return e;
         unsigned long long fc = 0;
-        unsigned int of = 0;
-        if ((e = cudaMemcpyAsync(&fc, &sc->face_count, sizeof(fc), cudaMemcpyDeviceToHost, c->stream))) return e;
-        if ((e = cudaMemcpyAsync(&of, &sc->overflow, sizeof(of), cudaMemcpyDeviceToHost, c->stream))) return e;
-        if ((e = cudaStreamSynchronize(c->stream))) return e;
+        unsigned of = 0, unc = 0;
+        if ((e = clip_pass(c, (const uint32_t*)c->qs.p, c->n_query, c->prm.k, (const uint32_t*)c->knn.p, true, &fc, &of,
+                           &unc)))
+            return e;
         c->num_faces = (int64_t)fc;
+        c->n_uncertified = unc;
+        c->n_refit = 0;
         if (!of) return cudaSuccess;
-        c->face_cap = (size_t)fc + 1024;  // retry with room for all faces
+        c->face_cap = (size_t)fc * 5 / 4 + 1024;  // retry with room for all faces
     }
     return cudaErrorMemoryAllocation;
+}
+
+cudaError_t launch_fallback(pgpu_ctx* c) {
+    cudaError_t e = cudaSuccess;
+    const int64_t nq = c->n_query;
+    const int K2 = c->prm.k_fallback;
+    uint32_t* flag = ensure<uint32_t>(c->qflag, nq + 1, &e);
+    uint32_t* off = ensure<uint32_t>(c->qoff, nq + 1, &e);
+    uint32_t* fq = ensure<uint32_t>(c->fb_qs, nq + 1, &e);
+    if (e) return e;
+    k_flag_uncertified<<<nblk(nq, 256), 256, 0, c->stream>>>((const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p,
+                                                              (const int*)c->status.p, nq, c->n_hydro, flag);
+    if ((e = exclusive_scan_u32(flag, off, nq, c->scan_tmp, c->stream))) return e;
+    k_compact_list<<<nblk(nq, 256), 256, 0, c->stream>>>((const uint32_t*)c->qs.p, flag, off, nq, fq);
+    count_launches(2);
+    uint32_t nf = 0;
+    if ((e = cudaMemcpyAsync(&nf, off + nq, sizeof(nf), cudaMemcpyDeviceToHost, c->stream))) return e;
+    if ((e = cudaStreamSynchronize(c->stream))) return e;
+    if (nf == 0) return cudaSuccess;
+    uint32_t* kl = ensure<uint32_t>(c->fb_knn, (size_t)nf * K2 + 1, &e);
+    if (e) return e;
+    if ((e = launch_knn_list(c, fq, nf, K2, kl))) return e;
+    unsigned long long fc = 0;
+    unsigned of = 0, unc = 0;
+    if ((e = clip_pass(c, fq, nf, K2, kl, false, &fc, &of, &unc))) return e;
+    if (of) return cudaErrorMemoryAllocation;
+    c->num_faces = (int64_t)fc;
+    c->n_uncertified = unc;
+    c->n_refit = nf;
+    return cudaSuccess;
 }
 
 }  // namespace pgpu

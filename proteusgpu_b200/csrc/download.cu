@@ -75,6 +75,7 @@ cudaError_t launch_mesh_compact(pgpu_ctx* c, uint32_t* new_ptr, int32_t* nb_out,
         k_gather_faces<<<nblk(n * 32, 256), 256, 0, c->stream>>>(
             (const uint32_t*)c->fptr.p, (const uint32_t*)c->fcnt.p, new_ptr, (const int32_t*)c->f_nb.p,
             (const double4*)c->f_geo.p, n, nb_out, nrm_out, area_out);
+    if (n > 0) count_launches(1);
     return cudaGetLastError();
 }
 
@@ -85,6 +86,7 @@ cudaError_t launch_seeds(pgpu_ctx* c, double* out, bool no_scale) {
         k_seeds<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, (const int*)c->status.p, n, c->unit_scale, no_scale, out);
     else
         k_seeds<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, (const int*)c->status.p, n, c->unit_scale, no_scale, out);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -93,6 +95,7 @@ cudaError_t launch_knn_rows(pgpu_ctx* c, uint32_t* out) {
     if (nq <= 0) return cudaSuccess;
     k_knn_rows<<<nblk(nq * 32, 256), 256, 0, c->stream>>>((const uint32_t*)c->knn.p, (const uint32_t*)c->qs.p,
                                                            (const uint32_t*)c->perm.p, nq, c->prm.k, out);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -102,6 +105,7 @@ cudaError_t launch_unpack_points(pgpu_ctx* c, const void* pts, int64_t n, double
         k_unpack_points<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)pts, n, out);
     else
         k_unpack_points<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)pts, n, out);
+    count_launches(1);
     return cudaGetLastError();
 }
 

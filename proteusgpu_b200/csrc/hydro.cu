@@ -293,6 +293,7 @@ cudaError_t launch_dt_ref(pgpu_ctx* c, double cfl) {
             k_dt_ref<3><<<nblk(n, HT), HT, 0, c->stream>>>((const double*)c->rho.p, (const double*)c->vel.p,
                                                             (const double*)c->energy.p, (const double*)c->vol.p, n,
                                                             cfl, c->prm.gamma, &sc->dt_bits);
+        count_launches(1);
     }
     return cudaGetLastError();
 }
@@ -319,6 +320,7 @@ cudaError_t launch_hydro_ref(pgpu_ctx* c, double dt) {
             if (phys) PGPU_HREF(3, true); else PGPU_HREF(3, false);
         }
 #undef PGPU_HREF
+        count_launches(1);
     }
     if ((e = cudaGetLastError())) return e;
     std::swap(c->rho, c->rho2);
@@ -344,6 +346,7 @@ cudaError_t launch_cons_from_prim(pgpu_ctx* c, const double* dep) {
             k_cons_from_prim<3><<<nblk(n, HT), HT, 0, c->stream>>>(
                 (const double*)c->rho.p, (const double*)c->vel.p, (const double*)c->energy.p, dep,
                 (const double*)c->vol.p, n, (double*)c->mass.p, (double*)c->mom.p, (double*)c->en.p);
+        count_launches(1);
     }
     return cudaGetLastError();
 }
@@ -375,6 +378,7 @@ cudaError_t launch_prim_dt(pgpu_ctx* c, double cfl, double fixed_dt) {
                                                             (const double*)c->en.p, (const double*)c->vol.p,
                                                             (const int*)c->status.p, (const int*)c->certk.p, n, cfl,
                                                             c->prm.gamma, w4, we, sc);
+        count_launches(1);
     }
     return cudaGetLastError();
 }
@@ -405,6 +409,7 @@ cudaError_t launch_flux_update(pgpu_ctx* c, double fixed_dt) {
         }
     }
 #undef PGPU_FLUX
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -423,6 +428,7 @@ cudaError_t launch_sums(pgpu_ctx* c) {
             k_partial_sums<3><<<(unsigned)nb, HT, 0, c->stream>>>((const double*)c->mass.p, (const double*)c->mom.p,
                                                                   (const double*)c->en.p, n, part);
         k_final_sums<<<1, 32, 0, c->stream>>>(part, nb, sc->sums);
+        count_launches(2);
     }
     return cudaGetLastError();
 }

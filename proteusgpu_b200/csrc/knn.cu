@@ -270,15 +270,14 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
 }
 
 template <int D>
-cudaError_t knn_dispatch(pgpu_ctx* c, int K, uint32_t* out, unsigned long long* cc) {
-    const int64_t nq = c->n_query;
+cudaError_t knn_dispatch(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, uint32_t* out,
+                         unsigned long long* cc) {
     if (nq <= 0) return cudaSuccess;
     const unsigned blocks = (unsigned)((nq + KNN_WARPS - 1) / KNN_WARPS);
     using PT = typename PointOf<D>::type;
     const PT* sp = (const PT*)c->spts.p;
     const uint32_t* perm = (const uint32_t*)c->perm.p;
     const uint32_t* bs = (const uint32_t*)c->bin_start.p;
-    const uint32_t* qs = (const uint32_t*)c->qs.p;
     const int G = c->grid_G;
 #define PGPU_KNN_CASE(RR) k_knn<D, RR><<<blocks, KNN_WARPS * 32, 0, c->stream>>>(sp, perm, bs, G, qs, nq, K, out, cc)
     if (K <= 32)
@@ -294,10 +293,17 @@ cudaError_t knn_dispatch(pgpu_ctx* c, int K, uint32_t* out, unsigned long long* 
     else
         PGPU_KNN_CASE(8);
 #undef PGPU_KNN_CASE
+    count_launches(1);
     return cudaGetLastError();
 }
 
 }  // namespace
+
+cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, uint32_t* out) {
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    unsigned long long* cc = &sc->knn_cand;
+    return c->prm.dim == 2 ? knn_dispatch<2>(c, qs, nq, K, out, cc) : knn_dispatch<3>(c, qs, nq, K, out, cc);
+}
 
 cudaError_t launch_knn(pgpu_ctx* c) {
     cudaError_t e = cudaSuccess;
@@ -305,9 +311,8 @@ cudaError_t launch_knn(pgpu_ctx* c) {
     uint32_t* out = ensure<uint32_t>(c->knn, (size_t)c->n_query * K + 1, &e);
     if (e) return e;
     DevScalars* sc = (DevScalars*)c->scalars.p;
-    unsigned long long* cc = &sc->knn_cand;
-    if ((e = cudaMemsetAsync(cc, 0, sizeof(unsigned long long), c->stream))) return e;
-    return c->prm.dim == 2 ? knn_dispatch<2>(c, K, out, cc) : knn_dispatch<3>(c, K, out, cc);
+    if ((e = cudaMemsetAsync(&sc->knn_cand, 0, sizeof(unsigned long long), c->stream))) return e;
+    return launch_knn_list(c, (const uint32_t*)c->qs.p, c->n_query, K, out);
 }
 
 }  // namespace pgpu

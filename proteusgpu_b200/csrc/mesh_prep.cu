@@ -164,6 +164,7 @@ cudaError_t launch_ghosts(pgpu_ctx* c, const double* pos_dev, int64_t n, bool no
             else
                 k_ghost_count<3><<<nblk(n, 256), 256, 0, c->stream>>>(pos_dev, n, buff, cnt);
         }
+        if (n > 0) count_launches(1);
         if ((e = exclusive_scan_u32(cnt, off, n, c->scan_tmp, c->stream))) return e;
         uint32_t total = 0;
         if ((e = cudaMemcpyAsync(&total, off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream))) return e;
@@ -188,6 +189,7 @@ cudaError_t launch_ghosts(pgpu_ctx* c, const double* pos_dev, int64_t n, bool no
                 pos_dev, n, buff, scale, c->prm.boundary == PGPU_REFLECTIVE, no_ghosts, off, (double4*)c->ext.p,
                 (uint32_t*)c->ghost_src.p, (uint32_t*)c->ghost_code.p);
     }
+    if (n > 0) count_launches(1);
     c->unit_scale = no_ghosts ? 1.0 : 1. + (2 * buff);
     return cudaGetLastError();
 }
@@ -227,6 +229,7 @@ cudaError_t launch_grid_sort(pgpu_ctx* c) {
         else
             k_bin_count<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, G, key, cnt);
     }
+    if (n > 0) count_launches(1);
     if ((e = exclusive_scan_u32(cnt, start, M, c->scan_tmp, c->stream))) return e;
     if ((e = cudaMemsetAsync(cnt, 0, (M + 1) * sizeof(uint32_t), c->stream))) return e;
     if (n > 0) {
@@ -236,6 +239,7 @@ cudaError_t launch_grid_sort(pgpu_ctx* c) {
         else
             k_bin_scatter<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, key, start, cnt,
                                                                   (double4*)c->spts.p, perm, inv);
+        count_launches(1);
     }
     return cudaGetLastError();
 }
@@ -248,7 +252,10 @@ cudaError_t launch_query_list(pgpu_ctx* c, bool all_cells) {
     c->all_cells = all_cells;
     if (all_cells || c->n_hydro == n) {
         c->n_query = n;
-        if (n > 0) k_iota<<<nblk(n, 256), 256, 0, c->stream>>>(qs, n);
+        if (n > 0) {
+            k_iota<<<nblk(n, 256), 256, 0, c->stream>>>(qs, n);
+            count_launches(1);
+        }
         return cudaGetLastError();
     }
     uint32_t* flag = ensure<uint32_t>(c->qflag, n + 1, &e);
@@ -257,6 +264,7 @@ cudaError_t launch_query_list(pgpu_ctx* c, bool all_cells) {
     k_query_flags<<<nblk(n, 256), 256, 0, c->stream>>>((const uint32_t*)c->perm.p, n, c->n_hydro, flag);
     if ((e = exclusive_scan_u32(flag, off, n, c->scan_tmp, c->stream))) return e;
     k_query_compact<<<nblk(n, 256), 256, 0, c->stream>>>(flag, off, n, qs);
+    count_launches(2);
     c->n_query = c->n_hydro;
     return cudaGetLastError();
 }

@@ -105,11 +105,11 @@ struct Flux {
     double rho, mx, my, mz, E;
 };
 
-__device__ __forceinline__ double dmin_ref(double a, double b) { return (b < a) ? b : a; }  // std::min
-__device__ __forceinline__ double dmax_ref(double a, double b) { return (a < b) ? b : a; }  // std::max
+__host__ __device__ __forceinline__ double dmin_ref(double a, double b) { return (b < a) ? b : a; }  // std::min
+__host__ __device__ __forceinline__ double dmax_ref(double a, double b) { return (a < b) ? b : a; }  // std::max
 
 template <int D>
-__device__ __forceinline__ double pressure(const Prim& s, double gamma) {
+__host__ __device__ __forceinline__ double pressure(const Prim& s, double gamma) {
     if (D == 2) return (gamma - 1) * (s.E - (0.5 * s.rho * (s.vx * s.vx + s.vy * s.vy)));
     return (gamma - 1) * (s.E - (0.5 * s.rho * (s.vx * s.vx + s.vy * s.vy + s.vz * s.vz)));
 }
@@ -119,7 +119,7 @@ struct Frame {
 };
 
 // compute_geom (riemann.cpp:75-97)
-__device__ __forceinline__ Frame make_frame(double ax, double ay, double az) {
+__host__ __device__ __forceinline__ Frame make_frame(double ax, double ay, double az) {
     Frame g;
     double nn = sqrt(ax * ax + ay * ay + az * az);
     g.nx = ax / nn;
@@ -146,7 +146,7 @@ __device__ __forceinline__ Frame make_frame(double ax, double ay, double az) {
 }
 
 template <int D>
-__device__ __forceinline__ void to_face(Prim& s, const Frame& g) {  // rotate_to_face
+__host__ __device__ __forceinline__ void to_face(Prim& s, const Frame& g) {  // rotate_to_face
     double vx = s.vx, vy = s.vy;
     if (D == 2) {
         s.vx = vx * g.nx + vy * g.ny;
@@ -160,7 +160,7 @@ __device__ __forceinline__ void to_face(Prim& s, const Frame& g) {  // rotate_to
 }
 
 template <int D>
-__device__ __forceinline__ Flux phys_flux(const Prim& s, double gamma) {  // get_flux
+__host__ __device__ __forceinline__ Flux phys_flux(const Prim& s, double gamma) {  // get_flux
     double P = pressure<D>(s, gamma);
     Flux f;
     f.rho = s.rho * s.vx;
@@ -173,7 +173,7 @@ __device__ __forceinline__ Flux phys_flux(const Prim& s, double gamma) {  // get
 
 // riemann_hll with the face normal (ax, ay, az); returns the lab-frame flux.
 template <int D>
-__device__ __forceinline__ Flux hll(Prim L, Prim R, double ax, double ay, double az, double gamma) {
+__host__ __device__ __forceinline__ Flux hll(Prim L, Prim R, double ax, double ay, double az, double gamma) {
     Frame g = make_frame(ax, ay, az);
     to_face<D>(L, g);
     to_face<D>(R, g);

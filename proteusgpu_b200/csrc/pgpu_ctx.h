@@ -35,7 +35,7 @@ struct DevScalars {
     unsigned int unpaired;          // faces without a reverse partner
     unsigned int failed;            // hydro cells not certified
     int cert_k_max;
-    unsigned int pad;
+    unsigned int uncertified;       // hydro cells with SECURITY_RADIUS_NOT_REACHED in the last clip
     double dt;                      // the step's dt (device copy)
     double sums[5];                 // mass, mom x/y/z, energy
 };
@@ -80,9 +80,15 @@ struct pgpu_ctx {
     // download staging
     pgpu::DevBuf dl_ptr, dl_a, dl_b, dl_c;
     size_t face_cap = 0;
+    int64_t n_uncertified = 0;  // hydro cells of the last clip with SECURITY_RADIUS_NOT_REACHED
+    int64_t n_refit = 0;        // cells recomputed with the fallback budget in the last step
+    pgpu::DevBuf fb_qs, fb_knn; // fallback query list and lists
 };
 
 namespace pgpu {
+
+// Process-wide count of kernel launches (statistics, pgpu_launch_count).
+void count_launches(int n);
 
 // ---- launch wrappers (defined in the .cu files) ----
 // scan.cu
@@ -93,8 +99,10 @@ cudaError_t launch_grid_sort(pgpu_ctx* c);
 cudaError_t launch_query_list(pgpu_ctx* c, bool all_cells);
 // knn.cu
 cudaError_t launch_knn(pgpu_ctx* c);
+cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, uint32_t* out);
 // clip.cu
 cudaError_t launch_clip(pgpu_ctx* c);
+cudaError_t launch_fallback(pgpu_ctx* c);
 // hydro.cu
 cudaError_t launch_prim_dt(pgpu_ctx* c, double cfl, double fixed_dt);
 cudaError_t launch_flux_update(pgpu_ctx* c, double fixed_dt);

@@ -103,6 +103,7 @@ cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, Dev
     k_block_sums<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, sums);
     k_scan_sums<<<1, SCAN_THREADS, 0, s>>>(sums, nb);
     k_rescan<<<(unsigned)nb, SCAN_THREADS, 0, s>>>(in, n, sums, out);
+    count_launches(3);
     return cudaGetLastError();
 }
 
