@@ -166,7 +166,7 @@ void pgpu_destroy(pgpu_ctx* c) {
     if (!c) return;
     cudaSetDevice(c->prm.device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    DevBuf* bufs[] = {&c->fb_qs, &c->fb_knn, &c->pos,   &c->ext,     &c->gcnt,     &c->goff,   &c->ghost_src, &c->ghost_code, &c->bin_cnt,
+    DevBuf* bufs[] = {&c->knn_table, &c->fb_qs, &c->fb_knn, &c->pos,   &c->ext,     &c->gcnt,     &c->goff,   &c->ghost_src, &c->ghost_code, &c->bin_cnt,
                       &c->bin_start, &c->bin_key, &c->spts, &c->perm,  &c->inv,       &c->qflag,      &c->qoff,
                       &c->qs,    &c->knn,     &c->vol,      &c->fptr,   &c->fcnt,      &c->status,     &c->certk,
                       &c->centroid, &c->f_nb, &c->f_own,    &c->f_geo,  &c->scan_tmp,  &c->scalars,    &c->rho,

@@ -1,24 +1,32 @@
 // Exact K nearest neighbours on the Morton-ordered grid (replaces
 // knn::solve / cpu_knearest, src/knn/knn.cpp:225-315).
 //
-// One warp per query point.  Bins are visited in Chebyshev rings around the
-// query's bin (as the reference's ring-sorted offset table does), each ring's
-// bins expanded 32 at a time into a flat candidate range by a warp prefix sum,
-// so that every lane evaluates one candidate per iteration whatever the bin
-// occupancy.  A bin is skipped once the list is full and its box lies farther
-// than the current K-th neighbour; the search stops when the K-th neighbour is
-// closer than everything outside the rings visited so far.
+// One warp per query point.  Neighbour bins are visited in the order of a
+// host-built offset table sorted by the lower bound of the distance from any
+// point of the query's bin to the offset bin, h^2 * sum_a max(|d_a| - 1, 0)^2
+// (the reference's ring table, knn.cpp:39-89, orders by Chebyshev ring with the
+// bound (ring - 1)^2 h^2; this order is tighter).  Thirty-two table entries are
+// taken per step, one per lane; a bin whose box lies farther than the current
+// K-th neighbour is skipped, and the search ends as soon as the table's bound
+// passes the K-th neighbour.  The chunk's bins are expanded into one flat
+// candidate range by a warp prefix sum so that every lane evaluates one
+// candidate per step whatever the bin occupancy.  Beyond the table (sparse
+// regions) the search continues ring by ring.
 //
-// The K best are kept ascending in R registers per lane (element r*32 + lane).
-// Candidates that beat the current K-th best are queued in shared memory;
-// a full queue is bitonic-sorted across the warp with shuffles and merged row
-// by row (bitonic merge of the row with the reversed queue).  Keys are
-// (squared distance, extended id), so ties break by index.
+// The K best are kept ascending in shared memory, ceil(K/32) rows of 32 per
+// warp.  Candidates that beat the current K-th best queue in shared memory; a
+// full queue is bitonic-sorted across the warp with shuffles and merged row by
+// row (bitonic merge of the row with the reversed queue), in a loop that is not
+// unrolled so the kernel's code stays small.  Keys are (squared distance,
+// extended id): ties break by index.
 //
 // The squared distance is the reference's dist2_point (src/knn/knn.h:64-75),
-// dx*dx + dy*dy (+ dz*dz) with dx = query - candidate, compiled without FMA:
-// the values, and therefore the order, equal the reference's.
+// dx*dx + dy*dy (+ dz*dz) with dx = query - candidate, without FMA, so the
+// values and therefore the order equal the reference's.
 #include <math_constants.h>
+
+#include <algorithm>
+#include <vector>
 
 #include "pgpu_common.cuh"
 #include "pgpu_ctx.h"
@@ -27,7 +35,10 @@ namespace pgpu {
 namespace {
 
 constexpr int KNN_WARPS = 4;
+constexpr int MAX_ROWS = MAX_K / 32;
 constexpr unsigned FULL = 0xffffffffu;
+constexpr int TABLE_R3 = 8;   // offsets with |d|_inf <= 8 in 3D (17^3 entries)
+constexpr int TABLE_R2 = 24;  // and |d|_inf <= 24 in 2D (49^2 entries)
 
 __device__ __forceinline__ bool key_less(double ad, uint32_t ai, double bd, uint32_t bi) {
     return ad < bd || (ad == bd && ai < bi);
@@ -76,233 +87,298 @@ __device__ __forceinline__ void bitonic_merge32(double& d, uint32_t& id, int lan
     }
 }
 
-// Merges qn queued keys into the ascending rows (rd, ri), keeping the 32R smallest.
-template <int R>
-__device__ __forceinline__ void merge_queue(double (&rd)[R], uint32_t (&ri)[R], const double* qd,
-                                            const uint32_t* qi, int qn, int lane) {
+struct KnnSmem {
+    double row_d[KNN_WARPS][MAX_ROWS * 32];
+    uint32_t row_i[KNN_WARPS][MAX_ROWS * 32];
+    double q_d[KNN_WARPS][32];
+    uint32_t q_i[KNN_WARPS][32];
+    uint32_t b_start[KNN_WARPS][32];
+    uint32_t b_excl[KNN_WARPS][32];
+};
+
+// Merges qn queued keys into the warp's ascending rows (rows of 32 in shared
+// memory), keeping the 32 * nrows smallest.
+__device__ __noinline__ void merge_queue(double* rd, uint32_t* ri, const double* qd, const uint32_t* qi, int qn,
+                                         int nrows, int lane) {
     double d = lane < qn ? qd[lane] : CUDART_INF;
     uint32_t id = lane < qn ? qi[lane] : NO_NEIGHBOR;
     bitonic_sort32(d, id, lane);
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        double qmin = __shfl_sync(FULL, d, 0);
-        uint32_t qmini = __shfl_sync(FULL, id, 0);
-        double rmax = __shfl_sync(FULL, rd[r], 31);
-        uint32_t rmaxi = __shfl_sync(FULL, ri[r], 31);
+#pragma unroll 1
+    for (int r = 0; r < nrows; r++) {
+        const double qmin = __shfl_sync(FULL, d, 0);
+        const uint32_t qmini = __shfl_sync(FULL, id, 0);
+        const double rmax = rd[r * 32 + 31];
+        const uint32_t rmaxi = ri[r * 32 + 31];
         if (!key_less(qmin, qmini, rmax, rmaxi)) continue;  // the queue lies entirely above this row
         double od = __shfl_sync(FULL, d, 31 - lane);
         uint32_t oi = __shfl_sync(FULL, id, 31 - lane);
-        bool rl = key_less(rd[r], ri[r], od, oi);
-        double lod = rl ? rd[r] : od, hid = rl ? od : rd[r];
-        uint32_t loi = rl ? ri[r] : oi, hii = rl ? oi : ri[r];
+        const double cd = rd[r * 32 + lane];
+        const uint32_t ci = ri[r * 32 + lane];
+        const bool rl = key_less(cd, ci, od, oi);
+        double lod = rl ? cd : od, hid = rl ? od : cd;
+        uint32_t loi = rl ? ci : oi, hii = rl ? oi : ci;
         bitonic_merge32(lod, loi, lane);
         bitonic_merge32(hid, hii, lane);
-        rd[r] = lod;
-        ri[r] = loi;
+        __syncwarp();
+        rd[r * 32 + lane] = lod;
+        ri[r * 32 + lane] = loi;
+        __syncwarp();
         d = hid;
         id = hii;
     }
 }
 
-template <int R>
-__device__ __forceinline__ void kth_key(const double (&rd)[R], const uint32_t (&ri)[R], int rk, int lk, double& td,
-                                        uint32_t& ti) {
-    double d = rd[0];
-    uint32_t i = ri[0];
+// Processes one set of up to 32 bins (bstart, bcnt per lane) against the query.
+template <int D>
+__device__ __forceinline__ void scan_bins(const typename PointOf<D>::type* __restrict__ spts,
+                                          const uint32_t* __restrict__ perm, uint32_t bstart, uint32_t bcnt,
+                                          const typename PointOf<D>::type& p, uint32_t qid, KnnSmem& S, int w,
+                                          int lane, int nrows, int K, int& qn, double& thr_d, uint32_t& thr_i,
+                                          unsigned long long& ncand) {
+    using PT = typename PointOf<D>::type;
+    const uint32_t incl = warp_incl_scan_u32(bcnt, lane);
+    const uint32_t total = __shfl_sync(FULL, incl, 31);
+    if (total == 0) return;
+    __syncwarp();
+    S.b_start[w][lane] = bstart;
+    S.b_excl[w][lane] = incl - bcnt;
+    __syncwarp();
+    ncand += total;
+    for (uint32_t k0 = 0; k0 < total; k0 += 32) {
+        const uint32_t tt = k0 + lane;
+        bool valid = tt < total;
+        double d2 = CUDART_INF;
+        uint32_t eid = NO_NEIGHBOR;
+        if (valid) {
+            int j = 0;
 #pragma unroll
-    for (int r = 1; r < R; r++)
-        if (r == rk) {
-            d = rd[r];
-            i = ri[r];
+            for (int step = 16; step > 0; step >>= 1)
+                if (j + step < 32 && S.b_excl[w][j + step] <= tt) j += step;
+            const uint32_t sidx = S.b_start[w][j] + (tt - S.b_excl[w][j]);
+            eid = perm[sidx];
+            if (eid == qid) {
+                valid = false;
+            } else {
+                const PT c = spts[sidx];
+                double ddx = p.x - c.x;
+                double ddy = p.y - c.y;
+                if (D == 2) {
+                    d2 = ddx * ddx + ddy * ddy;
+                } else {
+                    double ddz = pz(p) - pz(c);
+                    d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                }
+            }
         }
-    td = __shfl_sync(FULL, d, lk);
-    ti = __shfl_sync(FULL, i, lk);
+        bool surv = valid && key_less(d2, eid, thr_d, thr_i);
+        unsigned bal = __ballot_sync(FULL, surv);
+        if (bal == 0) continue;
+        if (qn + __popc(bal) > 32) {
+            __syncwarp();
+            merge_queue(S.row_d[w], S.row_i[w], S.q_d[w], S.q_i[w], qn, nrows, lane);
+            qn = 0;
+            __syncwarp();
+            thr_d = S.row_d[w][K - 1];
+            thr_i = S.row_i[w][K - 1];
+            surv = surv && key_less(d2, eid, thr_d, thr_i);
+            bal = __ballot_sync(FULL, surv);
+        }
+        if (surv) {
+            const int pos = qn + __popc(bal & ((1u << lane) - 1u));
+            S.q_d[w][pos] = d2;
+            S.q_i[w][pos] = eid;
+        }
+        qn += __popc(bal);
+        __syncwarp();
+    }
 }
 
-template <int D, int R>
+__device__ __forceinline__ void flush_queue(KnnSmem& S, int w, int lane, int nrows, int K, int& qn, double& thr_d,
+                                            uint32_t& thr_i) {
+    if (qn == 0) return;
+    __syncwarp();
+    merge_queue(S.row_d[w], S.row_i[w], S.q_d[w], S.q_i[w], qn, nrows, lane);
+    qn = 0;
+    __syncwarp();
+    thr_d = S.row_d[w][K - 1];
+    thr_i = S.row_i[w][K - 1];
+}
+
+// Squared distance from p to the box of bin (x, y, z).
+template <int D>
+__device__ __forceinline__ double box_d2(const double* pc, int x, int y, int z, double h) {
+    const int bx[3] = {x, y, z};
+    double bd2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        double lo = (double)bx[a] * h, hi = (double)(bx[a] + 1) * h;
+        double dd = pc[a] < lo ? lo - pc[a] : (pc[a] > hi ? pc[a] - hi : 0.0);
+        bd2 += dd * dd;
+    }
+    return bd2;
+}
+
+template <int D>
 __global__ void __launch_bounds__(KNN_WARPS * 32)
     k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm,
-          const uint32_t* __restrict__ bin_start, int G, const uint32_t* __restrict__ qs, int64_t nq, int K,
-          uint32_t* __restrict__ out, unsigned long long* __restrict__ cand_counter) {
-    __shared__ double sq_d[KNN_WARPS][32];
-    __shared__ uint32_t sq_i[KNN_WARPS][32];
-    __shared__ uint32_t sb_start[KNN_WARPS][32];
-    __shared__ uint32_t sb_excl[KNN_WARPS][32];
+          const uint32_t* __restrict__ bin_start, int G, const int2* __restrict__ table, int table_n, int table_r,
+          const uint32_t* __restrict__ qs, int64_t nq, int K, uint32_t* __restrict__ out,
+          unsigned long long* __restrict__ cand_counter) {
+    __shared__ KnnSmem S;
     using PT = typename PointOf<D>::type;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t t = (int64_t)blockIdx.x * KNN_WARPS + w;
     if (t >= nq) return;  // warp-uniform
+    const int nrows = (K + 31) >> 5;
+    for (int r = 0; r < nrows; r++) {
+        S.row_d[w][r * 32 + lane] = CUDART_INF;
+        S.row_i[w][r * 32 + lane] = NO_NEIGHBOR;
+    }
+    __syncwarp();
     const uint32_t s = qs[t];
     const PT p = spts[s];
     const uint32_t qid = perm[s];
     const double pc[3] = {p.x, p.y, pz(p)};
     const int bc[3] = {bin_coord(p.x, G), bin_coord(p.y, G), D == 3 ? bin_coord(pz(p), G) : 0};
     const double h = 1.0 / (double)G;
-
-    double rd[R];
-    uint32_t ri[R];
-#pragma unroll
-    for (int r = 0; r < R; r++) rd[r] = CUDART_INF, ri[r] = NO_NEIGHBOR;
-    const int rk = (K - 1) >> 5, lk = (K - 1) & 31;
     double thr_d = CUDART_INF;
     uint32_t thr_i = NO_NEIGHBOR;
     int qn = 0;
     unsigned long long ncand = 0;
+    bool done = false;
 
-    for (int r = 0;; r++) {
-        if (r >= 1) {
-            // Every point not yet visited lies outside the cube of rings <= r-1.
-            double lb = CUDART_INF;
-            bool all = true;
-#pragma unroll
-            for (int a = 0; a < D; a++) {
-                int lo = bc[a] - (r - 1), hi = bc[a] + (r - 1);
-                if (lo > 0) {
-                    all = false;
-                    lb = fmin(lb, pc[a] - (double)lo * h);
-                }
-                if (hi < G - 1) {
-                    all = false;
-                    lb = fmin(lb, (double)(hi + 1) * h - pc[a]);
-                }
-            }
-            if (all) break;
-            if (thr_i != NO_NEIGHBOR && lb > 0.0 && thr_d < lb * lb * (1.0 - 1e-12)) break;
-            if (r > G) break;
+    // 1. offsets in order of their lower bound
+    for (int c0 = 0; c0 < table_n; c0 += 32) {
+        const int2 first = table[c0];
+        if (thr_i != NO_NEIGHBOR && (double)first.y * h * h * (1.0 - 1e-12) > thr_d) {
+            done = true;  // every remaining bin is farther than the K-th neighbour
+            break;
         }
+        const int ci = c0 + lane;
+        uint32_t bstart = 0, bcnt = 0;
+        if (ci < table_n) {
+            const int2 ent = table[ci];
+            const int dx = (int)(signed char)(ent.x & 255), dy = (int)(signed char)((ent.x >> 8) & 255),
+                      dz = (int)(signed char)((ent.x >> 16) & 255);
+            const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
+            bool ok = x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G));
+            if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
+            if (ok) {
+                const uint32_t key = morton<D>(x, y, z);
+                bstart = bin_start[key];
+                bcnt = bin_start[key + 1] - bstart;
+            }
+        }
+        scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, w, lane, nrows, K, qn, thr_d, thr_i, ncand);
+        // the bound is tested at chunk boundaries: merge what is queued
+        flush_queue(S, w, lane, nrows, K, qn, thr_d, thr_i);
+    }
+
+    // 2. beyond the table: Chebyshev rings table_r + 1, table_r + 2, ... (sparse regions)
+    for (int r = table_r + 1; !done; r++) {
+        double lb = CUDART_INF;
+        bool all = true;
+#pragma unroll
+        for (int a = 0; a < D; a++) {
+            int lo = bc[a] - (r - 1), hi = bc[a] + (r - 1);
+            if (lo > 0) {
+                all = false;
+                lb = fmin(lb, pc[a] - (double)lo * h);
+            }
+            if (hi < G - 1) {
+                all = false;
+                lb = fmin(lb, (double)(hi + 1) * h - pc[a]);
+            }
+        }
+        if (all || r > G + 1) break;
+        if (thr_i != NO_NEIGHBOR && lb > 0.0 && thr_d < lb * lb * (1.0 - 1e-12)) break;
         const int w1 = 2 * r + 1;
         const int ncube = D == 2 ? w1 * w1 : w1 * w1 * w1;
         for (int c0 = 0; c0 < ncube; c0 += 32) {
             const int ci = c0 + lane;
             uint32_t bstart = 0, bcnt = 0;
             if (ci < ncube) {
-                int dx = ci % w1 - r;
-                int rest = ci / w1;
-                int dy = rest % w1 - r;
-                int dz = D == 3 ? rest / w1 - r : 0;
-                int cheb = max(abs(dx), max(abs(dy), abs(dz)));
-                int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
+                const int dx = ci % w1 - r;
+                const int rest = ci / w1;
+                const int dy = rest % w1 - r;
+                const int dz = D == 3 ? rest / w1 - r : 0;
+                const int cheb = max(abs(dx), max(abs(dy), abs(dz)));
+                const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
                 bool ok = cheb == r && x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G));
-                if (ok && thr_i != NO_NEIGHBOR) {
-                    const int bx[3] = {x, y, z};
-                    double bd2 = 0.0;
-#pragma unroll
-                    for (int a = 0; a < D; a++) {
-                        double lo = (double)bx[a] * h, hi = (double)(bx[a] + 1) * h;
-                        double dd = pc[a] < lo ? lo - pc[a] : (pc[a] > hi ? pc[a] - hi : 0.0);
-                        bd2 += dd * dd;
-                    }
-                    if (bd2 * (1.0 - 1e-12) > thr_d) ok = false;
-                }
+                if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
                 if (ok) {
-                    uint32_t key = morton<D>(x, y, z);
+                    const uint32_t key = morton<D>(x, y, z);
                     bstart = bin_start[key];
                     bcnt = bin_start[key + 1] - bstart;
                 }
             }
-            const uint32_t incl = warp_incl_scan_u32(bcnt, lane);
-            const uint32_t total = __shfl_sync(FULL, incl, 31);
-            if (total == 0) continue;
-            sb_start[w][lane] = bstart;
-            sb_excl[w][lane] = incl - bcnt;
-            __syncwarp();
-            ncand += total;
-            for (uint32_t k0 = 0; k0 < total; k0 += 32) {
-                const uint32_t tt = k0 + lane;
-                bool valid = tt < total;
-                double d2 = CUDART_INF;
-                uint32_t eid = NO_NEIGHBOR;
-                if (valid) {
-                    int j = 0;
-#pragma unroll
-                    for (int step = 16; step > 0; step >>= 1)
-                        if (j + step < 32 && sb_excl[w][j + step] <= tt) j += step;
-                    const uint32_t sidx = sb_start[w][j] + (tt - sb_excl[w][j]);
-                    eid = perm[sidx];
-                    if (eid == qid) {
-                        valid = false;
-                    } else {
-                        const PT c = spts[sidx];
-                        double ddx = p.x - c.x;
-                        double ddy = p.y - c.y;
-                        if (D == 2) {
-                            d2 = ddx * ddx + ddy * ddy;
-                        } else {
-                            double ddz = pz(p) - pz(c);
-                            d2 = ddx * ddx + ddy * ddy + ddz * ddz;
-                        }
-                    }
-                }
-                bool surv = valid && key_less(d2, eid, thr_d, thr_i);
-                unsigned bal = __ballot_sync(FULL, surv);
-                if (bal == 0) continue;
-                if (qn + __popc(bal) > 32) {
-                    __syncwarp();
-                    merge_queue<R>(rd, ri, sq_d[w], sq_i[w], qn, lane);
-                    qn = 0;
-                    kth_key<R>(rd, ri, rk, lk, thr_d, thr_i);
-                    surv = surv && key_less(d2, eid, thr_d, thr_i);
-                    bal = __ballot_sync(FULL, surv);
-                }
-                if (surv) {
-                    int pos = qn + __popc(bal & ((1u << lane) - 1u));
-                    sq_d[w][pos] = d2;
-                    sq_i[w][pos] = eid;
-                }
-                qn += __popc(bal);
-                __syncwarp();
-            }
-            __syncwarp();
+            scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, w, lane, nrows, K, qn, thr_d, thr_i, ncand);
         }
-        if (qn > 0) {
-            __syncwarp();
-            merge_queue<R>(rd, ri, sq_d[w], sq_i[w], qn, lane);
-            qn = 0;
-            kth_key<R>(rd, ri, rk, lk, thr_d, thr_i);
-        }
+        flush_queue(S, w, lane, nrows, K, qn, thr_d, thr_i);
     }
-#pragma unroll
-    for (int r = 0; r < R; r++) {
-        int idx = r * 32 + lane;
-        if (idx < K) out[t * K + idx] = ri[r];
-    }
+    __syncwarp();
+    for (int idx = lane; idx < K; idx += 32) out[t * K + idx] = S.row_i[w][idx];
     if (cand_counter && lane == 0) atomicAdd(cand_counter, ncand);
-}
-
-template <int D>
-cudaError_t knn_dispatch(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, uint32_t* out,
-                         unsigned long long* cc) {
-    if (nq <= 0) return cudaSuccess;
-    const unsigned blocks = (unsigned)((nq + KNN_WARPS - 1) / KNN_WARPS);
-    using PT = typename PointOf<D>::type;
-    const PT* sp = (const PT*)c->spts.p;
-    const uint32_t* perm = (const uint32_t*)c->perm.p;
-    const uint32_t* bs = (const uint32_t*)c->bin_start.p;
-    const int G = c->grid_G;
-#define PGPU_KNN_CASE(RR) k_knn<D, RR><<<blocks, KNN_WARPS * 32, 0, c->stream>>>(sp, perm, bs, G, qs, nq, K, out, cc)
-    if (K <= 32)
-        PGPU_KNN_CASE(1);
-    else if (K <= 64)
-        PGPU_KNN_CASE(2);
-    else if (K <= 96)
-        PGPU_KNN_CASE(3);
-    else if (K <= 128)
-        PGPU_KNN_CASE(4);
-    else if (K <= 192)
-        PGPU_KNN_CASE(6);
-    else
-        PGPU_KNN_CASE(8);
-#undef PGPU_KNN_CASE
-    count_launches(1);
-    return cudaGetLastError();
 }
 
 }  // namespace
 
+// Offset table: every (dx, dy, dz) with |d|_inf <= R, sorted by the lower bound
+// sum_a max(|d_a| - 1, 0)^2 (bin units), then by Chebyshev ring, then by index.
+cudaError_t build_knn_table(pgpu_ctx* c) {
+    const int D = c->prm.dim;
+    const int R = D == 2 ? TABLE_R2 : TABLE_R3;
+    struct E {
+        int lb, ring, order, packed;
+    };
+    std::vector<E> es;
+    int order = 0;
+    for (int dz = (D == 3 ? -R : 0); dz <= (D == 3 ? R : 0); dz++)
+        for (int dy = -R; dy <= R; dy++)
+            for (int dx = -R; dx <= R; dx++) {
+                auto g = [](int d) { return std::max(std::abs(d) - 1, 0); };
+                E e;
+                e.lb = g(dx) * g(dx) + g(dy) * g(dy) + g(dz) * g(dz);
+                e.ring = std::max(std::abs(dx), std::max(std::abs(dy), std::abs(dz)));
+                e.order = order++;
+                e.packed = (dx & 255) | ((dy & 255) << 8) | ((dz & 255) << 16);
+                es.push_back(e);
+            }
+    std::sort(es.begin(), es.end(), [](const E& a, const E& b) {
+        if (a.lb != b.lb) return a.lb < b.lb;
+        if (a.ring != b.ring) return a.ring < b.ring;
+        return a.order < b.order;
+    });
+    std::vector<int2> host(es.size());
+    for (size_t i = 0; i < es.size(); i++) host[i] = make_int2(es[i].packed, es[i].lb);
+    cudaError_t e = cudaSuccess;
+    int2* d = ensure<int2>(c->knn_table, host.size(), &e);
+    if (e) return e;
+    if ((e = cudaMemcpyAsync(d, host.data(), host.size() * sizeof(int2), cudaMemcpyHostToDevice, c->stream))) return e;
+    c->knn_table_n = (int)host.size();
+    c->knn_table_r = R;
+    return cudaStreamSynchronize(c->stream);
+}
+
 cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, uint32_t* out) {
+    if (nq <= 0) return cudaSuccess;
+    cudaError_t e = cudaSuccess;
+    if (c->knn_table_n == 0 && (e = build_knn_table(c))) return e;
     DevScalars* sc = (DevScalars*)c->scalars.p;
-    unsigned long long* cc = &sc->knn_cand;
-    return c->prm.dim == 2 ? knn_dispatch<2>(c, qs, nq, K, out, cc) : knn_dispatch<3>(c, qs, nq, K, out, cc);
+    const unsigned blocks = (unsigned)((nq + KNN_WARPS - 1) / KNN_WARPS);
+    const uint32_t* perm = (const uint32_t*)c->perm.p;
+    const uint32_t* bs = (const uint32_t*)c->bin_start.p;
+    const int2* tab = (const int2*)c->knn_table.p;
+    if (c->prm.dim == 2)
+        k_knn<2><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double2*)c->spts.p, perm, bs, c->grid_G, tab,
+                                                           c->knn_table_n, c->knn_table_r, qs, nq, K, out,
+                                                           &sc->knn_cand);
+    else
+        k_knn<3><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double4*)c->spts.p, perm, bs, c->grid_G, tab,
+                                                           c->knn_table_n, c->knn_table_r, qs, nq, K, out,
+                                                           &sc->knn_cand);
+    count_launches(1);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_knn(pgpu_ctx* c) {

@@ -71,6 +71,8 @@ struct pgpu_ctx {
     pgpu::DevBuf vol, fptr, fcnt, status, certk, centroid;  // per cell, indexed by ext id
     pgpu::DevBuf f_nb, f_own, f_geo;  // faces: ext id, owner|code, (normal, area)
     pgpu::DevBuf scan_tmp;     // scan block sums
+    pgpu::DevBuf knn_table;    // neighbour-bin offsets sorted by lower-bound distance (int2)
+    int knn_table_n = 0, knn_table_r = 0;
     pgpu::DevBuf scalars;      // DevScalars
     // hydro state
     pgpu::DevBuf rho, vel, energy, rho2, vel2, energy2;  // primitives (drop-in hydro)

@@ -14,12 +14,16 @@ TOL = {
 }
 
 
-def rel_err(a, b):
+def rel_err(a, b, floor_frac=1e-9):
+    """max |a - b| / max(|b|, floor), floor = floor_frac x median |b|: relative error,
+    except for values that are zero up to rounding (degenerate faces of mirror-symmetric
+    point sets), where only an absolute error far below the typical magnitude is meaningful."""
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     if a.size == 0:
         return 0.0
-    return float((np.abs(a - b) / np.maximum(np.abs(b), 1e-300)).max())
+    floor = max(floor_frac * float(np.median(np.abs(b))), 1e-300)
+    return float((np.abs(a - b) / np.maximum(np.abs(b), floor)).max())
 
 
 def status_pairs(g, o):
