@@ -64,6 +64,7 @@ def parse():
     ap.add_argument("--config", choices=sorted(CONFIGS), default="sedov3d_1m")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the end-to-end leg")
+    ap.add_argument("--skip-forms", action="store_true", help="omit the FP32-clipping form beside the plain one")
     return ap.parse_args()
 
 
@@ -257,6 +258,42 @@ def run_ours(args, rank, world, local_rank):
                "d2h_bytes_per_step": nbytes, "steps": ke,
                "path": "pgpu_sim_step_host (C ABI), pinned host state in/out every step"}
 
+    # the precision form: FP32 local-frame clipping, same mesh (timed on the same state)
+    forms = None
+    if not args.skip_forms:
+        x, m_, p_, e_ = ctx.sim_get()
+        with Context(dim=cfg["dim"], k=cfg["k"], buff=cfg["buff"], boundary=cfg["boundary"], flux="physical",
+                     gamma=ic.gamma, device=local_rank, precision="fp32") as c32:
+            c32.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+            c32.sim_set(x, m_, p_, e_)
+            for _ in range(max(args.warmup, 1)):
+                c32.sim_step(cfg["cfl"], want_dt=False)
+            c32.enable_timing(True)
+            c32.sim_step(cfg["cfl"], want_dt=False)
+            st32 = c32.stage_times()
+            c32.enable_timing(False)
+            s32 = torch.cuda.ExternalStream(c32.stream)
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(s32)
+            for _ in range(args.steps):
+                c32.sim_step(cfg["cfl"], want_dt=False)
+            f1.record(s32)
+            torch.cuda.synchronize()
+            ms32 = f0.elapsed_time(f1)
+            if dist:
+                t = torch.tensor([ms32], device="cuda")
+                dist.all_reduce(t, op=dist.ReduceOp.MAX)
+                ms32 = float(t.item())
+            stats32 = c32.stats()
+        v32 = ic.n * args.steps * world / (ms32 / 1e3)
+        forms = {"plain_fp64": {"value": value, "ms_per_step": ms / args.steps},
+                 "fp32_clip": {"value": v32, "ms_per_step": ms32 / args.steps,
+                               "stages_ms": dict(zip(STAGES, st32)), "reclip_cells": stats32["reclip_cells"],
+                               "speedup_vs_plain": v32 / value}}
+
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -316,7 +353,7 @@ def run_ours(args, rank, world, local_rank):
                    "parallelism": f"replicas x{world}"},
         "roofline": roof, "roofline_hydro": roof_hydro,
         "stages_ms": dict(zip(STAGES, stage)),
-        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "forms": forms,
         "clocks": clk.summary(),
         "mesh": {"n_ext": stats["n_ext"], "faces": stats["num_faces"], "cert_k_max": stats["cert_k_max"],
                  "failed_cells": stats["failed_cells"], "knn_candidates_per_query":

@@ -51,6 +51,12 @@ extern "C" {
 #define PGPU_PRED_ROBUST 1    /* the vertex is kept (treated as not cut); needed for mirror walls,
                                  whose symmetric point sets make exact degeneracies */
 
+/* clipping precision (extension): FP32 clips in a frame centred on each seed with an
+ * error-bounded predicate, hands undecided cells to the FP64 kernel, and extracts
+ * certified cells in FP64 -- same topology, statuses and geometry as FP64 */
+#define PGPU_CLIP_FP64 0
+#define PGPU_CLIP_FP32 1
+
 /* cell status codes: the reference's Status enum, src/global/allvars.h:13-20 */
 #define PGPU_TRIANGLE_OVERFLOW 0
 #define PGPU_VERTEX_OVERFLOW 1
@@ -74,6 +80,7 @@ typedef struct {
     int predicates;   /* PGPU_PRED_REFERENCE or PGPU_PRED_ROBUST */
     int k_fallback;   /* moving-mesh steps only: hydro cells whose certificate does not close
                          within k neighbours are recomputed with this budget (0 = off; k < k_fallback <= 256) */
+    int precision;    /* PGPU_CLIP_FP64 or PGPU_CLIP_FP32 */
 } pgpu_params;
 
 /* Fills p with the reference's defaults: dim 3, K 190, periodic, reference flux,
@@ -179,6 +186,7 @@ typedef struct {
     int32_t n_grid;
     int64_t refit_cells;        /* cells recomputed with k_fallback in the last step */
     int64_t uncertified_cells;  /* hydro cells still without a certificate after it */
+    int64_t reclip_cells;       /* cells the FP32 clip handed to the FP64 clip in the last step */
 } pgpu_stats;
 
 /* Statistics of the last step (synchronises the stream). */

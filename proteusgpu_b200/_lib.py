@@ -31,7 +31,7 @@ EXPORTED = [
 class Params(C.Structure):
     _fields_ = [("dim", C.c_int), ("k", C.c_int), ("boundary", C.c_int), ("flux_mode", C.c_int),
                 ("buff", C.c_double), ("gamma", C.c_double), ("device", C.c_int), ("verbose", C.c_int),
-                ("predicates", C.c_int), ("k_fallback", C.c_int)]
+                ("predicates", C.c_int), ("k_fallback", C.c_int), ("precision", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -39,7 +39,8 @@ class Stats(C.Structure):
                 ("failed_cells", C.c_int64), ("box_faces", C.c_int64), ("unpaired_faces", C.c_int64),
                 ("knn_candidates", C.c_int64), ("last_dt", C.c_double), ("total_mass", C.c_double),
                 ("total_energy", C.c_double), ("total_mom", C.c_double * 3), ("cert_k_max", C.c_int32),
-                ("n_grid", C.c_int32), ("refit_cells", C.c_int64), ("uncertified_cells", C.c_int64)]
+                ("n_grid", C.c_int32), ("refit_cells", C.c_int64), ("uncertified_cells", C.c_int64),
+                ("reclip_cells", C.c_int64)]
 
 
 _LIB = None

@@ -61,11 +61,13 @@ class Context:
     "physical" (outward normal, face-pair-symmetric area).  predicates:
     "reference" (a near-degenerate predicate fails the cell, cell.cpp:216-218) or
     "robust" (the vertex is kept).  k_fallback: moving-mesh steps recompute cells
-    whose certificate does not close within k neighbours with this budget."""
+    whose certificate does not close within k neighbours with this budget.
+    precision: "fp64" (the reference's arithmetic) or "fp32" (local-frame FP32 clipping,
+    FP64 re-clip of undecided cells, FP64 extraction; same mesh)."""
 
     def __init__(self, dim: int = 3, k: int = 190, boundary: str = "periodic", flux: str = "reference",
                  buff: float = 0.04, gamma: float = 5.0 / 3.0, device: int = 0, predicates: str = "reference",
-                 k_fallback: int = 0):
+                 k_fallback: int = 0, precision: str = "fp64"):
         L = _lib.load()
         p = _lib.Params()
         L.pgpu_default_params(C.byref(p))
@@ -74,6 +76,7 @@ class Context:
         p.flux_mode = {"reference": 0, "physical": 1}[flux]
         p.predicates = {"reference": 0, "robust": 1}[predicates]
         p.k_fallback = k_fallback
+        p.precision = {"fp64": 0, "fp32": 1}[precision]
         h = C.c_void_p()
         rc = L.pgpu_create(C.byref(p), C.byref(h))
         if rc != 0:

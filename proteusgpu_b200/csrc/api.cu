@@ -140,6 +140,7 @@ int pgpu_create(const pgpu_params* p, pgpu_ctx** out) {
     if (p->boundary != PGPU_PERIODIC && p->boundary != PGPU_REFLECTIVE) return PGPU_EINVAL;
     if (p->flux_mode != PGPU_FLUX_REFERENCE && p->flux_mode != PGPU_FLUX_PHYSICAL) return PGPU_EINVAL;
     if (p->predicates != PGPU_PRED_REFERENCE && p->predicates != PGPU_PRED_ROBUST) return PGPU_EINVAL;
+    if (p->precision != PGPU_CLIP_FP64 && p->precision != PGPU_CLIP_FP32) return PGPU_EINVAL;
     if (p->k_fallback != 0 && (p->k_fallback <= p->k || p->k_fallback > pgpu::MAX_K)) return PGPU_EINVAL;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) return PGPU_ECUDA;
@@ -582,6 +583,7 @@ int pgpu_sim_stats(pgpu_ctx* c, pgpu_stats* out) {
     out->cert_k_max = h.cert_k_max;
     out->n_grid = c->grid_G;
     out->refit_cells = c->n_refit;
+    out->reclip_cells = c->n_reclip;
     out->uncertified_cells = c->n_uncertified;
     return PGPU_OK;
 }

@@ -52,6 +52,8 @@ struct WarpCell {
         struct {
             unsigned long long emask[MAX_P];
             unsigned char nxt[MAX_P];
+            float4 hp32[MAX_P];   // FP32 local-frame planes (k_clip32)
+            float vd2f[MAX_T];    // FP32 squared vertex distances (k_clip32)
         } b;
         double vpos[MAX_T][3];
     } u;
@@ -152,6 +154,7 @@ __device__ __forceinline__ double max_vd2(const WarpCell& W, int n, int lane, co
 
 struct ClipParams {
     const uint32_t* qs;
+    const uint32_t* slots;  // optional: work item t is query slot slots[t] (lists of qs/knn reused)
     const uint32_t* perm;
     const void* spts;
     const void* ext;
@@ -163,6 +166,7 @@ struct ClipParams {
     int K;
     int robust;
     unsigned int* uncertified;  // hydro cells ending with SECURITY_RADIUS_NOT_REACHED
+    unsigned int* reclip;       // cells the FP32 kernel hands to the FP64 kernel
     double vscale, ascale, scale;  // unit box -> physical
     double* vol;
     uint32_t* fptr;
@@ -178,6 +182,244 @@ struct ClipParams {
     unsigned long long face_cap;
 };
 
+// Cell outputs of a cell that was not extracted (the reference leaves volume 0
+// and no faces, voronoi.cpp:236-238).
+__device__ __forceinline__ void store_failed(const ClipParams& P, int lane, uint32_t e, int status) {
+    if (lane == 0) {
+        if (status == ST_SECURITY_RADIUS_NOT_REACHED && (int64_t)e < P.n_hydro) atomicAdd(P.uncertified, 1u);
+        P.vol[e] = 0.0;
+        P.fptr[e] = 0;
+        P.fcnt[e] = 0;
+        P.status[e] = status;
+        P.certk[e] = 0;
+        P.centroid[3 * (size_t)e] = P.centroid[3 * (size_t)e + 1] = P.centroid[3 * (size_t)e + 2] = 0.0;
+    }
+}
+
+// Extraction (cell.cpp:416-669) of a certified cell held in W with FP64 planes:
+// vertices, faces in plane order, areas, volume, centroid; faces written at a
+// reserved slot, cell outputs at extended id e.
+template <int D>
+__device__ __forceinline__ void compute_vpos(WarpCell& W, int lane, int nb_t) {
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        int i = lane + 32 * j;
+        if (i < nb_t) vertex_pos<D>(W.hp, W.tri[i], W.u.vpos[i][0], W.u.vpos[i][1], W.u.vpos[i][2]);
+    }
+    __syncwarp();
+}
+
+template <int D>
+__device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams& P, int w, int lane, int nb_v, int nb_t,
+                                                  uint32_t e, int certk, double sx, double sy, double sz,
+                                                  bool vpos_ready = false) {
+    if (!vpos_ready) compute_vpos<D>(W, lane, nb_t);
+
+    double cell_vol = 0.0, cen[3] = {0.0, 0.0, 0.0};
+    if (D == 2) {
+        // compute_cell_area_2d (cell.cpp:475-498): vertices ordered by angle about their mean
+        double cx = 0, cy = 0;
+        for (int i = 0; i < nb_t; i++) cx += W.u.vpos[i][0], cy += W.u.vpos[i][1];
+        cx /= nb_t;
+        cy /= nb_t;
+        // rank of each vertex by angle; lane-parallel, then lane 0 sums in order
+        __shared__ unsigned char order_s[CLIP_WARPS][MAX_T];
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            int i = lane + 32 * j;
+            if (i < nb_t) W.vd2[i] = atan2(W.u.vpos[i][1] - cy, W.u.vpos[i][0] - cx);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            int i = lane + 32 * j;
+            if (i < nb_t) {
+                const double ai = W.vd2[i];
+                int rank = 0;
+                for (int q = 0; q < nb_t; q++) {
+                    const double aq = W.vd2[q];
+                    rank += (aq < ai || (aq == ai && q < i)) ? 1 : 0;
+                }
+                order_s[w][rank] = (unsigned char)i;
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            double a = 0, mx = 0, my = 0, sa = 0;
+            for (int i = 0; i < nb_t; i++) {
+                int j = (i + 1) % nb_t;
+                const double* pp = W.u.vpos[order_s[w][i]];
+                const double* qq = W.u.vpos[order_s[w][j]];
+                a += pp[0] * qq[1];
+                a -= qq[0] * pp[1];
+                double cr = (pp[0] - cx) * (qq[1] - cy) - (qq[0] - cx) * (pp[1] - cy);
+                mx += (pp[0] + qq[0] - 2 * cx) * cr;
+                my += (pp[1] + qq[1] - 2 * cy) * cr;
+                sa += cr;
+            }
+            cell_vol = fabs(a) / 2.0;
+            cen[0] = cx + mx / (3.0 * sa);
+            cen[1] = cy + my / (3.0 * sa);
+        }
+    }
+
+    // faces: lane handles planes p = lane and p = lane + 32
+    bool valid[2] = {false, false};
+    double area[2] = {0.0, 0.0};
+#pragma unroll
+    for (int pass = 0; pass < 2; pass++) {
+        const int p = lane + 32 * pass;
+        if (p >= nb_v) continue;
+        if (D == 2) {
+            int cnt = 0, v0 = -1, v1 = -1;
+            for (int i = 0; i < nb_t; i++) {
+                uint32_t tv = W.tri[i];
+                if ((int)tri_a(tv) == p || (int)tri_b(tv) == p) {
+                    if (cnt == 0) v0 = i; else if (cnt == 1) v1 = i;
+                    cnt++;
+                }
+            }
+            if (cnt >= 2) {
+                double ddx = W.u.vpos[v1][0] - W.u.vpos[v0][0];
+                double ddy = W.u.vpos[v1][1] - W.u.vpos[v0][1];
+                area[pass] = sqrt(ddx * ddx + ddy * ddy);
+                valid[pass] = true;
+            }
+        } else {
+            unsigned char fa[FACE_MAX_V], fb[FACE_MAX_V], fi[FACE_MAX_V];
+            int cnt = 0;
+            bool over = false;
+            for (int i = 0; i < nb_t; i++) {
+                uint32_t tv = W.tri[i];
+                uint32_t a = tri_a(tv), b = tri_b(tv), c = tri_c(tv);
+                uint32_t x, y;
+                if ((int)a == p) x = b, y = c;
+                else if ((int)b == p) x = c, y = a;
+                else if ((int)c == p) x = a, y = b;
+                else continue;
+                if (cnt < FACE_MAX_V) {
+                    fa[cnt] = (unsigned char)x;
+                    fb[cnt] = (unsigned char)y;
+                    fi[cnt] = (unsigned char)i;
+                } else {
+                    over = true;
+                }
+                cnt++;
+            }
+            double fv = 0.0, fc0 = 0.0, fc1 = 0.0, fc2 = 0.0;
+            if (cnt >= 3 && !over) {
+                // Walk the polygon: after vertex (p, a, b) comes (p, b, c).  Fan
+                // triangles (v0, v_{i-1}, v_i) give the area and, with the seed,
+                // the signed volume and first moment (cell.cpp:611-627).
+                const double* v0 = W.u.vpos[fi[0]];
+                const double a0 = v0[0] - sx, a1 = v0[1] - sy, a2 = v0[2] - sz;
+                int curv = 0;
+                double meas = 0.0;
+                bool ok = true;
+                for (int st = 1; st < cnt; st++) {
+                    int nx = -1;
+                    for (int q = 1; q < cnt; q++)
+                        if (fa[q] == fb[curv]) {
+                            nx = q;
+                            break;
+                        }
+                    if (nx < 0) {
+                        ok = false;
+                        break;
+                    }
+                    if (st >= 2) {
+                        const double* vi = W.u.vpos[fi[curv]];
+                        const double* vj = W.u.vpos[fi[nx]];
+                        double e1x = vi[0] - v0[0], e1y = vi[1] - v0[1], e1z = vi[2] - v0[2];
+                        double e2x = vj[0] - v0[0], e2y = vj[1] - v0[1], e2z = vj[2] - v0[2];
+                        double crx = e1y * e2z - e1z * e2y;
+                        double cry = e1z * e2x - e1x * e2z;
+                        double crz = e1x * e2y - e1y * e2x;
+                        meas += 0.5 * sqrt(crx * crx + cry * cry + crz * crz);
+                        double b0 = vi[0] - sx, b1 = vi[1] - sy, b2 = vi[2] - sz;
+                        double c0 = vj[0] - sx, c1 = vj[1] - sy, c2 = vj[2] - sz;
+                        double x0 = b1 * c2 - b2 * c1;
+                        double x1 = b2 * c0 - b0 * c2;
+                        double x2 = b0 * c1 - b1 * c0;
+                        double tv = (a0 * x0 + a1 * x1 + a2 * x2) / 6.0;
+                        fv += tv;
+                        fc0 += tv * (a0 + b0 + c0) * 0.25;
+                        fc1 += tv * (a1 + b1 + c1) * 0.25;
+                        fc2 += tv * (a2 + b2 + c2) * 0.25;
+                    }
+                    curv = nx;
+                }
+                if (ok && fb[curv] != fa[0]) ok = false;  // the walk must close on v0
+                if (ok) {
+                    valid[pass] = true;
+                    area[pass] = meas;
+                }
+            }
+            W.fvol[p] = valid[pass] ? fv : 0.0;
+            W.fcen[p][0] = valid[pass] ? fc0 : 0.0;
+            W.fcen[p][1] = valid[pass] ? fc1 : 0.0;
+            W.fcen[p][2] = valid[pass] ? fc2 : 0.0;
+        }
+    }
+    const uint32_t vb0 = __ballot_sync(FULL, valid[0]);
+    const uint32_t vb1 = __ballot_sync(FULL, valid[1]);
+    const int nf = __popc(vb0) + __popc(vb1);
+    __syncwarp();
+    if (D == 3 && lane == 0) {
+        for (int p = 0; p < nb_v; p++) {  // plane order, as the reference accumulates
+            cell_vol += W.fvol[p];
+            cen[0] += W.fcen[p][0];
+            cen[1] += W.fcen[p][1];
+            cen[2] += W.fcen[p][2];
+        }
+        const double sv = cell_vol;
+        cell_vol = fabs(sv);
+        cen[0] = sx + cen[0] / sv;
+        cen[1] = sy + cen[1] / sv;
+        cen[2] = sz + cen[2] / sv;
+    }
+    unsigned long long base = 0;
+    if (lane == 0) base = atomicAdd(P.face_counter, (unsigned long long)nf);
+    base = __shfl_sync(FULL, base, 0);
+    const bool fits = base + (unsigned long long)nf <= P.face_cap;
+    if (!fits) {
+        if (lane == 0) atomicOr(P.overflow, 1u);
+    } else {
+#pragma unroll
+        for (int pass = 0; pass < 2; pass++) {
+            if (!valid[pass]) continue;
+            const int p = lane + 32 * pass;
+            const uint32_t vb = pass == 0 ? vb0 : vb1;
+            const int idx = (pass == 0 ? 0 : __popc(vb0)) + __popc(vb & ((1u << lane) - 1u));
+            const size_t f = base + idx;
+            const double4 pe = W.hp[p];
+            const double nlen = sqrt(pe.x * pe.x + pe.y * pe.y + pe.z * pe.z);  // compute_face_normal
+            const int nbr = W.vid[p];
+            P.f_nb[f] = nbr;
+            uint32_t own = BOX_FACE;
+            if (nbr >= 0) {
+                if ((int64_t)nbr < P.n_hydro)
+                    own = pack_owner((uint32_t)nbr, 0);
+                else
+                    own = pack_owner(P.ghost_src[nbr - P.n_hydro], P.ghost_code[nbr - P.n_hydro]);
+            }
+            P.f_own[f] = own;
+            P.f_geo[f] = make_double4(pe.x / nlen, pe.y / nlen, pe.z / nlen, P.ascale * area[pass]);
+        }
+    }
+    if (lane == 0) {
+        P.vol[e] = P.vscale * cell_vol;
+        P.fptr[e] = fits ? (uint32_t)base : 0u;
+        P.fcnt[e] = fits ? (uint32_t)nf : 0u;
+        P.status[e] = ST_SUCCESS;
+        P.certk[e] = certk;
+        P.centroid[3 * (size_t)e] = (cen[0] - 0.5) * P.scale + 0.5;
+        P.centroid[3 * (size_t)e + 1] = (cen[1] - 0.5) * P.scale + 0.5;
+        P.centroid[3 * (size_t)e + 2] = D == 3 ? (cen[2] - 0.5) * P.scale + 0.5 : 0.0;
+    }
+}
+
 template <int D>
 __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
     using PT = typename PointOf<D>::type;
@@ -188,12 +430,13 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
     WarpCell& W = cells[w];
     const PT* spts = (const PT*)P.spts;
     const PT* ext = (const PT*)P.ext;
-    const uint32_t s = P.qs[t];
+    const int64_t tq = P.slots ? (int64_t)P.slots[t] : t;
+    const uint32_t s = P.qs[tq];
     const uint32_t e = P.perm[s];
     const PT sp = spts[s];
     const double sx = sp.x, sy = sp.y, sz = pz(sp);
     const int K = P.K;
-    const uint32_t* kl = P.knn + (size_t)t * K;
+    const uint32_t* kl = P.knn + (size_t)tq * K;
 
     // ---- ConvexCell::ConvexCell (cell.cpp:42-104): bounding box [-1e-14, 1 + 1e-14]^D
     const double beps = 1e-14;
@@ -464,229 +707,456 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
         }
     }
     if (status != ST_SUCCESS) {
-        if (lane == 0) {
-            if (status == ST_SECURITY_RADIUS_NOT_REACHED && (int64_t)e < P.n_hydro) atomicAdd(P.uncertified, 1u);
-            P.vol[e] = 0.0;
-            P.fptr[e] = 0;
-            P.fcnt[e] = 0;
-            P.status[e] = status;
-            P.certk[e] = 0;
-            P.centroid[3 * (size_t)e] = P.centroid[3 * (size_t)e + 1] = P.centroid[3 * (size_t)e + 2] = 0.0;
-        }
+        store_failed(P, lane, e, status);
         return;
     }
+    extract_and_store<D>(W, P, w, lane, nb_v, nb_t, e, certk, sx, sy, sz);
+}
 
-    // ---- extraction (cell.cpp:416-669)
-    __syncwarp();
+
+// ============================================================================
+// FP32 local-frame clipping (BASELINE's precision form).  The cell is clipped
+// in single precision in a frame centred on its seed: a neighbour b = B - seed
+// gives the plane (-b, |b|^2 / 2), the box planes get w + n.seed.  Every
+// plane-vertex determinant is accepted only when it exceeds a bound on its
+// rounding error, 64 u times the permanent of the absolute entries (u = 2^-24);
+// otherwise, and on any overflow or inconsistent cavity, the cell is handed to
+// the FP64 kernel (status ST_RECLIP).  Certified cells are extracted in FP64:
+// the plane equations are recomputed from the points with the reference's
+// formula, vertices follow in FP64 from the same triples, and the security
+// radius is checked again in FP64 over the final vertex set, which also yields
+// the exact certified K.  A cell whose FP64 check disagrees is re-clipped.  So
+// topology, statuses and geometry are those of the FP64 path.
+// ============================================================================
+
+constexpr int ST_RECLIP = 7;
+constexpr float F32_BOUND = 64.0f * 5.9604645e-8f;
+
+__device__ __forceinline__ float det2f(float a11, float a12, float a21, float a22) {
+    return fmaf(a11, a22, -(a12 * a21));
+}
+__device__ __forceinline__ float per2f(float a11, float a12, float a21, float a22) {
+    return fabsf(a11 * a22) + fabsf(a12 * a21);
+}
+__device__ __forceinline__ float det3f(float a11, float a12, float a13, float a21, float a22, float a23, float a31,
+                                       float a32, float a33) {
+    float t = a11 * det2f(a22, a23, a32, a33);
+    t = fmaf(-a21, det2f(a12, a13, a32, a33), t);
+    return fmaf(a31, det2f(a12, a13, a22, a23), t);
+}
+__device__ __forceinline__ float per3f(float a11, float a12, float a13, float a21, float a22, float a23, float a31,
+                                       float a32, float a33) {
+    return fabsf(a11) * per2f(a22, a23, a32, a33) + fabsf(a21) * per2f(a12, a13, a32, a33) +
+           fabsf(a31) * per2f(a12, a13, a22, a23);
+}
+
+// det4 of the reference's expansion and its permanent, single precision.
+__device__ __forceinline__ void det4f(float a11, float a12, float a13, float a14, float a21, float a22, float a23,
+                                      float a24, float a31, float a32, float a33, float a34, float a41, float a42,
+                                      float a43, float a44, float& det, float& per) {
+    const float m12 = fmaf(a21, a12, -(a11 * a22)), p12 = fabsf(a21 * a12) + fabsf(a11 * a22);
+    const float m13 = fmaf(a31, a12, -(a11 * a32)), p13 = fabsf(a31 * a12) + fabsf(a11 * a32);
+    const float m14 = fmaf(a41, a12, -(a11 * a42)), p14 = fabsf(a41 * a12) + fabsf(a11 * a42);
+    const float m23 = fmaf(a31, a22, -(a21 * a32)), p23 = fabsf(a31 * a22) + fabsf(a21 * a32);
+    const float m24 = fmaf(a41, a22, -(a21 * a42)), p24 = fabsf(a41 * a22) + fabsf(a21 * a42);
+    const float m34 = fmaf(a41, a32, -(a31 * a42)), p34 = fabsf(a41 * a32) + fabsf(a31 * a42);
+    const float m123 = fmaf(m12, a33, fmaf(m23, a13, -(m13 * a23)));
+    const float m124 = fmaf(m12, a43, fmaf(m24, a13, -(m14 * a23)));
+    const float m134 = fmaf(m13, a43, fmaf(m34, a13, -(m14 * a33)));
+    const float m234 = fmaf(m23, a43, fmaf(m34, a23, -(m24 * a33)));
+    const float q123 = p23 * fabsf(a13) + p13 * fabsf(a23) + p12 * fabsf(a33);
+    const float q124 = p24 * fabsf(a13) + p14 * fabsf(a23) + p12 * fabsf(a43);
+    const float q134 = p34 * fabsf(a13) + p14 * fabsf(a33) + p13 * fabsf(a43);
+    const float q234 = p34 * fabsf(a23) + p24 * fabsf(a33) + p23 * fabsf(a43);
+    det = fmaf(-m123, a44, fmaf(m124, a34, fmaf(m234, a14, -(m134 * a24))));
+    per = q234 * fabsf(a14) + q134 * fabsf(a24) + q124 * fabsf(a34) + q123 * fabsf(a44);
+}
+
+// 0 = not in conflict, 1 = in conflict, 2 = undecided in FP32
+template <int D>
+__device__ __forceinline__ int conflict_f(const float4* hp, uint32_t t, const float4& e) {
+    const float4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)];
+    float det, per;
+    if (D == 2) {
+        det = det3f(p1.x, p2.x, e.x, p1.y, p2.y, e.y, p1.w, p2.w, e.w);
+        per = per3f(p1.x, p2.x, e.x, p1.y, p2.y, e.y, p1.w, p2.w, e.w);
+    } else {
+        const float4 p3 = hp[tri_c(t)];
+        det4f(p1.x, p2.x, p3.x, e.x, p1.y, p2.y, p3.y, e.y, p1.z, p2.z, p3.z, e.z, p1.w, p2.w, p3.w, e.w, det, per);
+    }
+    if (!(fabsf(det) > F32_BOUND * per)) return 2;
+    return det > 0.0f ? 1 : 0;
+}
+
+// Squared distance of a vertex to the seed (the origin of the local frame).
+template <int D>
+__device__ __forceinline__ float vertex_d2f(const float4* hp, uint32_t t) {
+    const float4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)];
+    if (D == 2) {
+        const float rx = -det2f(p1.w, p1.y, p2.w, p2.y);
+        const float ry = -det2f(p1.x, p1.w, p2.x, p2.w);
+        const float rw = det2f(p1.x, p1.y, p2.x, p2.y);
+        const float x = rx / rw, y = ry / rw;
+        return fmaf(x, x, y * y);
+    }
+    const float4 p3 = hp[tri_c(t)];
+    const float rx = -det3f(p1.w, p1.y, p1.z, p2.w, p2.y, p2.z, p3.w, p3.y, p3.z);
+    const float ry = -det3f(p1.x, p1.w, p1.z, p2.x, p2.w, p2.z, p3.x, p3.w, p3.z);
+    const float rz = -det3f(p1.x, p1.y, p1.w, p2.x, p2.y, p2.w, p3.x, p3.y, p3.w);
+    const float rw = det3f(p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z);
+    const float x = rx / rw, y = ry / rw, z = rz / rw;
+    return fmaf(x, x, fmaf(y, y, z * z));
+}
+
+__device__ __forceinline__ float nan_maxf(float a, float b) { return (a != a || b != b) ? (a + b) : fmaxf(a, b); }
+
+__device__ __forceinline__ float warp_maxf(float v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = nan_maxf(v, __shfl_xor_sync(FULL, v, o));
+    return v;
+}
+
+__device__ __forceinline__ float max_vd2f(const WarpCell& W, int n, int lane) {
+    float m = 0.0f;
 #pragma unroll
     for (int j = 0; j < 3; j++) {
-        int i = lane + 32 * j;
-        if (i < nb_t) vertex_pos<D>(W.hp, W.tri[i], W.u.vpos[i][0], W.u.vpos[i][1], W.u.vpos[i][2]);
+        const int i = lane + 32 * j;
+        if (i < n) m = nan_maxf(m, W.u.b.vd2f[i]);
+    }
+    return warp_maxf(m);
+}
+
+// The reference's FP64 plane p of the cell (box planes, or the bisector with
+// extended point vid), global coordinates (cell.cpp:75-82, 164-168).
+template <int D>
+__device__ __forceinline__ double4 plane64(int p, int vid, const typename PointOf<D>::type* ext, double sx, double sy,
+                                           double sz) {
+    const double beps = 1e-14, xmin = -beps, xmax = 1.0 + beps;
+    if (vid < 0) {
+        switch (p) {
+            case 0: return make_double4(1.0, 0.0, 0.0, -xmin);
+            case 1: return make_double4(-1.0, 0.0, 0.0, xmax);
+            case 2: return make_double4(0.0, 1.0, 0.0, -xmin);
+            case 3: return make_double4(0.0, -1.0, 0.0, xmax);
+            case 4: return make_double4(0.0, 0.0, 1.0, -xmin);
+            default: return make_double4(0.0, 0.0, -1.0, xmax);
+        }
+    }
+    const typename PointOf<D>::type B = ext[vid];
+    const double bx = B.x, by = B.y, bz = pz(B);
+    const double dx = sx - bx, dy = sy - by, dz = sz - bz;
+    const double ax = sx + bx, ay = sy + by, az = sz + bz;
+    const double dot = ax * dx + ay * dy + az * dz;
+    return make_double4(dx, dy, dz, -dot / 2.0);
+}
+
+template <int D>
+__global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip32(ClipParams P) {
+    using PT = typename PointOf<D>::type;
+    __shared__ WarpCell cells[CLIP_WARPS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t t = (int64_t)blockIdx.x * CLIP_WARPS + w;
+    if (t >= P.nq) return;  // warp-uniform
+    WarpCell& W = cells[w];
+    float4* hp = W.u.b.hp32;
+    const PT* spts = (const PT*)P.spts;
+    const PT* ext = (const PT*)P.ext;
+    const int64_t tq = P.slots ? (int64_t)P.slots[t] : t;
+    const uint32_t s = P.qs[tq];
+    const uint32_t e = P.perm[s];
+    const PT sp = spts[s];
+    const double sx = sp.x, sy = sp.y, sz = pz(sp);
+    const int K = P.K;
+    const uint32_t* kl = P.knn + (size_t)tq * K;
+
+    // bounding box in the local frame: w' = w + n . seed
+    const double beps = 1e-14;
+    const double xmin = -beps, xmax = 1.0 + beps;
+    if (lane < 2 * D) {
+        float4 pl;
+        switch (lane) {
+            case 0: pl = make_float4(1.f, 0.f, 0.f, (float)(sx - xmin)); break;
+            case 1: pl = make_float4(-1.f, 0.f, 0.f, (float)(xmax - sx)); break;
+            case 2: pl = make_float4(0.f, 1.f, 0.f, (float)(sy - xmin)); break;
+            case 3: pl = make_float4(0.f, -1.f, 0.f, (float)(xmax - sy)); break;
+            case 4: pl = make_float4(0.f, 0.f, 1.f, (float)(sz - xmin)); break;
+            default: pl = make_float4(0.f, 0.f, -1.f, (float)(xmax - sz)); break;
+        }
+        hp[lane] = pl;
+        W.vid[lane] = -1;
+    }
+    if (D == 3) {
+        W.u.b.emask[lane] = 0ull;
+        W.u.b.emask[lane + 32] = 0ull;
+    }
+    const int ntri0 = D == 2 ? 4 : 8;
+    if (lane < ntri0) {
+        uint32_t tv;
+        if (D == 2) {
+            const uint32_t t2[4] = {pack3(2, 0, 0), pack3(1, 2, 0), pack3(3, 1, 0), pack3(0, 3, 0)};
+            tv = t2[lane & 3];
+        } else {
+            const uint32_t t3[8] = {pack3(2, 5, 0), pack3(5, 3, 0), pack3(1, 5, 2), pack3(5, 1, 3),
+                                    pack3(4, 2, 0), pack3(4, 0, 3), pack3(2, 4, 1), pack3(4, 3, 1)};
+            tv = t3[lane & 7];
+        }
+        W.tri[lane] = tv;
     }
     __syncwarp();
+    if (lane < ntri0) W.u.b.vd2f[lane] = vertex_d2f<D>(hp, W.tri[lane]);
+    __syncwarp();
+    int nb_v = 2 * D, nb_t = ntri0;
+    bool reclip = false, certified = false;
+    int k_stop = 0, k_last = 0;
+    float v_dist = max_vd2f(W, nb_t, lane);
 
-    double cell_vol = 0.0, cen[3] = {0.0, 0.0, 0.0};
-    if (D == 2) {
-        // compute_cell_area_2d (cell.cpp:475-498): vertices ordered by angle about their mean
-        double cx = 0, cy = 0;
-        for (int i = 0; i < nb_t; i++) cx += W.u.vpos[i][0], cy += W.u.vpos[i][1];
-        cx /= nb_t;
-        cy /= nb_t;
-        // rank of each vertex by angle; lane-parallel, then lane 0 sums in order
-        __shared__ unsigned char order_s[CLIP_WARPS][MAX_T];
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            int i = lane + 32 * j;
-            if (i < nb_t) W.vd2[i] = atan2(W.u.vpos[i][1] - cy, W.u.vpos[i][0] - cx);
+    for (int k = 0; k < K; k++) {
+        const uint32_t z = kl[k];
+        if (z == NO_NEIGHBOR) break;
+        k_stop = k + 1;
+        const PT B = ext[z];
+        const double bx = B.x - sx, by = B.y - sy, bz = pz(B) - sz;  // local frame, exact in FP64
+        const float fx = (float)bx, fy = (float)by, fz = (float)bz;
+        const double d2B = seed_d2(B.x, B.y, pz(B), sx, sy, sz);
+        if (nb_v >= MAX_P) {
+            reclip = true;
+            break;
         }
+        const float4 eq = make_float4(-fx, -fy, -fz, 0.5f * fmaf(fx, fx, fmaf(fy, fy, fz * fz)));
+        const int cur = nb_v;
+        if (lane == 0) hp[cur] = eq;
         __syncwarp();
+
+        uint32_t cm[3];
+        bool undecided = false;
 #pragma unroll
         for (int j = 0; j < 3; j++) {
-            int i = lane + 32 * j;
+            const int i = lane + 32 * j;
+            bool cf = false;
             if (i < nb_t) {
-                const double ai = W.vd2[i];
-                int rank = 0;
-                for (int q = 0; q < nb_t; q++) {
-                    const double aq = W.vd2[q];
-                    rank += (aq < ai || (aq == ai && q < i)) ? 1 : 0;
-                }
-                order_s[w][rank] = (unsigned char)i;
+                const int c = conflict_f<D>(hp, W.tri[i], eq);
+                undecided |= c == 2;
+                cf = c == 1;
             }
+            cm[j] = __ballot_sync(FULL, cf);
         }
-        __syncwarp();
-        if (lane == 0) {
-            double a = 0, mx = 0, my = 0, sa = 0;
-            for (int i = 0; i < nb_t; i++) {
-                int j = (i + 1) % nb_t;
-                const double* pp = W.u.vpos[order_s[w][i]];
-                const double* qq = W.u.vpos[order_s[w][j]];
-                a += pp[0] * qq[1];
-                a -= qq[0] * pp[1];
-                double cr = (pp[0] - cx) * (qq[1] - cy) - (qq[0] - cx) * (pp[1] - cy);
-                mx += (pp[0] + qq[0] - 2 * cx) * cr;
-                my += (pp[1] + qq[1] - 2 * cy) * cr;
-                sa += cr;
+        if (__any_sync(FULL, undecided)) {
+            reclip = true;
+            break;
+        }
+        const int nb_r = __popc(cm[0]) + __popc(cm[1]) + __popc(cm[2]);
+        const uint32_t km[3] = {~cm[0], ~cm[1], ~cm[2]};
+        if (nb_r == 0) {
+            if ((float)d2B > 4.004f * v_dist) {
+                certified = true;
+                break;
             }
-            cell_vol = fabs(a) / 2.0;
-            cen[0] = cx + mx / (3.0 * sa);
-            cen[1] = cy + my / (3.0 * sa);
+            continue;
         }
-    }
-
-    // faces: lane handles planes p = lane and p = lane + 32
-    bool valid[2] = {false, false};
-    double area[2] = {0.0, 0.0};
-#pragma unroll
-    for (int pass = 0; pass < 2; pass++) {
-        const int p = lane + 32 * pass;
-        if (p >= nb_v) continue;
+        k_last = k + 1;
+        const int kept = nb_t - nb_r;
+        int n_new = 0;
+        bool bad = false;
+        uint32_t my_new[9];
+        int my_new_pos[9];
+        int my_new_cnt = 0;
         if (D == 2) {
-            int cnt = 0, v0 = -1, v1 = -1;
-            for (int i = 0; i < nb_t; i++) {
-                uint32_t tv = W.tri[i];
-                if ((int)tri_a(tv) == p || (int)tri_b(tv) == p) {
-                    if (cnt == 0) v0 = i; else if (cnt == 1) v1 = i;
-                    cnt++;
+            uint32_t lo = 0, hi = 0;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int i = lane + 32 * j;
+                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
+                    const uint32_t tv = W.tri[i];
+                    const uint32_t a = tri_a(tv), b = tri_b(tv);
+                    if (a < 32) lo ^= 1u << a; else hi ^= 1u << (a - 32);
+                    if (b < 32) lo ^= 1u << b; else hi ^= 1u << (b - 32);
                 }
             }
-            if (cnt >= 2) {
-                double ddx = W.u.vpos[v1][0] - W.u.vpos[v0][0];
-                double ddy = W.u.vpos[v1][1] - W.u.vpos[v0][1];
-                area[pass] = sqrt(ddx * ddx + ddy * ddy);
-                valid[pass] = true;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                lo ^= __shfl_xor_sync(FULL, lo, o);
+                hi ^= __shfl_xor_sync(FULL, hi, o);
+            }
+            const unsigned long long xm = (unsigned long long)lo | ((unsigned long long)hi << 32);
+            if (__popcll(xm) < 2) {
+                bad = true;
+            } else {
+                const int b0 = __ffsll((long long)xm) - 1;
+                const unsigned long long x2 = xm & (xm - 1);
+                const int b1 = __ffsll((long long)x2) - 1;
+                n_new = 2;
+                bool und = false;
+                if (lane < 2) {
+                    const int j = lane == 0 ? b0 : b1;
+                    const float4 hi_ = hp[cur], hj = hp[j];
+                    const float rw = det2f(hi_.x, hi_.y, hj.x, hj.y);
+                    und = !(fabsf(rw) > F32_BOUND * per2f(hi_.x, hi_.y, hj.x, hj.y));
+                    my_new[0] = rw > 0 ? pack3(j, cur, 0) : pack3(cur, j, 0);
+                    my_new_pos[0] = lane;
+                    my_new_cnt = 1;
+                }
+                if (__any_sync(FULL, und)) bad = true;
             }
         } else {
-            unsigned char fa[FACE_MAX_V], fb[FACE_MAX_V], fi[FACE_MAX_V];
-            int cnt = 0;
-            bool over = false;
-            for (int i = 0; i < nb_t; i++) {
-                uint32_t tv = W.tri[i];
-                uint32_t a = tri_a(tv), b = tri_b(tv), c = tri_c(tv);
-                uint32_t x, y;
-                if ((int)a == p) x = b, y = c;
-                else if ((int)b == p) x = c, y = a;
-                else if ((int)c == p) x = a, y = b;
-                else continue;
-                if (cnt < FACE_MAX_V) {
-                    fa[cnt] = (unsigned char)x;
-                    fb[cnt] = (unsigned char)y;
-                    fi[cnt] = (unsigned char)i;
-                } else {
-                    over = true;
+            unsigned long long* em = W.u.b.emask;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int i = lane + 32 * j;
+                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
+                    const uint32_t tv = W.tri[i];
+                    const uint32_t a = tri_a(tv), b = tri_b(tv), c = tri_c(tv);
+                    atomicOr(&em[a], 1ull << b);
+                    atomicOr(&em[b], 1ull << c);
+                    atomicOr(&em[c], 1ull << a);
                 }
-                cnt++;
             }
-            double fv = 0.0, fc0 = 0.0, fc1 = 0.0, fc2 = 0.0;
-            if (cnt >= 3 && !over) {
-                // Walk the polygon: after vertex (p, a, b) comes (p, b, c).  Fan
-                // triangles (v0, v_{i-1}, v_i) give the area and, with the seed,
-                // the signed volume and first moment (cell.cpp:611-627).
-                const double* v0 = W.u.vpos[fi[0]];
-                const double a0 = v0[0] - sx, a1 = v0[1] - sy, a2 = v0[2] - sz;
-                int curv = 0;
-                double meas = 0.0;
-                bool ok = true;
-                for (int st = 1; st < cnt; st++) {
-                    int nx = -1;
-                    for (int q = 1; q < cnt; q++)
-                        if (fa[q] == fb[curv]) {
-                            nx = q;
-                            break;
-                        }
-                    if (nx < 0) {
+            __syncwarp();
+            unsigned long long src = 0ull;
+            int base = 0;
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int i = lane + 32 * j;
+                const bool rem = i < nb_t && ((cm[j] >> lane) & 1u);
+                const uint32_t tv = rem ? W.tri[i] : 0u;
+                const uint32_t v3[3] = {tri_a(tv), tri_b(tv), tri_c(tv)};
+#pragma unroll
+                for (int ed = 0; ed < 3; ed++) {
+                    const uint32_t x = v3[ed], y = v3[(ed + 1) % 3];
+                    const bool isb = rem && !((em[y] >> x) & 1ull);
+                    const unsigned bal = __ballot_sync(FULL, isb);
+                    if (isb) {
+                        my_new[my_new_cnt] = pack3(cur, x, y);
+                        my_new_pos[my_new_cnt] = base + __popc(bal & ((1u << lane) - 1u));
+                        my_new_cnt++;
+                        src |= 1ull << x;
+                        W.u.b.nxt[x] = (unsigned char)y;
+                    }
+                    base += __popc(bal);
+                }
+            }
+            n_new = base;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) src |= __shfl_xor_sync(FULL, src, o);
+            __syncwarp();
+            bool ok = __popcll(src) == n_new && n_new >= 3;
+            if (ok && lane == 0) {
+                const int x0 = __ffsll((long long)src) - 1;
+                int x = x0;
+                for (int st = 1; st <= n_new; st++) {
+                    x = W.u.b.nxt[x];
+                    if (!((src >> x) & 1ull) || (x == x0 && st < n_new)) {
                         ok = false;
                         break;
                     }
-                    if (st >= 2) {
-                        const double* vi = W.u.vpos[fi[curv]];
-                        const double* vj = W.u.vpos[fi[nx]];
-                        double e1x = vi[0] - v0[0], e1y = vi[1] - v0[1], e1z = vi[2] - v0[2];
-                        double e2x = vj[0] - v0[0], e2y = vj[1] - v0[1], e2z = vj[2] - v0[2];
-                        double crx = e1y * e2z - e1z * e2y;
-                        double cry = e1z * e2x - e1x * e2z;
-                        double crz = e1x * e2y - e1y * e2x;
-                        meas += 0.5 * sqrt(crx * crx + cry * cry + crz * crz);
-                        double b0 = vi[0] - sx, b1 = vi[1] - sy, b2 = vi[2] - sz;
-                        double c0 = vj[0] - sx, c1 = vj[1] - sy, c2 = vj[2] - sz;
-                        double x0 = b1 * c2 - b2 * c1;
-                        double x1 = b2 * c0 - b0 * c2;
-                        double x2 = b0 * c1 - b1 * c0;
-                        double tv = (a0 * x0 + a1 * x1 + a2 * x2) / 6.0;
-                        fv += tv;
-                        fc0 += tv * (a0 + b0 + c0) * 0.25;
-                        fc1 += tv * (a1 + b1 + c1) * 0.25;
-                        fc2 += tv * (a2 + b2 + c2) * 0.25;
-                    }
-                    curv = nx;
                 }
-                if (ok && fb[curv] != fa[0]) ok = false;  // the walk must close on v0
-                if (ok) {
-                    valid[pass] = true;
-                    area[pass] = meas;
-                }
+                if (x != x0) ok = false;
             }
-            W.fvol[p] = valid[pass] ? fv : 0.0;
-            W.fcen[p][0] = valid[pass] ? fc0 : 0.0;
-            W.fcen[p][1] = valid[pass] ? fc1 : 0.0;
-            W.fcen[p][2] = valid[pass] ? fc2 : 0.0;
-        }
-    }
-    const uint32_t vb0 = __ballot_sync(FULL, valid[0]);
-    const uint32_t vb1 = __ballot_sync(FULL, valid[1]);
-    const int nf = __popc(vb0) + __popc(vb1);
-    __syncwarp();
-    if (D == 3 && lane == 0) {
-        for (int p = 0; p < nb_v; p++) {  // plane order, as the reference accumulates
-            cell_vol += W.fvol[p];
-            cen[0] += W.fcen[p][0];
-            cen[1] += W.fcen[p][1];
-            cen[2] += W.fcen[p][2];
-        }
-        const double sv = cell_vol;
-        cell_vol = fabs(sv);
-        cen[0] = sx + cen[0] / sv;
-        cen[1] = sy + cen[1] / sv;
-        cen[2] = sz + cen[2] / sv;
-    }
-    unsigned long long base = 0;
-    if (lane == 0) base = atomicAdd(P.face_counter, (unsigned long long)nf);
-    base = __shfl_sync(FULL, base, 0);
-    const bool fits = base + (unsigned long long)nf <= P.face_cap;
-    if (!fits) {
-        if (lane == 0) atomicOr(P.overflow, 1u);
-    } else {
+            ok = __shfl_sync(FULL, ok ? 1 : 0, 0) != 0;
+            bad = !ok;
 #pragma unroll
-        for (int pass = 0; pass < 2; pass++) {
-            if (!valid[pass]) continue;
-            const int p = lane + 32 * pass;
-            const uint32_t vb = pass == 0 ? vb0 : vb1;
-            const int idx = (pass == 0 ? 0 : __popc(vb0)) + __popc(vb & ((1u << lane) - 1u));
-            const size_t f = base + idx;
-            const double4 pe = W.hp[p];
-            const double nlen = sqrt(pe.x * pe.x + pe.y * pe.y + pe.z * pe.z);  // compute_face_normal
-            const int nbr = W.vid[p];
-            P.f_nb[f] = nbr;
-            uint32_t own = BOX_FACE;
-            if (nbr >= 0) {
-                if ((int64_t)nbr < P.n_hydro)
-                    own = pack_owner((uint32_t)nbr, 0);
-                else
-                    own = pack_owner(P.ghost_src[nbr - P.n_hydro], P.ghost_code[nbr - P.n_hydro]);
+            for (int j = 0; j < 3; j++) {
+                const int i = lane + 32 * j;
+                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
+                    const uint32_t tv = W.tri[i];
+                    em[tri_a(tv)] = 0ull;
+                    em[tri_b(tv)] = 0ull;
+                    em[tri_c(tv)] = 0ull;
+                }
             }
-            P.f_own[f] = own;
-            P.f_geo[f] = make_double4(pe.x / nlen, pe.y / nlen, pe.z / nlen, P.ascale * area[pass]);
+            __syncwarp();
+        }
+        if (bad || kept + n_new >= MAX_T) {
+            reclip = true;
+            break;
+        }
+        float nd2[9];
+        for (int q = 0; q < my_new_cnt; q++) nd2[q] = vertex_d2f<D>(hp, my_new[q]);
+        uint32_t kt[3];
+        float kd[3];
+        int kp[3];
+        int before = 0;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int i = lane + 32 * j;
+            const int nvalid = nb_t - 32 * j;
+            const uint32_t vm = nvalid >= 32 ? FULL : (nvalid > 0 ? ((1u << nvalid) - 1u) : 0u);
+            const uint32_t kmj = km[j] & vm;
+            const bool keep = (kmj >> lane) & 1u;
+            kt[j] = keep ? W.tri[i] : 0u;
+            kd[j] = keep ? W.u.b.vd2f[i] : 0.0f;
+            kp[j] = keep ? before + __popc(kmj & ((1u << lane) - 1u)) : -1;
+            before += __popc(kmj);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+            if (kp[j] >= 0) {
+                W.tri[kp[j]] = kt[j];
+                W.u.b.vd2f[kp[j]] = kd[j];
+            }
+        for (int q = 0; q < my_new_cnt; q++) {
+            W.tri[kept + my_new_pos[q]] = my_new[q];
+            W.u.b.vd2f[kept + my_new_pos[q]] = nd2[q];
+        }
+        if (lane == 0) W.vid[cur] = (int)z;
+        nb_v++;
+        nb_t = kept + n_new;
+        __syncwarp();
+        v_dist = max_vd2f(W, nb_t, lane);
+        if ((float)d2B > 4.004f * v_dist) {
+            certified = true;
+            break;
         }
     }
-    if (lane == 0) {
-        P.vol[e] = P.vscale * cell_vol;
-        P.fptr[e] = fits ? (uint32_t)base : 0u;
-        P.fcnt[e] = fits ? (uint32_t)nf : 0u;
-        P.status[e] = ST_SUCCESS;
-        P.certk[e] = certk;
-        P.centroid[3 * (size_t)e] = (cen[0] - 0.5) * P.scale + 0.5;
-        P.centroid[3 * (size_t)e + 1] = (cen[1] - 0.5) * P.scale + 0.5;
-        P.centroid[3 * (size_t)e + 2] = D == 3 ? (cen[2] - 0.5) * P.scale + 0.5 : 0.0;
+    if (reclip) {
+        if (lane == 0) {
+            P.status[e] = ST_RECLIP;
+            atomicAdd(P.reclip, 1u);
+        }
+        return;
     }
+    // ---- FP64: planes, vertices and the certificate over the final vertex set
+    __syncwarp();
+#pragma unroll
+    for (int pass = 0; pass < 2; pass++) {
+        const int p = lane + 32 * pass;
+        if (p < nb_v) W.hp[p] = plane64<D>(p, W.vid[p], ext, sx, sy, sz);
+    }
+    compute_vpos<D>(W, lane, nb_t);
+    double vm64 = 0.0;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int i = lane + 32 * j;
+        if (i < nb_t) vm64 = nan_max(vm64, seed_d2(W.u.vpos[i][0], W.u.vpos[i][1], W.u.vpos[i][2], sx, sy, sz));
+    }
+    vm64 = warp_max(vm64);
+    // first k >= k_last (1-based) whose neighbour lies beyond twice the farthest vertex
+    int certk = 0;
+    const int k_lo = k_last > 0 ? k_last : 1;
+    for (int k0 = k_lo; k0 <= k_stop && certk == 0; k0 += 32) {
+        const int k = k0 + lane;
+        bool pass = false;
+        if (k <= k_stop) {
+            const uint32_t z = kl[k - 1];
+            const PT B = ext[z];
+            pass = seed_d2(B.x, B.y, pz(B), sx, sy, sz) > 4 * vm64;
+        }
+        const unsigned bal = __ballot_sync(FULL, pass);
+        if (bal) certk = k0 + __ffs(bal) - 1;
+    }
+    const bool last_valid = kl[K - 1] != NO_NEIGHBOR;
+    if (certk == 0 || !last_valid) {
+        if (certified && last_valid) {  // FP32 stopped before FP64 agrees: clip again in FP64
+            if (lane == 0) {
+                P.status[e] = ST_RECLIP;
+                atomicAdd(P.reclip, 1u);
+            }
+            return;
+        }
+        store_failed(P, lane, e, ST_SECURITY_RADIUS_NOT_REACHED);
+        return;
+    }
+    extract_and_store<D>(W, P, w, lane, nb_v, nb_t, e, certk, sx, sy, sz, true);
 }
 
 }  // namespace
@@ -702,34 +1172,59 @@ __global__ void k_mark_not_computed(int* __restrict__ status, int* __restrict__ 
     certk[e] = 0;
 }
 
-__global__ void k_flag_uncertified(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ perm,
-                                   const int* __restrict__ status, int64_t nq, int64_t n_hydro,
-                                   uint32_t* __restrict__ flag) {
+// out[off[t]] = qs[t] (sorted positions) or t (query slots) for flagged t
+__global__ void k_compact_list(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ flag,
+                               const uint32_t* __restrict__ off, int64_t nq, int as_slots, uint32_t* __restrict__ out) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nq) return;
+    if (flag[t]) out[off[t]] = as_slots ? (uint32_t)t : qs[t];
+}
+
+// flag[t] = cell of query slot t (hydro only if hydro_only) has status `code`
+__global__ void k_flag_status(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ perm,
+                              const int* __restrict__ status, int64_t nq, int64_t n_hydro, int hydro_only, int code,
+                              uint32_t* __restrict__ flag) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nq) return;
     const uint32_t e = perm[qs[t]];
-    flag[t] = (e < (uint32_t)n_hydro && status[e] == ST_SECURITY_RADIUS_NOT_REACHED) ? 1u : 0u;
+    flag[t] = ((!hydro_only || e < (uint32_t)n_hydro) && status[e] == code) ? 1u : 0u;
 }
 
-__global__ void k_compact_list(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ flag,
-                               const uint32_t* __restrict__ off, int64_t nq, uint32_t* __restrict__ out) {
-    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nq) return;
-    if (flag[t]) out[off[t]] = qs[t];
+// Compacts the cells whose status is `code` into `out` (query slots, or sorted
+// positions when as_slots is false); returns the count.
+cudaError_t select_cells(pgpu_ctx* c, int code, bool hydro_only, bool as_slots, uint32_t* out, uint32_t* count) {
+    cudaError_t e = cudaSuccess;
+    const int64_t nq = c->n_query;
+    uint32_t* flag = ensure<uint32_t>(c->qflag, nq + 1, &e);
+    uint32_t* off = ensure<uint32_t>(c->qoff, nq + 1, &e);
+    if (e) return e;
+    k_flag_status<<<nblk(nq, 256), 256, 0, c->stream>>>((const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p,
+                                                         (const int*)c->status.p, nq, c->n_hydro, hydro_only ? 1 : 0,
+                                                         code, flag);
+    if ((e = exclusive_scan_u32(flag, off, nq, c->scan_tmp, c->stream))) return e;
+    k_compact_list<<<nblk(nq, 256), 256, 0, c->stream>>>((const uint32_t*)c->qs.p, flag, off, nq, as_slots ? 1 : 0,
+                                                          out);
+    count_launches(2);
+    if ((e = cudaMemcpyAsync(count, off + nq, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream))) return e;
+    return cudaStreamSynchronize(c->stream);
 }
+
 
 // One clipping pass over the query list qs[0, nq) with K-neighbour lists `knn`.
 // reset: start a fresh face array (else faces are appended to the current one).
 cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const uint32_t* knn, bool reset,
-                      unsigned long long* fc, unsigned* overflow, unsigned* uncert) {
+                      unsigned long long* fc, unsigned* overflow, unsigned* uncert, bool fp32 = false,
+                      unsigned* reclip = nullptr, const uint32_t* slots = nullptr) {
     const int D = c->prm.dim;
     cudaError_t e = cudaSuccess;
     DevScalars* sc = (DevScalars*)c->scalars.p;
     if (reset && (e = cudaMemsetAsync(&sc->face_count, 0, sizeof(unsigned long long), c->stream))) return e;
     if ((e = cudaMemsetAsync(&sc->overflow, 0, sizeof(unsigned int), c->stream))) return e;
     if ((e = cudaMemsetAsync(&sc->uncertified, 0, sizeof(unsigned int), c->stream))) return e;
+    if ((e = cudaMemsetAsync(&sc->reclip, 0, sizeof(unsigned int), c->stream))) return e;
     ClipParams P;
     P.qs = qs;
+    P.slots = slots;
     P.perm = (const uint32_t*)c->perm.p;
     P.spts = c->spts.p;
     P.ext = c->ext.p;
@@ -741,6 +1236,7 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     P.K = K;
     P.robust = c->prm.predicates == PGPU_PRED_ROBUST;
     P.uncertified = &sc->uncertified;
+    P.reclip = &sc->reclip;
     P.scale = c->unit_scale;
     P.vscale = D == 2 ? P.scale * P.scale : P.scale * P.scale * P.scale;
     P.ascale = D == 2 ? P.scale : P.scale * P.scale;
@@ -758,16 +1254,25 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     P.face_cap = c->face_cap;
     if (nq > 0) {
         const unsigned blocks = (unsigned)((nq + CLIP_WARPS - 1) / CLIP_WARPS);
-        if (D == 2)
-            k_clip<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
-        else
-            k_clip<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+        if (fp32) {
+            if (D == 2)
+                k_clip32<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+            else
+                k_clip32<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+        } else {
+            if (D == 2)
+                k_clip<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+            else
+                k_clip<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+        }
         count_launches(1);
     }
     if ((e = cudaGetLastError())) return e;
     if ((e = cudaMemcpyAsync(fc, &sc->face_count, sizeof(*fc), cudaMemcpyDeviceToHost, c->stream))) return e;
     if ((e = cudaMemcpyAsync(overflow, &sc->overflow, sizeof(*overflow), cudaMemcpyDeviceToHost, c->stream))) return e;
     if ((e = cudaMemcpyAsync(uncert, &sc->uncertified, sizeof(*uncert), cudaMemcpyDeviceToHost, c->stream))) return e;
+    if (reclip && (e = cudaMemcpyAsync(reclip, &sc->reclip, sizeof(*reclip), cudaMemcpyDeviceToHost, c->stream)))
+        return e;
     return cudaStreamSynchronize(c->stream);
 }
 
@@ -802,10 +1307,24 @@ cudaError_t launch_clip(pgpu_ctx* c) {
         if (e) return e;
         c->face_cap = want;
         unsigned long long fc = 0;
-        unsigned of = 0, unc = 0;
+        unsigned of = 0, unc = 0, rc = 0;
+        const bool fp32 = c->prm.precision == PGPU_CLIP_FP32;
         if ((e = clip_pass(c, (const uint32_t*)c->qs.p, c->n_query, c->prm.k, (const uint32_t*)c->knn.p, true, &fc, &of,
-                           &unc)))
+                           &unc, fp32, &rc)))
             return e;
+        c->n_reclip = rc;
+        if (!of && rc > 0) {
+            // cells the FP32 clip could not decide: the FP64 kernel, faces appended
+            uint32_t* fq = ensure<uint32_t>(c->fb_qs, c->n_query + 1, &e);
+            if (e) return e;
+            uint32_t nr = 0;
+            if ((e = select_cells(c, ST_RECLIP, false, true, fq, &nr))) return e;
+            unsigned unc2 = 0, rc2 = 0;
+            if ((e = clip_pass(c, (const uint32_t*)c->qs.p, nr, c->prm.k, (const uint32_t*)c->knn.p, false, &fc, &of,
+                               &unc2, false, &rc2, fq)))
+                return e;
+            unc += unc2;
+        }
         c->num_faces = (int64_t)fc;
         c->n_uncertified = unc;
         c->n_refit = 0;
@@ -819,18 +1338,10 @@ cudaError_t launch_fallback(pgpu_ctx* c) {
     cudaError_t e = cudaSuccess;
     const int64_t nq = c->n_query;
     const int K2 = c->prm.k_fallback;
-    uint32_t* flag = ensure<uint32_t>(c->qflag, nq + 1, &e);
-    uint32_t* off = ensure<uint32_t>(c->qoff, nq + 1, &e);
     uint32_t* fq = ensure<uint32_t>(c->fb_qs, nq + 1, &e);
     if (e) return e;
-    k_flag_uncertified<<<nblk(nq, 256), 256, 0, c->stream>>>((const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p,
-                                                              (const int*)c->status.p, nq, c->n_hydro, flag);
-    if ((e = exclusive_scan_u32(flag, off, nq, c->scan_tmp, c->stream))) return e;
-    k_compact_list<<<nblk(nq, 256), 256, 0, c->stream>>>((const uint32_t*)c->qs.p, flag, off, nq, fq);
-    count_launches(2);
     uint32_t nf = 0;
-    if ((e = cudaMemcpyAsync(&nf, off + nq, sizeof(nf), cudaMemcpyDeviceToHost, c->stream))) return e;
-    if ((e = cudaStreamSynchronize(c->stream))) return e;
+    if ((e = select_cells(c, ST_SECURITY_RADIUS_NOT_REACHED, true, false, fq, &nf))) return e;
     if (nf == 0) return cudaSuccess;
     uint32_t* kl = ensure<uint32_t>(c->fb_knn, (size_t)nf * K2 + 1, &e);
     if (e) return e;

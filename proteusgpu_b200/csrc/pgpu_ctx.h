@@ -36,6 +36,7 @@ struct DevScalars {
     unsigned int failed;            // hydro cells not certified
     int cert_k_max;
     unsigned int uncertified;       // hydro cells with SECURITY_RADIUS_NOT_REACHED in the last clip
+    unsigned int reclip;            // cells the FP32 clip could not decide
     double dt;                      // the step's dt (device copy)
     double sums[5];                 // mass, mom x/y/z, energy
 };
@@ -84,6 +85,7 @@ struct pgpu_ctx {
     size_t face_cap = 0;
     int64_t n_uncertified = 0;  // hydro cells of the last clip with SECURITY_RADIUS_NOT_REACHED
     int64_t n_refit = 0;        // cells recomputed with the fallback budget in the last step
+    int64_t n_reclip = 0;       // cells the FP32 clip handed to the FP64 clip in the last step
     pgpu::DevBuf fb_qs, fb_knn; // fallback query list and lists
 };
 
