@@ -45,15 +45,22 @@ struct WarpCell {
     double4 hp[MAX_P];
     int vid[MAX_P];
     uint32_t tri[MAX_T];
-    double vd2[MAX_T];
-    double fvol[MAX_P];      // per-face volume contribution (3D) for an ordered sum
-    double fcen[MAX_P][3];   // per-face centroid moment (3D)
+    union {
+        struct {
+            double vd2[MAX_T];
+            double fvol[MAX_P];      // per-face volume contribution (3D) for an ordered sum
+            double fcen[MAX_P][3];   // per-face centroid moment (3D)
+        };
+        struct {                     // k_clip32 while clipping
+            float4 V32[MAX_T];       // homogeneous vertex coordinates (rx, ry, rz, rw)
+            float4 P32[MAX_T];       // permanents of the same minors (their rounding bounds)
+        };
+    };
     union {
         struct {
             unsigned long long emask[MAX_P];
             unsigned char nxt[MAX_P];
             float4 hp32[MAX_P];   // FP32 local-frame planes (k_clip32)
-            float vd2f[MAX_T];    // FP32 squared vertex distances (k_clip32)
         } b;
         double vpos[MAX_T][3];
     } u;
@@ -788,6 +795,52 @@ __device__ __forceinline__ int conflict_f(const float4* hp, uint32_t t, const fl
     return det > 0.0f ? 1 : 0;
 }
 
+// Homogeneous coordinates of a vertex in the local frame -- the cofactors of the
+// plane-vertex determinant: det4(p1, p2, p3, e) = e . V (and det3 in 2D) -- and
+// the permanents of the same minors, which bound their rounding errors.  The
+// entries of a plane differ in scale (normal ~ h, offset ~ h^2), so each
+// cofactor keeps its own bound: |e| . P is the permanent of the full matrix.
+template <int D>
+__device__ __forceinline__ void vertex_h32(const float4* hp, uint32_t t, float4& V, float4& Pb) {
+    const float4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)];
+    if (D == 2) {
+        V.x = -det2f(p1.w, p1.y, p2.w, p2.y);
+        V.y = -det2f(p1.x, p1.w, p2.x, p2.w);
+        V.z = 0.0f;
+        V.w = det2f(p1.x, p1.y, p2.x, p2.y);
+        Pb = make_float4(per2f(p1.w, p1.y, p2.w, p2.y), per2f(p1.x, p1.w, p2.x, p2.w), 0.0f,
+                         per2f(p1.x, p1.y, p2.x, p2.y));
+        return;
+    }
+    const float4 p3 = hp[tri_c(t)];
+    V.x = -det3f(p1.w, p1.y, p1.z, p2.w, p2.y, p2.z, p3.w, p3.y, p3.z);
+    V.y = -det3f(p1.x, p1.w, p1.z, p2.x, p2.w, p2.z, p3.x, p3.w, p3.z);
+    V.z = -det3f(p1.x, p1.y, p1.w, p2.x, p2.y, p2.w, p3.x, p3.y, p3.w);
+    V.w = det3f(p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z);
+    Pb = make_float4(per3f(p1.w, p1.y, p1.z, p2.w, p2.y, p2.z, p3.w, p3.y, p3.z),
+                     per3f(p1.x, p1.w, p1.z, p2.x, p2.w, p2.z, p3.x, p3.w, p3.z),
+                     per3f(p1.x, p1.y, p1.w, p2.x, p2.y, p2.w, p3.x, p3.y, p3.w),
+                     per3f(p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z));
+}
+
+// Squared distance to the seed (the origin of the local frame) of a vertex given
+// in homogeneous coordinates.
+__device__ __forceinline__ float vd2_of(const float4& V) {
+    const float x = V.x / V.w, y = V.y / V.w, z = V.z / V.w;
+    return fmaf(x, x, fmaf(y, y, z * z));
+}
+
+// Plane-vertex predicate from the cached cofactors: 0 = not in conflict,
+// 1 = in conflict, 2 = undecided in FP32.  The bound covers the cofactors'
+// rounding, the dot product's and the planes' own entry errors (all first order
+// in the permanent |e| . P).
+__device__ __forceinline__ int conflict_h32(const float4& V, const float4& P, const float4& e) {
+    const float t = fmaf(e.w, V.w, fmaf(e.z, V.z, fmaf(e.y, V.y, e.x * V.x)));
+    const float per = fmaf(fabsf(e.w), P.w, fmaf(fabsf(e.z), P.z, fmaf(fabsf(e.y), P.y, fabsf(e.x) * P.x)));
+    if (!(fabsf(t) > F32_BOUND * per)) return 2;
+    return t > 0.0f ? 1 : 0;
+}
+
 // Squared distance of a vertex to the seed (the origin of the local frame).
 template <int D>
 __device__ __forceinline__ float vertex_d2f(const float4* hp, uint32_t t) {
@@ -821,7 +874,7 @@ __device__ __forceinline__ float max_vd2f(const WarpCell& W, int n, int lane) {
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         const int i = lane + 32 * j;
-        if (i < n) m = nan_maxf(m, W.u.b.vd2f[i]);
+        if (i < n) m = nan_maxf(m, vd2_of(W.V32[i]));
     }
     return warp_maxf(m);
 }
@@ -903,7 +956,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip32(ClipParams P) {
         W.tri[lane] = tv;
     }
     __syncwarp();
-    if (lane < ntri0) W.u.b.vd2f[lane] = vertex_d2f<D>(hp, W.tri[lane]);
+    if (lane < ntri0) vertex_h32<D>(hp, W.tri[lane], W.V32[lane], W.P32[lane]);
     __syncwarp();
     int nb_v = 2 * D, nb_t = ntri0;
     bool reclip = false, certified = false;
@@ -934,7 +987,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip32(ClipParams P) {
             const int i = lane + 32 * j;
             bool cf = false;
             if (i < nb_t) {
-                const int c = conflict_f<D>(hp, W.tri[i], eq);
+                const int c = conflict_h32(W.V32[i], W.P32[i], eq);
                 undecided |= c == 2;
                 cf = c == 1;
             }
@@ -1069,10 +1122,12 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip32(ClipParams P) {
             reclip = true;
             break;
         }
-        float nd2[9];
-        for (int q = 0; q < my_new_cnt; q++) nd2[q] = vertex_d2f<D>(hp, my_new[q]);
+        float4 nV[9];
+        float4 nP[9];
+        for (int q = 0; q < my_new_cnt; q++) vertex_h32<D>(hp, my_new[q], nV[q], nP[q]);
         uint32_t kt[3];
-        float kd[3];
+        float4 kd[3];
+        float4 kb[3];
         int kp[3];
         int before = 0;
 #pragma unroll
@@ -1083,7 +1138,8 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip32(ClipParams P) {
             const uint32_t kmj = km[j] & vm;
             const bool keep = (kmj >> lane) & 1u;
             kt[j] = keep ? W.tri[i] : 0u;
-            kd[j] = keep ? W.u.b.vd2f[i] : 0.0f;
+            kd[j] = keep ? W.V32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            kb[j] = keep ? W.P32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
             kp[j] = keep ? before + __popc(kmj & ((1u << lane) - 1u)) : -1;
             before += __popc(kmj);
         }
@@ -1092,11 +1148,13 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip32(ClipParams P) {
         for (int j = 0; j < 3; j++)
             if (kp[j] >= 0) {
                 W.tri[kp[j]] = kt[j];
-                W.u.b.vd2f[kp[j]] = kd[j];
+                W.V32[kp[j]] = kd[j];
+                W.P32[kp[j]] = kb[j];
             }
         for (int q = 0; q < my_new_cnt; q++) {
             W.tri[kept + my_new_pos[q]] = my_new[q];
-            W.u.b.vd2f[kept + my_new_pos[q]] = nd2[q];
+            W.V32[kept + my_new_pos[q]] = nV[q];
+            W.P32[kept + my_new_pos[q]] = nP[q];
         }
         if (lane == 0) W.vid[cur] = (int)z;
         nb_v++;

@@ -128,8 +128,36 @@ def test_robust_predicates_reflective(dim):
         assert (o.status[:nh] == 4).all()
         assert abs(g.volumes[:nh].sum() - 1.0) < 1e-11
     assert_same_topology(g, o)
+    if dim == 2:
+        check_fields(g, o, dim)
+        return
     # 3D mirror walls leave exactly-degenerate faces whose computed areas are pure rounding
-    check_fields(g, o, dim, floor_frac=1e-9 if dim == 2 else 1e-6)
+    # (a sum of nearly cancelling fan triangles), and nearly degenerate vertices (mirror
+    # images are cospherical) whose rounding is amplified: areas are compared as an
+    # absolute error on the scale of the median face, observed below 5e-11 of it.
+    assert rel_err(g.area, o.area, 1.0) <= 10 * TOL["area_3d"]
+    # The reference orients each face by the cross product of its first three vertices
+    # (cell.cpp:591-627); on wall cells that start is often (nearly) collinear, the sign is
+    # rounding noise and a face's volume term enters with the wrong sign.  The device
+    # orients faces by the clipping triangles' combinatorial orientation.  Volumes are
+    # therefore checked against the pyramid volume sum_f area_f * |x_nb - x_c| / 6, which
+    # needs no orientation: the device matches it on every certified cell, and the oracle
+    # matches the device wherever the oracle itself matches it.
+    ext, _, _ = om.ghosts(pts, buff, om.REFLECTIVE)
+    fc = np.asarray(o.face_counts).astype(np.int64)
+    owner = np.repeat(np.arange(len(fc)), fc)
+    nb = np.asarray(o.neighbor).astype(np.int64)
+    dist = np.linalg.norm(ext[nb] - ext[owner], axis=1) * (1.0 + 2.0 * buff)
+    pyr = np.bincount(owner, np.asarray(o.area) * dist / 6.0, minlength=len(fc))
+    ok = np.asarray(o.status) == 4
+    ok[nh:] = False
+    assert rel_err(g.volumes[ok], pyr[ok]) <= 1e-9
+    ref_ok = ok & (np.abs(o.volumes - pyr) <= 1e-9 * pyr)
+    assert (ok & ~ref_ok).sum() < 0.05 * ok.sum()
+    assert rel_err(g.volumes[ref_ok], o.volumes[ref_ok]) <= TOL["volume_3d"]
+    assert np.abs(g.centroid[ref_ok] - o.centroid[ref_ok]).max() <= TOL["centroid"]
+    assert np.array_equal(g.normal, o.normal) and np.array_equal(g.seeds, o.seeds)
+    assert np.array_equal(np.asarray(g.cert_k)[ok], np.asarray(o.cert_k)[ok])
 
 
 def test_clustered_3d_mesh():
