@@ -148,6 +148,30 @@ int pgpu_dt_cfl(pgpu_ctx *ctx, double cfl, double *dt);
  * mesh and primitives, in the context's flux_mode. */
 int pgpu_hydro_step(pgpu_ctx *ctx, double dt);
 
+/* No counterpart in the reference.  The CFL step of pgpu_dt_cfl (the same
+ * per-cell formula and minimum, starting from 1e100) computed from the
+ * caller's own DEVICE arrays -- rho[n], v[n * dim], E[n], volumes[n] of the n
+ * hydro cells -- without a context and without allocating anything: no
+ * cudaMalloc/cudaFree, no allocating library.  It is for callers that keep
+ * their cell data in device memory they manage themselves and cannot let a
+ * library allocate: a code whose device memory is reserved up front by its own
+ * pool (a further cudaMalloc would fail or fragment it), or one whose time loop
+ * cannot afford the device-wide synchronisation of cudaFree.
+ *   Scratch: a fixed 128 KiB array in the library's device image, one partial
+ * minimum per 1024 cells, hence n <= PGPU_DT_STATIC_MAX_CELLS; a larger n (or a
+ * device ordinal >= PGPU_DT_STATIC_MAX_DEVICES) returns PGPU_ECAPACITY before
+ * any device work.  Nothing in the scratch has to start at zero.  The first
+ * call on each device looks up the scratch's address (cudaGetSymbolAddress)
+ * with that device current; make that first call before capturing work on a
+ * stream.  Calls that overlap on one device (other threads, other streams)
+ * share the scratch and race: order them.
+ *   Runs on the current device, on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream), and waits for it before writing *dt on the host. */
+#define PGPU_DT_STATIC_MAX_CELLS 16777216
+#define PGPU_DT_STATIC_MAX_DEVICES 64
+int pgpu_dt_cfl_static(int dim, double gamma, double cfl, const double *rho, const double *v, const double *E,
+                       const double *volumes, int64_t n, void *stream, double *dt);
+
 /* -------------------------------------------------- moving-mesh stepping ---
  * Extension (the reference's time loop, src/main.cpp:50-63, keeps its mesh
  * fixed).  The simulation state is conserved mass, momentum and energy per

@@ -24,7 +24,7 @@ EXPORTED = [
     "pgpu_mesh_sizes", "pgpu_upload_mesh", "pgpu_set_prim", "pgpu_get_prim", "pgpu_dt_cfl",
     "pgpu_hydro_step", "pgpu_sim_init", "pgpu_sim_step", "pgpu_sim_step_host", "pgpu_sim_get",
     "pgpu_sim_set", "pgpu_sim_stats", "pgpu_enable_timing", "pgpu_stage_times", "pgpu_stream",
-    "pgpu_launch_count", "pgpu_fp64_peak", "pgpu_riemann_hll",
+    "pgpu_launch_count", "pgpu_fp64_peak", "pgpu_riemann_hll", "pgpu_dt_cfl_static",
 ]
 
 
@@ -90,6 +90,7 @@ def load(path: str = LIB_PATH):
     L.pgpu_launch_count.restype = C.c_int64
     L.pgpu_fp64_peak.argtypes = [C.c_int, C.c_float, vp]
     L.pgpu_riemann_hll.argtypes = [C.c_int, dbl, vp, vp, vp, vp]
+    L.pgpu_dt_cfl_static.argtypes = [C.c_int, dbl, dbl, vp, vp, vp, vp, i64, vp, vp]
     for name in EXPORTED:
         getattr(L, name)  # raises AttributeError if a declared symbol is missing
     _LIB = L

@@ -19,6 +19,8 @@
 // so a flux computed from the same inputs is bit-identical.
 #include <math_constants.h>
 
+#include <mutex>
+
 #include "pgpu_common.cuh"
 #include "pgpu_ctx.h"
 
@@ -434,3 +436,83 @@ cudaError_t launch_sums(pgpu_ctx* c) {
 }
 
 }  // namespace pgpu
+
+// ---------------------------------------------------------------------------
+// pgpu_dt_cfl_static: hydro::dt_CFL on the caller's device arrays, with no
+// allocation.  Its scratch is a file-scope device array: one partial minimum
+// per block of DT_STATIC_CELLS_PER_BLOCK cells, then the result.  Every slot is
+// written before it is read in the same call, so nothing has to start at zero;
+// two calls that overlap on one device share the array and race.
+namespace pgpu {
+namespace {
+
+constexpr int DT_STATIC_CELLS_PER_THREAD = 4;
+constexpr int64_t DT_STATIC_CELLS_PER_BLOCK = (int64_t)HT * DT_STATIC_CELLS_PER_THREAD;
+constexpr int DT_STATIC_MAX_BLOCKS = (int)(PGPU_DT_STATIC_MAX_CELLS / DT_STATIC_CELLS_PER_BLOCK);
+static_assert((int64_t)DT_STATIC_MAX_BLOCKS * DT_STATIC_CELLS_PER_BLOCK == PGPU_DT_STATIC_MAX_CELLS,
+              "the cell limit is a whole number of blocks");
+
+// 16384 partials + the result: 128 KiB + 8 bytes of the library's device image.
+static __device__ __align__(256) double g_dt_scratch[DT_STATIC_MAX_BLOCKS + 1];
+
+template <int D>
+__global__ void k_dt_static_partial(const double* __restrict__ rho, const double* __restrict__ v,
+                                    const double* __restrict__ E, const double* __restrict__ vol, int64_t n,
+                                    double cfl, double gamma, double* __restrict__ partial) {
+    const int64_t base = (int64_t)blockIdx.x * DT_STATIC_CELLS_PER_BLOCK + threadIdx.x;
+    double d = 1e100;  // the reference's starting value of the minimum
+#pragma unroll
+    for (int j = 0; j < DT_STATIC_CELLS_PER_THREAD; j++) {
+        const int64_t i = base + (int64_t)j * HT;
+        if (i < n) d = fmin(d, dt_cell<D>(load_prim<D>(rho, v, E, i), vol[i], cfl, gamma));
+    }
+    d = block_min(d);
+    if (threadIdx.x == 0) partial[blockIdx.x] = d;
+}
+
+__global__ void k_dt_static_final(const double* __restrict__ partial, int nb, double* __restrict__ out) {
+    double d = 1e100;
+    for (int b = threadIdx.x; b < nb; b += HT) d = fmin(d, partial[b]);
+    d = block_min(d);
+    if (threadIdx.x == 0) *out = d;
+}
+
+std::mutex g_dt_static_mu;
+double* g_dt_static_ptr[PGPU_DT_STATIC_MAX_DEVICES];
+
+}  // namespace
+}  // namespace pgpu
+
+extern "C" int pgpu_dt_cfl_static(int dim, double gamma, double cfl, const double* rho, const double* v,
+                                  const double* E, const double* volumes, int64_t n, void* stream, double* dt) {
+    using namespace pgpu;
+    if ((dim != 2 && dim != 3) || !rho || !v || !E || !volumes || !dt || n <= 0) return PGPU_EINVAL;
+    if (n > PGPU_DT_STATIC_MAX_CELLS) return PGPU_ECAPACITY;
+    int dev = -1;
+    if (cudaGetDevice(&dev) != cudaSuccess) return PGPU_ECUDA;
+    if (dev < 0 || dev >= PGPU_DT_STATIC_MAX_DEVICES) return PGPU_ECAPACITY;
+    double* scratch;
+    {
+        std::lock_guard<std::mutex> lock(g_dt_static_mu);
+        if (!g_dt_static_ptr[dev]) {
+            void* p = nullptr;
+            if (cudaGetSymbolAddress(&p, g_dt_scratch) != cudaSuccess || !p) return PGPU_ECUDA;
+            g_dt_static_ptr[dev] = (double*)p;
+        }
+        scratch = g_dt_static_ptr[dev];
+    }
+    cudaStream_t s = (cudaStream_t)stream;
+    const int nb = (int)((n + DT_STATIC_CELLS_PER_BLOCK - 1) / DT_STATIC_CELLS_PER_BLOCK);
+    if (dim == 2)
+        k_dt_static_partial<2><<<nb, HT, 0, s>>>(rho, v, E, volumes, n, cfl, gamma, scratch);
+    else
+        k_dt_static_partial<3><<<nb, HT, 0, s>>>(rho, v, E, volumes, n, cfl, gamma, scratch);
+    k_dt_static_final<<<1, HT, 0, s>>>(scratch, nb, scratch + DT_STATIC_MAX_BLOCKS);
+    count_launches(2);
+    if (cudaGetLastError() != cudaSuccess) return PGPU_ECUDA;
+    if (cudaMemcpyAsync(dt, scratch + DT_STATIC_MAX_BLOCKS, sizeof(double), cudaMemcpyDeviceToHost, s) !=
+        cudaSuccess)
+        return PGPU_ECUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return PGPU_ECUDA;
+    return PGPU_OK;
+}
