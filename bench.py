@@ -2,10 +2,11 @@
 """Benchmark of the per-timestep mesh-and-flux path (one JSON line on stdout).
 
 A step is one full moving-mesh step of the 3D Sedov-Taylor workload
-(1,048,576 uniform points, K = 190, FP64): ghost layer, Morton grid sort, KNN,
-clipping with the security-radius certificate, extraction, CFL time step,
-HLL flux + conserved update + drift.  The metric is hydro cell-updates per
-second (one hydro cell advanced one full step).
+(1,048,576 uniform points): ghost layer, Morton grid sort, KNN, clipping with
+the security-radius certificate, extraction, CFL time step, HLL flux +
+conserved update + drift.  The metric is hydro cell-updates per second (one
+hydro cell advanced one full step) of the learned-K + FP32-clipping form, with
+the plain fixed-K (190) FP64 form timed beside it on the same states.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -64,7 +65,8 @@ def parse():
     ap.add_argument("--config", choices=sorted(CONFIGS), default="sedov3d_1m")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the end-to-end leg")
-    ap.add_argument("--skip-forms", action="store_true", help="omit the FP32-clipping form beside the plain one")
+    ap.add_argument("--skip-forms", action="store_true",
+                    help="time only the headline form and the plain baseline (not fp32_clip, learned_fp64)")
     return ap.parse_args()
 
 
@@ -89,10 +91,12 @@ class ClockSampler:
     Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_id: str | None):
-        self.gpu_id, self.proc, self.lines = gpu_id, None, []
+    def __init__(self, gpu_id: str | None, enabled: bool = True):
+        self.gpu_id, self.proc, self.lines, self.enabled = gpu_id, None, [], enabled
 
     def __enter__(self):
+        if not self.enabled:
+            return self
         cmd = ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits", "-lms", "200"]
         if self.gpu_id:
             cmd += ["-i", self.gpu_id]
@@ -179,9 +183,104 @@ def cpu_reference_step_rate(steps: int, n_sample: int = 20000, nthreads: int | N
 
 
 # ---------------------------------------------------------------- our arm
-def run_ours(args, rank, world, local_rank):
+# Forms of the step.  The headline is the learned neighbour budget with FP32
+# local-frame clipping; the plain FP64 fixed-K method is the baseline it is
+# compared with (same mesh bit for bit, same states at every step).
+FORMS = {
+    "plain_fp64": dict(precision="fp64", kbudget=False),
+    "fp32_clip": dict(precision="fp32", kbudget=False),
+    "learned_fp64": dict(precision="fp64", kbudget=True),
+    "learned_fp32": dict(precision="fp32", kbudget=True),
+}
+HEADLINE, BASELINE_FORM = "learned_fp32", "plain_fp64"
+
+# DRAM bytes per cell of one k_clip32 launch, from the ncu capture summarised in
+# profiles/k_clip32_sedov3d_256k.md (read + write / cells), used for `traffic`.
+CLIP32_DRAM_BYTES_PER_CELL = (143.396608e6 + 161.378048e6) / 262_144
+
+
+def _barrier(dist):
+    if dist:
+        dist.barrier()
+
+
+def _max_over_ranks(dist, ms):
+    if not dist:
+        return ms
+    import torch
+    t = torch.tensor([ms], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks=False):
+    """Runs one form from the initial condition: W warm-up steps (the learned forms
+    train their proposal on them), one step with per-stage CUDA events, then K timed
+    steps bracketed by a barrier and synchronize (max over ranks)."""
     import torch
     from proteusgpu_b200 import Context, _lib
+    L = _lib.load()
+    spec = FORMS[form]
+    ctx = Context(dim=cfg["dim"], k=cfg["k"], buff=cfg["buff"], boundary=cfg["boundary"], flux="physical",
+                  gamma=ic.gamma, device=local_rank, precision=spec["precision"])
+    if spec["kbudget"]:
+        # the warm-up steps but the last train the proposal; the last one already uses it
+        ctx.kbudget_enable(train_steps=max(1, args.warmup - 1), iters_per_step=64, quantile=0.99, seed=1)
+    ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+    for _ in range(max(args.warmup, 0)):
+        ctx.sim_step(cfg["cfl"], want_dt=False)
+    ctx.enable_timing(True)
+    ctx.sim_step(cfg["cfl"], want_dt=False)
+    stage = ctx.stage_times()
+    ctx.enable_timing(False)
+    stats = ctx.stats()
+    kb = ctx.kbudget_stats() if spec["kbudget"] else None
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    torch.cuda.synchronize()
+    _barrier(dist)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
+    except Exception:
+        pass
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = L.pgpu_launch_count()
+    with ClockSampler(uuid, enabled=want_clocks) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            ctx.sim_step(cfg["cfl"], want_dt=False)
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    ms = _max_over_ranks(dist, ev0.elapsed_time(ev1))
+    launches = L.pgpu_launch_count() - l0
+    kb_after = ctx.kbudget_stats() if spec["kbudget"] else None
+    out = {"ms": ms, "stage": stage, "stats": stats, "launches": launches, "clocks": clk.summary(),
+           "kbudget": kb_after or kb}
+    if want_e2e:
+        # end to end: the same step through the C ABI with the state in pinned host
+        # memory, copied to the device before and back after every step
+        x, m_, p_, e_ = ctx.sim_get()
+        hp = [torch.from_numpy(a).pin_memory() for a in (x, m_, p_, e_)]
+        hn = [t.numpy() for t in hp]
+        ke = max(1, min(args.steps, 5))
+        ctx.sim_step_host(cfg["cfl"], 0.0, *hn)  # warm the path
+        torch.cuda.synchronize()
+        _barrier(dist)
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            ctx.sim_step_host(cfg["cfl"], 0.0, *hn)
+        torch.cuda.synchronize()
+        e_ms = _max_over_ranks(dist, (time.perf_counter() - t0) * 1e3)
+        nbytes = int(sum(a.nbytes for a in hn))
+        out["e2e"] = {"ms": e_ms, "steps": ke, "bytes": nbytes}
+    ctx.close()
+    return out
+
+
+def run_ours(args, rank, world, local_rank):
+    import ctypes
+    import torch
+    from proteusgpu_b200 import _lib
     cfg = CONFIGS[args.config]
     torch.cuda.set_device(local_rank)
     dist = None
@@ -191,145 +290,72 @@ def run_ours(args, rank, world, local_rank):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
     ic = make_ic(cfg)
-    ctx = Context(dim=cfg["dim"], k=cfg["k"], buff=cfg["buff"], boundary=cfg["boundary"], flux="physical",
-                  gamma=ic.gamma, device=local_rank)
-    ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
-    for _ in range(max(args.warmup, 0)):
-        ctx.sim_step(cfg["cfl"], want_dt=False)
-    stream = torch.cuda.ExternalStream(ctx.stream)
-    L = _lib.load()
-    # per-stage device times (CUDA events on the context's stream), one step, outside the timed region
-    ctx.enable_timing(True)
-    ctx.sim_step(cfg["cfl"], want_dt=False)
-    stage = ctx.stage_times()
-    ctx.enable_timing(False)
-    stats = ctx.stats()
-
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
-    uuid = None
-    try:
-        uuid = "GPU-" + str(torch.cuda.get_device_properties(local_rank).uuid)
-    except Exception:
-        pass
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    l0 = L.pgpu_launch_count()
-    with ClockSampler(uuid) as clk:
-        ev0.record(stream)
-        for _ in range(args.steps):
-            ctx.sim_step(cfg["cfl"], want_dt=False)
-        ev1.record(stream)
-        torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1)
-    launches = L.pgpu_launch_count() - l0
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        dist.barrier()
     n = ic.n
-    value = n * args.steps * world / (ms / 1e3)
-
-    # end to end: the same step through the C ABI with the state in pinned host memory,
-    # copied to the device before and back after every step
-    e2e = None
-    if not args.skip_e2e:
-        D = cfg["dim"]
-        x, m_, p_, e_ = ctx.sim_get()
-        hp = [torch.from_numpy(a).pin_memory() for a in (x, m_, p_, e_)]
-        hn = [t.numpy() for t in hp]
-        ke = max(1, min(args.steps, 5))
-        ctx.sim_step_host(cfg["cfl"], 0.0, *hn)  # warm the path
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        t0 = time.perf_counter()
-        for _ in range(ke):
-            ctx.sim_step_host(cfg["cfl"], 0.0, *hn)
-        torch.cuda.synchronize()
-        e_ms = (time.perf_counter() - t0) * 1e3
-        if dist:
-            t = torch.tensor([e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
-        nbytes = int(sum(a.nbytes for a in hn))
-        e2e = {"value": n * ke * world / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": nbytes,
-               "d2h_bytes_per_step": nbytes, "steps": ke,
-               "path": "pgpu_sim_step_host (C ABI), pinned host state in/out every step"}
-
-    # the precision form: FP32 local-frame clipping, same mesh (timed on the same state)
-    forms = None
-    if not args.skip_forms:
-        x, m_, p_, e_ = ctx.sim_get()
-        with Context(dim=cfg["dim"], k=cfg["k"], buff=cfg["buff"], boundary=cfg["boundary"], flux="physical",
-                     gamma=ic.gamma, device=local_rank, precision="fp32") as c32:
-            c32.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
-            c32.sim_set(x, m_, p_, e_)
-            for _ in range(max(args.warmup, 1)):
-                c32.sim_step(cfg["cfl"], want_dt=False)
-            c32.enable_timing(True)
-            c32.sim_step(cfg["cfl"], want_dt=False)
-            st32 = c32.stage_times()
-            c32.enable_timing(False)
-            s32 = torch.cuda.ExternalStream(c32.stream)
-            torch.cuda.synchronize()
-            if dist:
-                dist.barrier()
-            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            f0.record(s32)
-            for _ in range(args.steps):
-                c32.sim_step(cfg["cfl"], want_dt=False)
-            f1.record(s32)
-            torch.cuda.synchronize()
-            ms32 = f0.elapsed_time(f1)
-            if dist:
-                t = torch.tensor([ms32], device="cuda")
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                ms32 = float(t.item())
-            stats32 = c32.stats()
-        v32 = ic.n * args.steps * world / (ms32 / 1e3)
-        forms = {"plain_fp64": {"value": value, "ms_per_step": ms / args.steps},
-                 "fp32_clip": {"value": v32, "ms_per_step": ms32 / args.steps,
-                               "stages_ms": dict(zip(STAGES, st32)), "reclip_cells": stats32["reclip_cells"],
-                               "speedup_vs_plain": v32 / value}}
-
+    names = [BASELINE_FORM, HEADLINE] if args.skip_forms else list(FORMS)
+    res = {}
+    for f in names:
+        res[f] = time_form(args, cfg, ic, local_rank, dist, f, want_e2e=(f == HEADLINE and not args.skip_e2e),
+                           want_clocks=(f == HEADLINE))
+    _barrier(dist)
     if dist:
-        dist.barrier()
         dist.destroy_process_group()
     if rank != 0:
-        ctx.close()
         return None
 
-    # roofline of the dominant stage
+    def rate(r):
+        return n * args.steps * world / (r["ms"] / 1e3)
+
+    head, base = res[HEADLINE], res[BASELINE_FORM]
+    value = rate(head)
+    forms = {}
+    for f, r in res.items():
+        forms[f] = {"value": rate(r), "ms_per_step": r["ms"] / args.steps,
+                    "stages_ms": dict(zip(STAGES, r["stage"])), "reclip_cells": r["stats"]["reclip_cells"],
+                    "speedup_vs_plain": rate(r) / rate(base)}
+        if r["kbudget"]:
+            kb = r["kbudget"]
+            forms[f]["learned_k"] = {"mean_k": kb["mean_k"], "plain_k": cfg["k"], "cells": kb["cells"],
+                                     "misses": kb["misses"], "miss_rate": kb["misses"] / max(kb["cells"], 1),
+                                     "train_steps": kb["steps_trained"], "last_train_loss": kb["last_loss"]}
+    e2e = None
+    if "e2e" in head:
+        e = head["e2e"]
+        e2e = {"value": n * e["steps"] * world / (e["ms"] / 1e3), "unit": UNIT, "h2d_bytes_per_step": e["bytes"],
+               "d2h_bytes_per_step": e["bytes"], "steps": e["steps"],
+               "path": f"pgpu_sim_step_host (C ABI), form {HEADLINE}, pinned host state in/out every step"}
+
+    # roofline of the headline's dominant stage
     D = cfg["dim"]
     W = WORK[D]
-    knn_ms, clip_ms, hydro_ms = stage[2], stage[3], stage[4]
+    stage, stats = head["stage"], head["stats"]
     dom = STAGES[int(np.argmax(stage))]
-    fp64 = C_double = None
-    import ctypes
-    C_double = ctypes.c_double()
-    L.pgpu_fp64_peak(local_rank, ctypes.c_float(200.0), ctypes.byref(C_double))
-    fp64 = C_double.value
+    fp64, fp32 = ctypes.c_double(), ctypes.c_double()
+    L = _lib.load()
+    L.pgpu_fp64_peak(local_rank, ctypes.c_float(200.0), ctypes.byref(fp64))
+    L.pgpu_fp32_peak(local_rank, ctypes.c_float(200.0), ctypes.byref(fp32))
     hbm, hbm_src = measured_peaks()
     n_query = stats["n_hydro"]
-    if dom == "knn":
-        ach = n_query * W["knn_flop_per_query"] / (knn_ms * 1e-3) / 1e12
-        roof = {"kernel": "k_knn", "bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
-                "frac": ach / fp64, "traffic": None,
+    if dom == "clip":
+        peak = fp32.value
+        ach = n_query * W["clip_flop_per_cell"] / (stage[3] * 1e-3) / 1e12
+        roof = {"kernel": "k_clip32 (+ FP64 re-clip of undecided cells)", "bound": "fp32", "achieved": ach,
+                "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
+                "traffic": CLIP32_DRAM_BYTES_PER_CELL * n_query,
+                "traffic_note": "DRAM bytes per launch, ncu capture at 262,144 cells scaled by cells",
+                "peak_source": "FP32 FMA rate measured in this run (pgpu_fp32_peak)",
+                "work": f"{W['clip_flop_per_cell']:.0f} algorithmic flop per cell x {n_query} cells"}
+    elif dom == "knn":
+        peak = fp64.value
+        ach = n_query * W["knn_flop_per_query"] / (stage[2] * 1e-3) / 1e12
+        roof = {"kernel": "k_knn", "bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
+                "frac": ach / peak, "traffic": None,
                 "peak_source": "FP64 FMA rate measured in this run (pgpu_fp64_peak)",
                 "work": f"{W['knn_flop_per_query']:.0f} algorithmic flop per query x {n_query} queries"}
-    elif dom == "clip":
-        ach = n_query * W["clip_flop_per_cell"] / (clip_ms * 1e-3) / 1e12
-        roof = {"kernel": "k_clip", "bound": "fp64", "achieved": ach, "peak": fp64, "unit": "TFLOP/s",
-                "frac": ach / fp64, "traffic": None,
-                "peak_source": "FP64 FMA rate measured in this run (pgpu_fp64_peak)",
-                "work": f"{W['clip_flop_per_cell']:.0f} algorithmic flop per cell x {n_query} cells"}
     else:
         ach = n_query * W["hydro_bytes_per_cell"] / (stage[STAGES.index(dom)] * 1e-3) / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                 "traffic": None, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})"}
-    hyd = n_query * W["hydro_bytes_per_cell"] / (hydro_ms * 1e-3) / 1e9
+    hyd = n_query * W["hydro_bytes_per_cell"] / (stage[4] * 1e-3) / 1e9
     roof_hydro = {"kernel": "k_prim_dt + k_flux_update", "bound": "hbm", "achieved": hyd, "peak": hbm,
                   "unit": "GB/s", "frac": hyd / hbm, "traffic": None,
                   "work": f"{W['hydro_bytes_per_cell']} compulsory bytes per cell-update"}
@@ -339,27 +365,31 @@ def run_ours(args, rank, world, local_rank):
         v, kind, cores, sample, t_step = cpu_reference_step_rate(steps=2)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
                "s_per_step": t_step}
+    wl = (f"{args.config}: 3D Sedov-Taylor blast, {cfg['n']} uniform points (seed {cfg['seed']}), "
+          f"moving mesh, {cfg['boundary']} box" if D == 3 else args.config)
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{args.config}: 3D Sedov-Taylor blast, {cfg['n']} uniform points (seed "
-                               f"{cfg['seed']}), K={cfg['k']}, plain FP64 method, moving mesh, "
-                               f"{cfg['boundary']} box" if D == 3 else args.config,
-                   "n_points": cfg["n"], "k": cfg["k"], "buff": cfg["buff"], "form": "plain",
+        "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": wl, "n_points": cfg["n"], "k": cfg["k"], "buff": cfg["buff"],
+                   "form": "learned-K (BF16 MLP proposal, plain-K fallback) + FP32 local-frame clipping "
+                           "(FP64 re-clip, FP64 extraction, hydro and sums)",
+                   "baseline_form": f"plain: fixed K={cfg['k']}, FP64 clipping",
                    "flux": "physical (outward normal, pair-symmetric area)",
                    "l2": "inputs larger than L2: per-step KNN lists alone are "
-                         f"{stats['n_hydro'] * cfg['k'] * 4 / 2 ** 20:.0f} MiB",
+                         f"{stats['n_hydro'] * cfg['k'] * 4 / 2 ** 20:.0f} MiB at the plain K",
                    "parallelism": f"replicas x{world}"},
+        "speedup_vs_plain_gpu": value / rate(base),
         "roofline": roof, "roofline_hydro": roof_hydro,
         "stages_ms": dict(zip(STAGES, stage)),
-        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "forms": forms,
-        "clocks": clk.summary(),
+        "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"], "forms": forms,
+        "clocks": head["clocks"],
         "mesh": {"n_ext": stats["n_ext"], "faces": stats["num_faces"], "cert_k_max": stats["cert_k_max"],
                  "failed_cells": stats["failed_cells"], "knn_candidates_per_query":
                      stats["knn_candidates"] / max(stats["n_hydro"], 1)},
+        "peaks": {"fp64_tflops": fp64.value, "fp32_tflops": fp32.value, "hbm_gbs": hbm},
     }
-    ctx.close()
     return out
 
 

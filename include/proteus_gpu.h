@@ -216,6 +216,43 @@ typedef struct {
 /* Statistics of the last step (synchronises the stream). */
 int pgpu_sim_stats(pgpu_ctx *ctx, pgpu_stats *out);
 
+/* ------------------------------------------- learned neighbour budget ---
+ * Extension (the reference uses one compile-time _K_ for every cell, Config.sh,
+ * src/knn/knn.cpp:225-315).  When enabled, every mesh build of a moving-mesh
+ * step gives each hydro cell its own K: an MLP (8 features -> 32 -> 32 -> 6,
+ * GELU; BF16 weights, FP32 accumulation on the tensor cores) picks one of six
+ * classes, {12,16,20,24,32,48} in 2D and {32,40,48,64,96,128} in 3D (capped at
+ * the context's k).  A cell that does not certify within its K is computed
+ * again at max(k, k_fallback), so the mesh equals the plain method's.  The
+ * first train_steps steps run the plain method and train the MLP on the K its
+ * certificate records (iters_per_step Adam iterations on 16384-cell batches);
+ * the proposal is the smallest class whose predicted cumulative probability
+ * reaches `quantile`.  train_steps 0 uses the current weights at once. */
+int pgpu_kbudget_enable(pgpu_ctx *ctx, int train_steps, int iters_per_step, double quantile, uint64_t seed);
+int pgpu_kbudget_classes(int dim, int *k_out6);
+
+typedef struct {
+    int32_t active;          /* proposals in use */
+    int64_t steps_trained;
+    double last_loss;        /* mean cross-entropy of the last training iteration */
+    int64_t cells;           /* last step: cells that got a proposal */
+    int64_t misses;          /* last step: proposals the certificate rejected */
+    double mean_k;           /* last step: mean proposed K */
+} pgpu_kbudget_info;
+int pgpu_kbudget_stats(pgpu_ctx *ctx, pgpu_kbudget_info *out);
+
+/* The MLP's FP32 master parameters, 1542 floats: W1[32][8], b1[32], W2[32][32],
+ * b2[32], W3[6][32], b3[6] (row-major, out x in); get and/or set (NULL skips). */
+int pgpu_kbudget_weights(pgpu_ctx *ctx, float *get, const float *set);
+
+/* The device MLP on host arrays: feat n x 8 -> logits n x 6 and the proposed K
+ * per row (either output may be NULL). */
+int pgpu_mlp_forward(pgpu_ctx *ctx, const float *feat, int64_t n, float *logits, uint16_t *kq);
+
+/* Gradient of the mean cross-entropy over n rows (labels = class indices 0-5)
+ * at the current weights, in the parameter layout above, and the loss. */
+int pgpu_mlp_grad(pgpu_ctx *ctx, const float *feat, const int32_t *labels, int64_t n, float *grad, float *loss);
+
 /* Per-stage device times of the last step in milliseconds, measured with CUDA
  * events when timing is enabled: ghosts, sort, knn, clip, hydro. */
 int pgpu_enable_timing(pgpu_ctx *ctx, int on);
@@ -239,6 +276,8 @@ int64_t pgpu_launch_count(void);
  * FP64 rate in TFLOP/s (the FP64 pipe peak that the KNN and clipping kernels
  * are measured against). */
 int pgpu_fp64_peak(int device, float ms, double *tflops);
+/* The same with FP32 FMAs (the FP32 pipe peak of the FP32 clipping kernel). */
+int pgpu_fp32_peak(int device, float ms, double *tflops);
 
 #ifdef __cplusplus
 }

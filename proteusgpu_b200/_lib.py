@@ -25,6 +25,8 @@ EXPORTED = [
     "pgpu_hydro_step", "pgpu_sim_init", "pgpu_sim_step", "pgpu_sim_step_host", "pgpu_sim_get",
     "pgpu_sim_set", "pgpu_sim_stats", "pgpu_enable_timing", "pgpu_stage_times", "pgpu_stream",
     "pgpu_launch_count", "pgpu_fp64_peak", "pgpu_riemann_hll", "pgpu_dt_cfl_static",
+    "pgpu_kbudget_enable", "pgpu_kbudget_classes", "pgpu_kbudget_stats", "pgpu_kbudget_weights",
+    "pgpu_mlp_forward", "pgpu_mlp_grad", "pgpu_fp32_peak",
 ]
 
 
@@ -42,6 +44,13 @@ class Stats(C.Structure):
                 ("n_grid", C.c_int32), ("refit_cells", C.c_int64), ("uncertified_cells", C.c_int64),
                 ("reclip_cells", C.c_int64)]
 
+
+class KBudgetInfo(C.Structure):
+    _fields_ = [("active", C.c_int32), ("steps_trained", C.c_int64), ("last_loss", C.c_double),
+                ("cells", C.c_int64), ("misses", C.c_int64), ("mean_k", C.c_double)]
+
+
+KB_NPARAM = 1542  # W1[32][8], b1[32], W2[32][32], b2[32], W3[6][32], b3[6]
 
 _LIB = None
 vp = C.c_void_p
@@ -89,8 +98,15 @@ def load(path: str = LIB_PATH):
     L.pgpu_stream.restype = vp
     L.pgpu_launch_count.restype = C.c_int64
     L.pgpu_fp64_peak.argtypes = [C.c_int, C.c_float, vp]
+    L.pgpu_fp32_peak.argtypes = [C.c_int, C.c_float, vp]
     L.pgpu_riemann_hll.argtypes = [C.c_int, dbl, vp, vp, vp, vp]
     L.pgpu_dt_cfl_static.argtypes = [C.c_int, dbl, dbl, vp, vp, vp, vp, i64, vp, vp]
+    L.pgpu_kbudget_enable.argtypes = [vp, C.c_int, C.c_int, dbl, C.c_uint64]
+    L.pgpu_kbudget_classes.argtypes = [C.c_int, vp]
+    L.pgpu_kbudget_stats.argtypes = [vp, C.POINTER(KBudgetInfo)]
+    L.pgpu_kbudget_weights.argtypes = [vp, vp, vp]
+    L.pgpu_mlp_forward.argtypes = [vp, vp, i64, vp, vp]
+    L.pgpu_mlp_grad.argtypes = [vp, vp, vp, i64, vp, vp]
     for name in EXPORTED:
         getattr(L, name)  # raises AttributeError if a declared symbol is missing
     _LIB = L

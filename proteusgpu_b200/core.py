@@ -226,6 +226,48 @@ class Context:
         check(self._h, self._L.pgpu_sim_stats(self._h, C.byref(s)), "pgpu_sim_stats")
         return {f: (list(getattr(s, f)) if f == "total_mom" else getattr(s, f)) for f, _ in s._fields_}
 
+    # ---- learned neighbour budget (extension; the reference has one _K_ for all cells)
+    def kbudget_enable(self, train_steps: int = 3, iters_per_step: int = 64, quantile: float = 0.99,
+                       seed: int = 1) -> None:
+        """Per-cell K from the device MLP on every moving-mesh step after train_steps
+        plain steps that train it; rejected proposals are recomputed at the plain K."""
+        check(self._h, self._L.pgpu_kbudget_enable(self._h, train_steps, iters_per_step, quantile, seed),
+              "pgpu_kbudget_enable")
+
+    def kbudget_stats(self) -> dict:
+        s = _lib.KBudgetInfo()
+        check(self._h, self._L.pgpu_kbudget_stats(self._h, C.byref(s)), "pgpu_kbudget_stats")
+        return {f: getattr(s, f) for f, _ in s._fields_}
+
+    def kbudget_weights(self, set_to: np.ndarray | None = None) -> np.ndarray:
+        """The MLP's FP32 master parameters (1542 floats); optionally replaces them first."""
+        out = np.zeros(_lib.KB_NPARAM, np.float32)
+        src = None if set_to is None else np.ascontiguousarray(set_to, np.float32)
+        if src is not None and src.size != _lib.KB_NPARAM:
+            raise ValueError("expected 1542 parameters")
+        check(self._h, self._L.pgpu_kbudget_weights(self._h, None, None if src is None else _ptr(src)),
+              "pgpu_kbudget_weights")
+        check(self._h, self._L.pgpu_kbudget_weights(self._h, _ptr(out), None), "pgpu_kbudget_weights")
+        return out
+
+    def mlp_forward(self, feat: np.ndarray):
+        """Device MLP on n x 8 features: (logits n x 6, proposed K per row)."""
+        f = np.ascontiguousarray(feat, np.float32)
+        n = len(f)
+        logits, kq = np.zeros((n, 6), np.float32), np.zeros(n, np.uint16)
+        check(self._h, self._L.pgpu_mlp_forward(self._h, _ptr(f), n, _ptr(logits), _ptr(kq)), "pgpu_mlp_forward")
+        return logits, kq
+
+    def mlp_grad(self, feat: np.ndarray, labels: np.ndarray):
+        """Gradient (1542 floats) and value of the mean cross-entropy at the current weights."""
+        f = np.ascontiguousarray(feat, np.float32)
+        y = np.ascontiguousarray(labels, np.int32)
+        g = np.zeros(_lib.KB_NPARAM, np.float32)
+        loss = C.c_float()
+        check(self._h, self._L.pgpu_mlp_grad(self._h, _ptr(f), _ptr(y), len(f), _ptr(g), C.byref(loss)),
+              "pgpu_mlp_grad")
+        return g, loss.value
+
     def enable_timing(self, on: bool = True) -> None:
         check(self._h, self._L.pgpu_enable_timing(self._h, int(on)), "pgpu_enable_timing")
 

@@ -1,5 +1,6 @@
 // The C ABI (include/proteus_gpu.h): argument checks, device memory, the order
 // of the stage launches, and host transfers.  No computation happens here.
+#include <algorithm>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -92,13 +93,44 @@ int build_mesh(pgpu_ctx* c, int64_t n, bool no_ghosts, bool all_cells) {
     mark(c, 1);
     CK(pgpu::launch_grid_sort(c));
     CK(pgpu::launch_query_list(c, all_cells));
+    // learned neighbour budget: features from the previous mesh, then one K per cell
+    pgpu::KBudget& kb = c->kb;
+    // (the first mesh of a simulation has no previous mesh to take features from)
+    const bool kb_on = kb.enabled && !all_cells && c->have_mesh;
+    c->use_kq = false;
+    if (kb_on) {
+        CK(pgpu::kb_features(c));
+        if (kb.trained) {
+            cudaError_t e = cudaSuccess;
+            uint16_t* kq = ensure<uint16_t>(c->kq, c->n_query + 1, &e);
+            CK(e);
+            CK(pgpu::kb_infer(c, (const float*)kb.feat.p, c->n_query, kq, nullptr));
+            c->use_kq = true;
+            c->knn_stride = std::min(c->prm.k, pgpu::kb_class_k(c->prm.dim, pgpu::KB_CLASSES - 1));
+        }
+    }
     mark(c, 2);
     CK(pgpu::launch_knn(c));
     mark(c, 3);
     CK(pgpu::launch_clip(c));
-    if (!all_cells && c->prm.k_fallback > c->prm.k && c->n_uncertified > 0) {
+    if (c->use_kq) {
+        // proposals the certificate rejected: KNN and clipping again at the plain budget
+        kb.cells = c->n_query;
+        kb.misses = c->n_uncertified;
+        const int K2 = std::max(c->prm.k, c->prm.k_fallback);
+        if (c->n_uncertified > 0) {
+            CK(pgpu::launch_fallback(c, K2));
+            CK(pgpu::kb_mark_miss(c, (const uint32_t*)c->fb_qs.p, c->n_refit));
+        }
+    } else if (!all_cells && c->prm.k_fallback > c->prm.k && c->n_uncertified > 0) {
         // cells whose certificate did not close within k: KNN and clipping again with the fallback budget
-        CK(pgpu::launch_fallback(c));
+        CK(pgpu::launch_fallback(c, c->prm.k_fallback));
+    }
+    if (kb_on && !kb.trained) {
+        // a plain-method step: its certified K train the proposal
+        CK(pgpu::kb_train_step(c));
+        kb.steps_seen++;
+        if (kb.steps_seen >= kb.train_steps) kb.trained = true;
     }
     mark(c, 4);
     c->have_mesh = true;
@@ -173,7 +205,8 @@ void pgpu_destroy(pgpu_ctx* c) {
                       &c->centroid, &c->f_nb, &c->f_own,    &c->f_geo,  &c->scan_tmp,  &c->scalars,    &c->rho,
                       &c->vel,   &c->energy,  &c->rho2,     &c->vel2,   &c->energy2,   &c->mass,       &c->mom,
                       &c->en,    &c->w4,      &c->we,       &c->red_tmp, &c->dl_ptr,   &c->dl_a,       &c->dl_b,
-                      &c->dl_c};
+                      &c->dl_c,  &c->kq,      &c->kb.w,     &c->kb.wbf,  &c->kb.adam_m, &c->kb.adam_v, &c->kb.part,
+                      &c->kb.feat, &c->kb.hist_vol, &c->kb.miss, &c->kb.ksum, &c->kb.labels, &c->kb.tmp_out};
     for (DevBuf* b : bufs) free_buf(*b);
     for (int i = 0; i < 6; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -585,6 +618,108 @@ int pgpu_sim_stats(pgpu_ctx* c, pgpu_stats* out) {
     out->refit_cells = c->n_refit;
     out->reclip_cells = c->n_reclip;
     out->uncertified_cells = c->n_uncertified;
+    return PGPU_OK;
+}
+
+// ------------------------------------------------------ learned neighbour budget
+int pgpu_kbudget_classes(int dim, int* k_out) {
+    if ((dim != 2 && dim != 3) || !k_out) return PGPU_EINVAL;
+    for (int i = 0; i < pgpu::KB_CLASSES; i++) k_out[i] = pgpu::kb_class_k(dim, i);
+    return PGPU_OK;
+}
+
+int pgpu_kbudget_enable(pgpu_ctx* c, int train_steps, int iters_per_step, double quantile, uint64_t seed) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (train_steps < 0 || iters_per_step < 1 || !(quantile > 0.0 && quantile <= 1.0))
+        return fail(c, PGPU_EINVAL, "pgpu_kbudget_enable: bad arguments");
+    pgpu::KBudget& kb = c->kb;
+    kb.enabled = true;
+    kb.train_steps = train_steps;
+    kb.iters = iters_per_step;
+    kb.quantile = (float)quantile;
+    kb.seed = seed;
+    kb.steps_seen = 0;
+    kb.trained = train_steps == 0;
+    kb.last_loss = 0.0;
+    kb.cells = kb.misses = 0;
+    CK(pgpu::kb_init_weights(c));
+    CK(cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+int pgpu_kbudget_stats(pgpu_ctx* c, pgpu_kbudget_info* out) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!out) return PGPU_EINVAL;
+    std::memset(out, 0, sizeof(*out));
+    const pgpu::KBudget& kb = c->kb;
+    out->active = kb.enabled && kb.trained ? 1 : 0;
+    out->steps_trained = std::min<int64_t>(kb.steps_seen, kb.train_steps);
+    out->last_loss = kb.last_loss;
+    if (c->use_kq) {
+        unsigned long long ks = 0;
+        CK(cudaMemcpyAsync(&ks, c->kb.ksum.p, sizeof(ks), cudaMemcpyDeviceToHost, c->stream));
+        CK(cudaStreamSynchronize(c->stream));
+        out->cells = kb.cells;
+        out->misses = kb.misses;
+        out->mean_k = kb.cells ? (double)ks / (double)kb.cells : 0.0;
+    }
+    return PGPU_OK;
+}
+
+int pgpu_kbudget_weights(pgpu_ctx* c, float* get, const float* set) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->kb.w.p) CK(pgpu::kb_init_weights(c));
+    float* w = (float*)c->kb.w.p;
+    if (get) CK(cudaMemcpyAsync(get, w, pgpu::KB_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    if (set) {
+        CK(cudaMemcpyAsync(w, set, pgpu::KB_NPARAM * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        CK(pgpu::kb_sync_bf16(c));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+int pgpu_mlp_forward(pgpu_ctx* c, const float* feat, int64_t n, float* logits, uint16_t* kq) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (n < 0 || (n > 0 && !feat)) return fail(c, PGPU_EINVAL, "pgpu_mlp_forward: bad arguments");
+    if (!c->kb.w.p) CK(pgpu::kb_init_weights(c));
+    cudaError_t e = cudaSuccess;
+    float* df = ensure<float>(c->dl_a, (size_t)n * pgpu::KB_FEATURES + 8, &e);
+    float* dl = ensure<float>(c->dl_b, (size_t)n * pgpu::KB_CLASSES + 8, &e);
+    uint16_t* dk = ensure<uint16_t>(c->dl_c, (size_t)n + 8, &e);
+    CK(e);
+    if (n > 0) {
+        CK(cudaMemcpyAsync(df, feat, (size_t)n * pgpu::KB_FEATURES * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+        CK(pgpu::kb_infer(c, df, n, dk, dl));
+        if (logits)
+            CK(cudaMemcpyAsync(logits, dl, (size_t)n * pgpu::KB_CLASSES * sizeof(float), cudaMemcpyDeviceToHost,
+                               c->stream));
+        if (kq) CK(cudaMemcpyAsync(kq, dk, (size_t)n * sizeof(uint16_t), cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+int pgpu_mlp_grad(pgpu_ctx* c, const float* feat, const int32_t* labels, int64_t n, float* grad, float* loss) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (n <= 0 || !feat || !labels) return fail(c, PGPU_EINVAL, "pgpu_mlp_grad: bad arguments");
+    if (!c->kb.w.p) CK(pgpu::kb_init_weights(c));
+    cudaError_t e = cudaSuccess;
+    float* df = ensure<float>(c->dl_a, (size_t)n * pgpu::KB_FEATURES + 8, &e);
+    int32_t* dy = ensure<int32_t>(c->dl_b, (size_t)n + 8, &e);
+    CK(e);
+    CK(cudaMemcpyAsync(df, feat, (size_t)n * pgpu::KB_FEATURES * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(dy, labels, (size_t)n * sizeof(int32_t), cudaMemcpyHostToDevice, c->stream));
+    CK(pgpu::kb_grad(c, df, dy, n, nullptr, n, false));
+    const float* g = (const float*)c->kb.tmp_out.p;
+    if (grad) CK(cudaMemcpyAsync(grad, g, pgpu::KB_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    if (loss) CK(cudaMemcpyAsync(loss, g + pgpu::KB_NPARAM, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return PGPU_OK;
 }
 

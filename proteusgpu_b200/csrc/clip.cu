@@ -166,6 +166,7 @@ struct ClipParams {
     const void* spts;
     const void* ext;
     const uint32_t* knn;
+    const uint16_t* kq;     // optional: neighbour budget of query slot t (<= K, the list stride)
     const uint32_t* ghost_src;
     const uint32_t* ghost_code;
     int64_t nq;
@@ -442,8 +443,8 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
     const uint32_t e = P.perm[s];
     const PT sp = spts[s];
     const double sx = sp.x, sy = sp.y, sz = pz(sp);
-    const int K = P.K;
-    const uint32_t* kl = P.knn + (size_t)tq * K;
+    const int K = P.kq ? (int)P.kq[tq] : P.K;  // per-cell budget (learned K) within rows of P.K
+    const uint32_t* kl = P.knn + (size_t)tq * P.K;
 
     // ---- ConvexCell::ConvexCell (cell.cpp:42-104): bounding box [-1e-14, 1 + 1e-14]^D
     const double beps = 1e-14;
@@ -919,8 +920,8 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip32(ClipParams P) {
     const uint32_t e = P.perm[s];
     const PT sp = spts[s];
     const double sx = sp.x, sy = sp.y, sz = pz(sp);
-    const int K = P.K;
-    const uint32_t* kl = P.knn + (size_t)tq * K;
+    const int K = P.kq ? (int)P.kq[tq] : P.K;  // per-cell budget (learned K) within rows of P.K
+    const uint32_t* kl = P.knn + (size_t)tq * P.K;
 
     // bounding box in the local frame: w' = w + n . seed
     const double beps = 1e-14;
@@ -1272,7 +1273,7 @@ cudaError_t select_cells(pgpu_ctx* c, int code, bool hydro_only, bool as_slots, 
 // reset: start a fresh face array (else faces are appended to the current one).
 cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const uint32_t* knn, bool reset,
                       unsigned long long* fc, unsigned* overflow, unsigned* uncert, bool fp32 = false,
-                      unsigned* reclip = nullptr, const uint32_t* slots = nullptr) {
+                      unsigned* reclip = nullptr, const uint32_t* slots = nullptr, const uint16_t* kq = nullptr) {
     const int D = c->prm.dim;
     cudaError_t e = cudaSuccess;
     DevScalars* sc = (DevScalars*)c->scalars.p;
@@ -1287,6 +1288,7 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     P.spts = c->spts.p;
     P.ext = c->ext.p;
     P.knn = knn;
+    P.kq = kq;
     P.ghost_src = (const uint32_t*)c->ghost_src.p;
     P.ghost_code = (const uint32_t*)c->ghost_code.p;
     P.nq = nq;
@@ -1367,8 +1369,9 @@ cudaError_t launch_clip(pgpu_ctx* c) {
         unsigned long long fc = 0;
         unsigned of = 0, unc = 0, rc = 0;
         const bool fp32 = c->prm.precision == PGPU_CLIP_FP32;
-        if ((e = clip_pass(c, (const uint32_t*)c->qs.p, c->n_query, c->prm.k, (const uint32_t*)c->knn.p, true, &fc, &of,
-                           &unc, fp32, &rc)))
+        const uint16_t* kq = c->use_kq ? (const uint16_t*)c->kq.p : nullptr;
+        if ((e = clip_pass(c, (const uint32_t*)c->qs.p, c->n_query, c->knn_stride, (const uint32_t*)c->knn.p, true, &fc,
+                           &of, &unc, fp32, &rc, nullptr, kq)))
             return e;
         c->n_reclip = rc;
         if (!of && rc > 0) {
@@ -1378,8 +1381,8 @@ cudaError_t launch_clip(pgpu_ctx* c) {
             uint32_t nr = 0;
             if ((e = select_cells(c, ST_RECLIP, false, true, fq, &nr))) return e;
             unsigned unc2 = 0, rc2 = 0;
-            if ((e = clip_pass(c, (const uint32_t*)c->qs.p, nr, c->prm.k, (const uint32_t*)c->knn.p, false, &fc, &of,
-                               &unc2, false, &rc2, fq)))
+            if ((e = clip_pass(c, (const uint32_t*)c->qs.p, nr, c->knn_stride, (const uint32_t*)c->knn.p, false, &fc, &of,
+                               &unc2, false, &rc2, fq, kq)))
                 return e;
             unc += unc2;
         }
@@ -1392,10 +1395,10 @@ cudaError_t launch_clip(pgpu_ctx* c) {
     return cudaErrorMemoryAllocation;
 }
 
-cudaError_t launch_fallback(pgpu_ctx* c) {
+cudaError_t launch_fallback(pgpu_ctx* c, int K2) {
     cudaError_t e = cudaSuccess;
     const int64_t nq = c->n_query;
-    const int K2 = c->prm.k_fallback;
+    c->n_refit = 0;
     uint32_t* fq = ensure<uint32_t>(c->fb_qs, nq + 1, &e);
     if (e) return e;
     uint32_t nf = 0;
@@ -1403,7 +1406,7 @@ cudaError_t launch_fallback(pgpu_ctx* c) {
     if (nf == 0) return cudaSuccess;
     uint32_t* kl = ensure<uint32_t>(c->fb_knn, (size_t)nf * K2 + 1, &e);
     if (e) return e;
-    if ((e = launch_knn_list(c, fq, nf, K2, kl))) return e;
+    if ((e = launch_knn_list(c, fq, nf, K2, kl, nullptr, K2))) return e;
     unsigned long long fc = 0;
     unsigned of = 0, unc = 0;
     if ((e = clip_pass(c, fq, nf, K2, kl, false, &fc, &of, &unc))) return e;

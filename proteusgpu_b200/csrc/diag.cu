@@ -1,5 +1,5 @@
-// Diagnostics with no reference counterpart: the FP64 FMA rate of the device,
-// the denominator of the FP64-pipe roofline of the KNN and clipping kernels.
+// Diagnostics with no reference counterpart: the FP64 and FP32 FMA rates of the
+// device, the denominators of the pipe rooflines of the KNN and clipping kernels.
 #include <cuda_runtime.h>
 
 #include "pgpu_ctx.h"
@@ -8,29 +8,29 @@ namespace {
 
 constexpr int CHAINS = 8;  // independent FMA chains per thread hide the pipe latency
 
-__global__ void k_fp64_fma(double* __restrict__ sink, int iters, double a, double b) {
-    double x[CHAINS];
+template <class T>
+__global__ void k_fma(T* __restrict__ sink, int iters, T a, T b) {
+    T x[CHAINS];
 #pragma unroll
-    for (int c = 0; c < CHAINS; c++) x[c] = (threadIdx.x + c) * 1e-7;
+    for (int c = 0; c < CHAINS; c++) x[c] = (T)((threadIdx.x + c) * 1e-7);
     for (int i = 0; i < iters; i++) {
 #pragma unroll
         for (int c = 0; c < CHAINS; c++) x[c] = fma(x[c], a, b);
     }
-    double s = 0;
+    T s = 0;
 #pragma unroll
     for (int c = 0; c < CHAINS; c++) s += x[c];
-    if (s == 1234.5678) sink[threadIdx.x] = s;  // never true; keeps the chains alive
+    if (s == (T)1234.5678) sink[threadIdx.x] = s;  // never true; keeps the chains alive
 }
 
-}  // namespace
-
-extern "C" int pgpu_fp64_peak(int device, float ms, double* tflops) {
+template <class T>
+int fma_peak(int device, float ms, double* tflops) {
     if (!tflops || ms <= 0) return PGPU_EINVAL;
     if (cudaSetDevice(device) != cudaSuccess) return PGPU_ECUDA;
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return PGPU_ECUDA;
-    double* sink = nullptr;
-    if (cudaMalloc(&sink, 1024 * sizeof(double)) != cudaSuccess) return PGPU_ECUDA;
+    T* sink = nullptr;
+    if (cudaMalloc(&sink, 1024 * sizeof(T)) != cudaSuccess) return PGPU_ECUDA;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -39,7 +39,7 @@ extern "C" int pgpu_fp64_peak(int device, float ms, double* tflops) {
     float t = 0;
     for (int rep = 0; rep < 12; rep++) {  // grow the loop until one launch lasts about `ms`
         cudaEventRecord(e0);
-        k_fp64_fma<<<blocks, threads>>>(sink, iters, 0.999999, 1e-9);
+        k_fma<T><<<blocks, threads>>>(sink, iters, (T)0.999999, (T)1e-9);
         pgpu::count_launches(1);
         cudaEventRecord(e1);
         if (cudaEventSynchronize(e1) != cudaSuccess) break;
@@ -55,3 +55,9 @@ extern "C" int pgpu_fp64_peak(int device, float ms, double* tflops) {
     cudaFree(sink);
     return cudaGetLastError() == cudaSuccess ? PGPU_OK : PGPU_ECUDA;
 }
+
+}  // namespace
+
+extern "C" int pgpu_fp64_peak(int device, float ms, double* tflops) { return fma_peak<double>(device, ms, tflops); }
+
+extern "C" int pgpu_fp32_peak(int device, float ms, double* tflops) { return fma_peak<float>(device, ms, tflops); }

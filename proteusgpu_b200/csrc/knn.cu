@@ -222,13 +222,14 @@ template <int D>
 __global__ void __launch_bounds__(KNN_WARPS * 32)
     k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm,
           const uint32_t* __restrict__ bin_start, int G, const int2* __restrict__ table, int table_n, int table_r,
-          const uint32_t* __restrict__ qs, int64_t nq, int K, uint32_t* __restrict__ out,
-          unsigned long long* __restrict__ cand_counter) {
+          const uint32_t* __restrict__ qs, int64_t nq, int K, const uint16_t* __restrict__ kq, int stride,
+          uint32_t* __restrict__ out, unsigned long long* __restrict__ cand_counter) {
     __shared__ KnnSmem S;
     using PT = typename PointOf<D>::type;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t t = (int64_t)blockIdx.x * KNN_WARPS + w;
     if (t >= nq) return;  // warp-uniform
+    if (kq) K = kq[t];
     const int nrows = (K + 31) >> 5;
     for (int r = 0; r < nrows; r++) {
         S.row_d[w][r * 32 + lane] = CUDART_INF;
@@ -317,7 +318,7 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
         flush_queue(S, w, lane, nrows, K, qn, thr_d, thr_i);
     }
     __syncwarp();
-    for (int idx = lane; idx < K; idx += 32) out[t * K + idx] = S.row_i[w][idx];
+    for (int idx = lane; idx < K; idx += 32) out[t * stride + idx] = S.row_i[w][idx];
     if (cand_counter && lane == 0) atomicAdd(cand_counter, ncand);
 }
 
@@ -360,7 +361,8 @@ cudaError_t build_knn_table(pgpu_ctx* c) {
     return cudaStreamSynchronize(c->stream);
 }
 
-cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, uint32_t* out) {
+cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, uint32_t* out, const uint16_t* kq,
+                            int stride) {
     if (nq <= 0) return cudaSuccess;
     cudaError_t e = cudaSuccess;
     if (c->knn_table_n == 0 && (e = build_knn_table(c))) return e;
@@ -371,24 +373,26 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
     const int2* tab = (const int2*)c->knn_table.p;
     if (c->prm.dim == 2)
         k_knn<2><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double2*)c->spts.p, perm, bs, c->grid_G, tab,
-                                                           c->knn_table_n, c->knn_table_r, qs, nq, K, out,
-                                                           &sc->knn_cand);
+                                                           c->knn_table_n, c->knn_table_r, qs, nq, K, kq, stride,
+                                                           out, &sc->knn_cand);
     else
         k_knn<3><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double4*)c->spts.p, perm, bs, c->grid_G, tab,
-                                                           c->knn_table_n, c->knn_table_r, qs, nq, K, out,
-                                                           &sc->knn_cand);
+                                                           c->knn_table_n, c->knn_table_r, qs, nq, K, kq, stride,
+                                                           out, &sc->knn_cand);
     count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_knn(pgpu_ctx* c) {
     cudaError_t e = cudaSuccess;
-    const int K = c->prm.k;
+    const int K = c->use_kq ? c->knn_stride : c->prm.k;
+    if (!c->use_kq) c->knn_stride = K;
     uint32_t* out = ensure<uint32_t>(c->knn, (size_t)c->n_query * K + 1, &e);
     if (e) return e;
     DevScalars* sc = (DevScalars*)c->scalars.p;
     if ((e = cudaMemsetAsync(&sc->knn_cand, 0, sizeof(unsigned long long), c->stream))) return e;
-    return launch_knn_list(c, (const uint32_t*)c->qs.p, c->n_query, K, out);
+    return launch_knn_list(c, (const uint32_t*)c->qs.p, c->n_query, K, out,
+                           c->use_kq ? (const uint16_t*)c->kq.p : nullptr, K);
 }
 
 }  // namespace pgpu

@@ -41,6 +41,35 @@ struct DevScalars {
     double sums[5];                 // mass, mom x/y/z, energy
 };
 
+// Learned neighbour budget: a per-cell MLP (8 features -> 32 -> 32 -> 6 classes,
+// GELU) proposes each cell's K; training and inference run on the device.
+constexpr int KB_FEATURES = 8;
+constexpr int KB_HIDDEN = 32;
+constexpr int KB_CLASSES = 6;
+// FP32 master parameters: W1[32][8], b1[32], W2[32][32], b2[32], W3[6][32], b3[6]
+constexpr int KB_W1 = 0, KB_B1 = 256, KB_W2 = 288, KB_B2 = 1312, KB_W3 = 1344, KB_B3 = 1536;
+constexpr int KB_NPARAM = 1542;
+constexpr int KB_PART = 1544;  // per-warp partial gradient row (parameters, loss, pad)
+// BF16 operand copies (u16): W1[32][8], W2[32][32], W2^T, W3[8][32] (rows 6-7 zero), W3^T[32][8]
+constexpr int KB_BW1 = 0, KB_BW2 = 256, KB_BW2T = 1280, KB_BW3 = 2304, KB_BW3T = 2560, KB_NBF = 2816;
+constexpr int KB_GRAD_BLOCKS = 148, KB_GRAD_WARPS = 4;
+
+struct KBudget {
+    bool enabled = false;
+    bool trained = false;
+    int train_steps = 0;       // steps of the plain method whose certified K train the model
+    int iters = 64;            // optimiser iterations per training step
+    int batch = 16384;         // cells per iteration
+    float quantile = 0.99f;    // smallest class whose cumulative probability reaches this
+    float lr = 3e-3f;
+    uint64_t seed = 1;
+    int64_t steps_seen = 0, adam_t = 0;
+    double last_loss = 0.0;
+    int64_t cells = 0, misses = 0;  // last step: cells proposed, cells that needed the fallback
+    double mean_k = 0.0;            // last step: mean proposed K
+    DevBuf w, wbf, adam_m, adam_v, part, feat, hist_vol, miss, ksum, labels, tmp_out;
+};
+
 }  // namespace pgpu
 
 struct pgpu_ctx {
@@ -68,7 +97,10 @@ struct pgpu_ctx {
     pgpu::DevBuf bin_cnt, bin_start, bin_key;  // grid bins (Morton slots) and per-point key
     pgpu::DevBuf spts, perm, inv;  // sorted points, sorted->ext id, ext id->sorted
     pgpu::DevBuf qflag, qoff, qs;  // query list (sorted positions of the cells to compute)
-    pgpu::DevBuf knn;          // n_query x K ext ids
+    pgpu::DevBuf knn;          // n_query rows of knn_stride ext ids
+    int knn_stride = 0;        // ids per row: prm.k, or the largest learned budget
+    pgpu::DevBuf kq;           // u16 per query slot: learned neighbour budget
+    bool use_kq = false;       // this step's lists and clip use kq
     pgpu::DevBuf vol, fptr, fcnt, status, certk, centroid;  // per cell, indexed by ext id
     pgpu::DevBuf f_nb, f_own, f_geo;  // faces: ext id, owner|code, (normal, area)
     pgpu::DevBuf scan_tmp;     // scan block sums
@@ -87,6 +119,7 @@ struct pgpu_ctx {
     int64_t n_refit = 0;        // cells recomputed with the fallback budget in the last step
     int64_t n_reclip = 0;       // cells the FP32 clip handed to the FP64 clip in the last step
     pgpu::DevBuf fb_qs, fb_knn; // fallback query list and lists
+    pgpu::KBudget kb;           // learned neighbour budget (optional form)
 };
 
 namespace pgpu {
@@ -103,10 +136,23 @@ cudaError_t launch_grid_sort(pgpu_ctx* c);
 cudaError_t launch_query_list(pgpu_ctx* c, bool all_cells);
 // knn.cu
 cudaError_t launch_knn(pgpu_ctx* c);
-cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, uint32_t* out);
+// K neighbours of each query (or kq[t] of query t, <= K) into rows of `stride` ids
+cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, uint32_t* out, const uint16_t* kq,
+                            int stride);
 // clip.cu
 cudaError_t launch_clip(pgpu_ctx* c);
-cudaError_t launch_fallback(pgpu_ctx* c);
+// uncertified hydro cells of the last clip: KNN and clipping again with budget K2
+cudaError_t launch_fallback(pgpu_ctx* c, int K2);
+// kbudget.cu
+cudaError_t kb_init_weights(pgpu_ctx* c);
+cudaError_t kb_features(pgpu_ctx* c);                 // before the step's clip (reads the previous mesh)
+cudaError_t kb_infer(pgpu_ctx* c, const float* feat, int64_t n, uint16_t* kq, float* logits);
+cudaError_t kb_train_step(pgpu_ctx* c);               // after the step's clip (labels = certified K)
+cudaError_t kb_grad(pgpu_ctx* c, const float* feat, const int32_t* labels, int64_t n, const uint32_t* sample,
+                    int64_t nb, bool update);
+cudaError_t kb_mark_miss(pgpu_ctx* c, const uint32_t* sorted_pos, int64_t n);
+cudaError_t kb_sync_bf16(pgpu_ctx* c);               // BF16 operand copies from the FP32 master weights
+int kb_class_k(int dim, int cls);
 // hydro.cu
 cudaError_t launch_prim_dt(pgpu_ctx* c, double cfl, double fixed_dt);
 cudaError_t launch_flux_update(pgpu_ctx* c, double fixed_dt);
