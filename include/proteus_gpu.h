@@ -211,6 +211,8 @@ typedef struct {
     int64_t refit_cells;        /* cells recomputed with k_fallback in the last step */
     int64_t uncertified_cells;  /* hydro cells still without a certificate after it */
     int64_t reclip_cells;       /* cells the FP32 clip handed to the FP64 clip in the last step */
+    int64_t pruned_cells;       /* moving-mesh steps: hydro cells whose certificate needed more than the
+                                   neighbour budget(s), clipped by walking the grid instead (extension) */
 } pgpu_stats;
 
 /* Statistics of the last step (synchronises the stream). */

@@ -70,7 +70,9 @@ int check_ctx(pgpu_ctx* c) {
 }
 
 void mark(pgpu_ctx* c, int i) {
-    if (c->timing) cudaEventRecord(c->ev[i], c->stream);
+    if (!c->timing) return;
+    if (i == 0) c->ev_mask = 0;
+    if (cudaEventRecord(c->ev[i], c->stream) == cudaSuccess) c->ev_mask |= 1u << i;
 }
 
 DevScalars* scalars(pgpu_ctx* c) { return (DevScalars*)c->scalars.p; }
@@ -126,6 +128,10 @@ int build_mesh(pgpu_ctx* c, int64_t n, bool no_ghosts, bool all_cells) {
         // cells whose certificate did not close within k: KNN and clipping again with the fallback budget
         CK(pgpu::launch_fallback(c, c->prm.k_fallback));
     }
+    if (!all_cells && c->n_uncertified > 0) {
+        // cells whose security sphere reaches past every budget (beside dense clumps): grid walk
+        CK(pgpu::launch_pruned(c));
+    }
     if (kb_on && !kb.trained) {
         // a plain-method step: its certified K train the proposal
         CK(pgpu::kb_train_step(c));
@@ -138,10 +144,18 @@ int build_mesh(pgpu_ctx* c, int64_t n, bool no_ghosts, bool all_cells) {
     return PGPU_OK;
 }
 
+// stages between consecutive recorded events (a mesh build alone records no hydro stage)
 void collect_times(pgpu_ctx* c) {
     if (!c->timing) return;
-    cudaEventSynchronize(c->ev[5]);
-    for (int i = 0; i < 5; i++) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
+    for (int i = 5; i >= 0; i--)
+        if (c->ev_mask & (1u << i)) {
+            cudaEventSynchronize(c->ev[i]);
+            break;
+        }
+    for (int i = 0; i < 5; i++) {
+        c->stage_ms[i] = 0.0f;
+        if ((c->ev_mask >> i & 3u) == 3u) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
+    }
 }
 
 }  // namespace
@@ -206,7 +220,8 @@ void pgpu_destroy(pgpu_ctx* c) {
                       &c->vel,   &c->energy,  &c->rho2,     &c->vel2,   &c->energy2,   &c->mass,       &c->mom,
                       &c->en,    &c->w4,      &c->we,       &c->red_tmp, &c->dl_ptr,   &c->dl_a,       &c->dl_b,
                       &c->dl_c,  &c->kq,      &c->kb.w,     &c->kb.wbf,  &c->kb.adam_m, &c->kb.adam_v, &c->kb.part,
-                      &c->kb.feat, &c->kb.hist_vol, &c->kb.miss, &c->kb.ksum, &c->kb.labels, &c->kb.tmp_out};
+                      &c->kb.feat, &c->kb.hist_vol, &c->kb.miss, &c->kb.ksum, &c->kb.labels, &c->kb.tmp_out,
+                      &c->bin_lvl, &c->sub_off, &c->sub_cnt, &c->sub_start};
     for (DevBuf* b : bufs) free_buf(*b);
     for (int i = 0; i < 6; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -618,6 +633,7 @@ int pgpu_sim_stats(pgpu_ctx* c, pgpu_stats* out) {
     out->refit_cells = c->n_refit;
     out->reclip_cells = c->n_reclip;
     out->uncertified_cells = c->n_uncertified;
+    out->pruned_cells = c->n_pruned;
     return PGPU_OK;
 }
 

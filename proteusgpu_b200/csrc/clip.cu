@@ -428,6 +428,235 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
     }
 }
 
+// One step of ConvexCell::clip_by_plane (cell.cpp:120-205) in FP64: the
+// bisector of the seed and ext point z = (bx, by, bz).  CLIP_FAIL sets status
+// (and the vertex distance the final certificate uses); CLIP_NONE leaves the
+// cell unchanged; CLIP_CUT updates the cell and v_dist.
+// REUSE (grid walk only): with all MAX_P plane slots taken, a neighbour plane
+// that no vertex uses any more gives its slot to the new plane instead of the
+// cell failing with VERTEX_OVERFLOW as the reference does.
+constexpr int CLIP_FAIL = -1, CLIP_NONE = 0, CLIP_CUT = 1;
+
+template <int D, bool REUSE = false>
+__device__ __forceinline__ int clip_by(WarpCell& W, int lane, uint32_t z, double bx, double by, double bz, double sx,
+                                       double sy, double sz, int robust, int& nb_v, int& nb_t, int& status,
+                                       double& v_dist, double& fail_vdist) {
+    int cur = nb_v;
+    if (nb_v >= MAX_P) {  // new_halfplane (cell.cpp:159-162)
+        int slot = -1;
+        if (REUSE) {
+            unsigned long long used = (1ull << (2 * D)) - 1ull;  // the box planes keep their slots
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                const int i = lane + 32 * j;
+                if (i < nb_t) {
+                    const uint32_t tv = W.tri[i];
+                    used |= (1ull << tri_a(tv)) | (1ull << tri_b(tv)) | (D == 3 ? (1ull << tri_c(tv)) : 0ull);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) used |= __shfl_xor_sync(FULL, used, o);
+            if (~used) slot = __ffsll((long long)~used) - 1;
+        }
+        if (slot < 0) {
+            status = ST_VERTEX_OVERFLOW;
+            fail_vdist = v_dist;
+            return CLIP_FAIL;
+        }
+        cur = slot;
+    }
+    // new_halfplane: bisector plane (cell.cpp:164-168)
+    const double dx = sx - bx, dy = sy - by, dz = sz - bz;
+    const double ax = sx + bx, ay = sy + by, az = sz + bz;
+    const double dot = ax * dx + ay * dy + az * dz;
+    const double4 eq = make_double4(dx, dy, dz, -dot / 2.0);
+    if (lane == 0) W.hp[cur] = eq;
+
+    // 1. conflicts
+    uint32_t cm[3];
+    bool near = false;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        int i = lane + 32 * j;
+        bool cf = false;
+        if (i < nb_t) cf = in_conflict<D>(W.hp, W.tri[i], eq, &near, robust);
+        cm[j] = __ballot_sync(FULL, cf);
+    }
+    const int nb_r = __popc(cm[0]) + __popc(cm[1]) + __popc(cm[2]);
+    const uint32_t km[3] = {~cm[0], ~cm[1], ~cm[2]};
+    if (__any_sync(FULL, near)) {  // needs_exact_predicates: the reference keeps only the kept vertices
+        status = ST_NEEDS_EXACT_PREDICATES;
+        fail_vdist = max_vd2(W, nb_t, lane, km);
+        return CLIP_FAIL;
+    }
+    if (nb_r == 0) return CLIP_NONE;  // plane does not cut the cell: dropped (cell.cpp:133-136)
+    __syncwarp();  // hp[cur] visible
+
+    // 2. cavity boundary
+    const int kept = nb_t - nb_r;
+    int n_new = 0;
+    bool bad = false;
+    uint32_t my_new[9];
+    int my_new_pos[9];
+    int my_new_cnt = 0;
+    if (D == 2) {
+        uint32_t lo = 0, hi = 0;  // XOR of the lines of removed vertices
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            int i = lane + 32 * j;
+            if (i < nb_t && ((cm[j] >> lane) & 1u)) {
+                uint32_t tv = W.tri[i];
+                uint32_t a = tri_a(tv), b = tri_b(tv);
+                if (a < 32) lo ^= 1u << a; else hi ^= 1u << (a - 32);
+                if (b < 32) lo ^= 1u << b; else hi ^= 1u << (b - 32);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            lo ^= __shfl_xor_sync(FULL, lo, o);
+            hi ^= __shfl_xor_sync(FULL, hi, o);
+        }
+        unsigned long long xm = (unsigned long long)lo | ((unsigned long long)hi << 32);
+        if (__popcll(xm) < 2) {
+            bad = true;
+        } else {
+            int b0 = __ffsll((long long)xm) - 1;
+            unsigned long long x2 = xm & (xm - 1);
+            int b1 = __ffsll((long long)x2) - 1;
+            n_new = 2;
+            if (lane < 2) {
+                int j = lane == 0 ? b0 : b1;
+                const double4 hi_ = W.hp[cur], hj = W.hp[j];
+                double rw = det2(hi_.x, hi_.y, hj.x, hj.y);  // new_vertex orientation (cell.cpp:351-359)
+                my_new[0] = rw > 0 ? pack3(j, cur, 0) : pack3(cur, j, 0);
+                my_new_pos[0] = lane;
+                my_new_cnt = 1;
+            }
+        }
+    } else {
+        unsigned long long* em = W.u.b.emask;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            int i = lane + 32 * j;
+            if (i < nb_t && ((cm[j] >> lane) & 1u)) {
+                uint32_t tv = W.tri[i];
+                uint32_t a = tri_a(tv), b = tri_b(tv), c = tri_c(tv);
+                atomicOr(&em[a], 1ull << b);
+                atomicOr(&em[b], 1ull << c);
+                atomicOr(&em[c], 1ull << a);
+            }
+        }
+        __syncwarp();
+        unsigned long long src = 0ull;
+        int base = 0;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            int i = lane + 32 * j;
+            bool rem = i < nb_t && ((cm[j] >> lane) & 1u);
+            uint32_t tv = rem ? W.tri[i] : 0u;
+            uint32_t v3[3] = {tri_a(tv), tri_b(tv), tri_c(tv)};
+#pragma unroll
+            for (int ed = 0; ed < 3; ed++) {
+                uint32_t x = v3[ed], y = v3[(ed + 1) % 3];
+                bool isb = rem && !((em[y] >> x) & 1ull);
+                unsigned bal = __ballot_sync(FULL, isb);
+                if (isb) {
+                    my_new[my_new_cnt] = pack3(cur, x, y);
+                    my_new_pos[my_new_cnt] = base + __popc(bal & ((1u << lane) - 1u));
+                    my_new_cnt++;
+                    src |= 1ull << x;
+                    W.u.b.nxt[x] = (unsigned char)y;
+                }
+                base += __popc(bal);
+            }
+        }
+        n_new = base;
+        // OR-reduce the source planes; a simple cycle visits each source once
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) src |= __shfl_xor_sync(FULL, src, o);
+        __syncwarp();
+        bool ok = __popcll(src) == n_new && n_new >= 3;
+        if (ok && lane == 0) {
+            int x0 = __ffsll((long long)src) - 1, x = x0;
+            for (int st = 1; st <= n_new; st++) {
+                x = W.u.b.nxt[x];
+                if (!((src >> x) & 1ull) || (x == x0 && st < n_new)) {
+                    ok = false;
+                    break;
+                }
+            }
+            if (x != x0) ok = false;
+        }
+        ok = __shfl_sync(FULL, ok ? 1 : 0, 0) != 0;
+        bad = !ok;
+        // clear the edge rows of removed vertices
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            int i = lane + 32 * j;
+            if (i < nb_t && ((cm[j] >> lane) & 1u)) {
+                uint32_t tv = W.tri[i];
+                em[tri_a(tv)] = 0ull;
+                em[tri_b(tv)] = 0ull;
+                em[tri_c(tv)] = 0ull;
+            }
+        }
+        __syncwarp();
+    }
+    if (bad) {
+        status = ST_INCONSISTENT_BOUNDARY;
+        fail_vdist = max_vd2(W, nb_t, lane, km);
+        return CLIP_FAIL;
+    }
+    // 3. new vertices and their certificate distances
+    double nd2[9];
+    double newmax = 0.0;
+    for (int q = 0; q < my_new_cnt; q++) {
+        double x, y, zz;
+        vertex_pos<D>(W.hp, my_new[q], x, y, zz);
+        nd2[q] = seed_d2(x, y, zz, sx, sy, sz);
+        newmax = nan_max(newmax, nd2[q]);
+    }
+    if (kept + n_new >= MAX_T) {  // new_vertex overflow (cell.cpp:347-350)
+        status = ST_TRIANGLE_OVERFLOW;
+        fail_vdist = nan_max(max_vd2(W, nb_t, lane, km), warp_max(newmax));
+        return CLIP_FAIL;
+    }
+    // compaction: kept vertices in order, then the new ones
+    uint32_t kt[3];
+    double kd[3];
+    int kp[3];
+    int before = 0;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int i = lane + 32 * j;
+        const int nvalid = nb_t - 32 * j;
+        const uint32_t vm = nvalid >= 32 ? FULL : (nvalid > 0 ? ((1u << nvalid) - 1u) : 0u);
+        const uint32_t kmj = km[j] & vm;
+        const bool keep = (kmj >> lane) & 1u;
+        kt[j] = keep ? W.tri[i] : 0u;
+        kd[j] = keep ? W.vd2[i] : 0.0;
+        kp[j] = keep ? before + __popc(kmj & ((1u << lane) - 1u)) : -1;
+        before += __popc(kmj);
+    }
+    __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 3; j++)
+        if (kp[j] >= 0) {
+            W.tri[kp[j]] = kt[j];
+            W.vd2[kp[j]] = kd[j];
+        }
+    for (int q = 0; q < my_new_cnt; q++) {
+        W.tri[kept + my_new_pos[q]] = my_new[q];
+        W.vd2[kept + my_new_pos[q]] = nd2[q];
+    }
+    if (lane == 0) W.vid[cur] = (int)z;
+    if (cur == nb_v) nb_v++;
+    nb_t = kept + n_new;
+    __syncwarp();
+    v_dist = max_vd2(W, nb_t, lane, nullptr);
+    return CLIP_CUT;
+}
+
 template <int D>
 __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
     using PT = typename PointOf<D>::type;
@@ -497,207 +726,9 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
         const PT B = ext[z];
         const double bx = B.x, by = B.y, bz = pz(B);
         const double d2B = seed_d2(bx, by, bz, sx, sy, sz);  // (B - seed)^2 as cell.cpp:381-382
-        if (nb_v >= MAX_P) {  // new_halfplane (cell.cpp:159-162)
-            status = ST_VERTEX_OVERFLOW;
-            fail_vdist = v_dist;
+        if (clip_by<D>(W, lane, z, bx, by, bz, sx, sy, sz, P.robust, nb_v, nb_t, status, v_dist, fail_vdist) ==
+            CLIP_FAIL)
             break;
-        }
-        // new_halfplane: bisector plane (cell.cpp:164-168)
-        const double dx = sx - bx, dy = sy - by, dz = sz - bz;
-        const double ax = sx + bx, ay = sy + by, az = sz + bz;
-        const double dot = ax * dx + ay * dy + az * dz;
-        const double4 eq = make_double4(dx, dy, dz, -dot / 2.0);
-        const int cur = nb_v;
-        if (lane == 0) W.hp[cur] = eq;
-
-        // 1. conflicts
-        uint32_t cm[3];
-        bool near = false;
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            int i = lane + 32 * j;
-            bool cf = false;
-            if (i < nb_t) cf = in_conflict<D>(W.hp, W.tri[i], eq, &near, P.robust);
-            cm[j] = __ballot_sync(FULL, cf);
-        }
-        const int nb_r = __popc(cm[0]) + __popc(cm[1]) + __popc(cm[2]);
-        const uint32_t km[3] = {~cm[0], ~cm[1], ~cm[2]};
-        if (__any_sync(FULL, near)) {  // needs_exact_predicates: the reference keeps only the kept vertices
-            status = ST_NEEDS_EXACT_PREDICATES;
-            fail_vdist = max_vd2(W, nb_t, lane, km);
-            break;
-        }
-        if (nb_r == 0) {  // plane does not cut the cell: dropped (cell.cpp:133-136)
-            if (d2B > 4 * v_dist) {
-                certk = k + 1;
-                break;
-            }
-            continue;
-        }
-        __syncwarp();  // hp[cur] visible
-
-        // 2. cavity boundary
-        const int kept = nb_t - nb_r;
-        int n_new = 0;
-        bool bad = false;
-        uint32_t my_new[9];
-        int my_new_pos[9];
-        int my_new_cnt = 0;
-        if (D == 2) {
-            uint32_t lo = 0, hi = 0;  // XOR of the lines of removed vertices
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                int i = lane + 32 * j;
-                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
-                    uint32_t tv = W.tri[i];
-                    uint32_t a = tri_a(tv), b = tri_b(tv);
-                    if (a < 32) lo ^= 1u << a; else hi ^= 1u << (a - 32);
-                    if (b < 32) lo ^= 1u << b; else hi ^= 1u << (b - 32);
-                }
-            }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                lo ^= __shfl_xor_sync(FULL, lo, o);
-                hi ^= __shfl_xor_sync(FULL, hi, o);
-            }
-            unsigned long long xm = (unsigned long long)lo | ((unsigned long long)hi << 32);
-            if (__popcll(xm) < 2) {
-                bad = true;
-            } else {
-                int b0 = __ffsll((long long)xm) - 1;
-                unsigned long long x2 = xm & (xm - 1);
-                int b1 = __ffsll((long long)x2) - 1;
-                n_new = 2;
-                if (lane < 2) {
-                    int j = lane == 0 ? b0 : b1;
-                    const double4 hi_ = W.hp[cur], hj = W.hp[j];
-                    double rw = det2(hi_.x, hi_.y, hj.x, hj.y);  // new_vertex orientation (cell.cpp:351-359)
-                    my_new[0] = rw > 0 ? pack3(j, cur, 0) : pack3(cur, j, 0);
-                    my_new_pos[0] = lane;
-                    my_new_cnt = 1;
-                }
-            }
-        } else {
-            unsigned long long* em = W.u.b.emask;
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                int i = lane + 32 * j;
-                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
-                    uint32_t tv = W.tri[i];
-                    uint32_t a = tri_a(tv), b = tri_b(tv), c = tri_c(tv);
-                    atomicOr(&em[a], 1ull << b);
-                    atomicOr(&em[b], 1ull << c);
-                    atomicOr(&em[c], 1ull << a);
-                }
-            }
-            __syncwarp();
-            unsigned long long src = 0ull;
-            int base = 0;
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                int i = lane + 32 * j;
-                bool rem = i < nb_t && ((cm[j] >> lane) & 1u);
-                uint32_t tv = rem ? W.tri[i] : 0u;
-                uint32_t v3[3] = {tri_a(tv), tri_b(tv), tri_c(tv)};
-#pragma unroll
-                for (int ed = 0; ed < 3; ed++) {
-                    uint32_t x = v3[ed], y = v3[(ed + 1) % 3];
-                    bool isb = rem && !((em[y] >> x) & 1ull);
-                    unsigned bal = __ballot_sync(FULL, isb);
-                    if (isb) {
-                        my_new[my_new_cnt] = pack3(cur, x, y);
-                        my_new_pos[my_new_cnt] = base + __popc(bal & ((1u << lane) - 1u));
-                        my_new_cnt++;
-                        src |= 1ull << x;
-                        W.u.b.nxt[x] = (unsigned char)y;
-                    }
-                    base += __popc(bal);
-                }
-            }
-            n_new = base;
-            // OR-reduce the source planes; a simple cycle visits each source once
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) src |= __shfl_xor_sync(FULL, src, o);
-            __syncwarp();
-            bool ok = __popcll(src) == n_new && n_new >= 3;
-            if (ok && lane == 0) {
-                int x0 = __ffsll((long long)src) - 1, x = x0;
-                for (int st = 1; st <= n_new; st++) {
-                    x = W.u.b.nxt[x];
-                    if (!((src >> x) & 1ull) || (x == x0 && st < n_new)) {
-                        ok = false;
-                        break;
-                    }
-                }
-                if (x != x0) ok = false;
-            }
-            ok = __shfl_sync(FULL, ok ? 1 : 0, 0) != 0;
-            bad = !ok;
-            // clear the edge rows of removed vertices
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                int i = lane + 32 * j;
-                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
-                    uint32_t tv = W.tri[i];
-                    em[tri_a(tv)] = 0ull;
-                    em[tri_b(tv)] = 0ull;
-                    em[tri_c(tv)] = 0ull;
-                }
-            }
-            __syncwarp();
-        }
-        if (bad) {
-            status = ST_INCONSISTENT_BOUNDARY;
-            fail_vdist = max_vd2(W, nb_t, lane, km);
-            break;
-        }
-        // 3. new vertices and their certificate distances
-        double nd2[9];
-        double newmax = 0.0;
-        for (int q = 0; q < my_new_cnt; q++) {
-            double x, y, zz;
-            vertex_pos<D>(W.hp, my_new[q], x, y, zz);
-            nd2[q] = seed_d2(x, y, zz, sx, sy, sz);
-            newmax = nan_max(newmax, nd2[q]);
-        }
-        if (kept + n_new >= MAX_T) {  // new_vertex overflow (cell.cpp:347-350)
-            status = ST_TRIANGLE_OVERFLOW;
-            fail_vdist = nan_max(max_vd2(W, nb_t, lane, km), warp_max(newmax));
-            break;
-        }
-        // compaction: kept vertices in order, then the new ones
-        uint32_t kt[3];
-        double kd[3];
-        int kp[3];
-        int before = 0;
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            const int i = lane + 32 * j;
-            const int nvalid = nb_t - 32 * j;
-            const uint32_t vm = nvalid >= 32 ? FULL : (nvalid > 0 ? ((1u << nvalid) - 1u) : 0u);
-            const uint32_t kmj = km[j] & vm;
-            const bool keep = (kmj >> lane) & 1u;
-            kt[j] = keep ? W.tri[i] : 0u;
-            kd[j] = keep ? W.vd2[i] : 0.0;
-            kp[j] = keep ? before + __popc(kmj & ((1u << lane) - 1u)) : -1;
-            before += __popc(kmj);
-        }
-        __syncwarp();
-#pragma unroll
-        for (int j = 0; j < 3; j++)
-            if (kp[j] >= 0) {
-                W.tri[kp[j]] = kt[j];
-                W.vd2[kp[j]] = kd[j];
-            }
-        for (int q = 0; q < my_new_cnt; q++) {
-            W.tri[kept + my_new_pos[q]] = my_new[q];
-            W.vd2[kept + my_new_pos[q]] = nd2[q];
-        }
-        if (lane == 0) W.vid[cur] = (int)z;
-        nb_v++;
-        nb_t = kept + n_new;
-        __syncwarp();
-        v_dist = max_vd2(W, nb_t, lane, nullptr);
         if (d2B > 4 * v_dist) {  // security radius reached (voronoi.cpp:224)
             certk = k + 1;
             break;
@@ -721,6 +752,243 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
     extract_and_store<D>(W, P, w, lane, nb_v, nb_t, e, certk, sx, sy, sz);
 }
 
+
+// ============================================================================
+// Security-radius clipping without a neighbour budget (extension).  Cells whose
+// certificate does not close within the K nearest neighbours -- large cells
+// beside dense clumps, whose security sphere holds thousands of clump points --
+// are clipped by walking the grid instead of a list: coarse bins in order of
+// their distance lower bound, dense bins descended sub-bin by sub-bin.  A box
+// is skipped when it lies beyond the security radius (2 sqrt(v_dist)) or when
+// no point in it can cut the cell: a point q cuts the convex cell iff some
+// vertex v is nearer to q than to the seed, so a box whose distance to every
+// vertex exceeds that vertex's distance to the seed holds no cutting point.
+// When the walk ends every point within the security radius has been clipped
+// or excluded, which is the certificate.  Points of a sub-bin are clipped in
+// their sorted order (by extended id within the sub-bin), so the result is
+// deterministic.
+constexpr int PRUNE_STACK = 64;
+
+// squared distance from (x, y, z) to the box [lo, lo + side)^D
+template <int D>
+__device__ __forceinline__ double pt_box_d2(double x, double y, double z, const double (&lo)[3], double side) {
+    const double c[3] = {x, y, z};
+    double d2 = 0.0;
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        const double hi = lo[a] + side;
+        const double dd = c[a] < lo[a] ? lo[a] - c[a] : (c[a] > hi ? c[a] - hi : 0.0);
+        d2 += dd * dd;
+    }
+    return d2;
+}
+
+template <int D>
+__global__ void __launch_bounds__(CLIP_WARPS * 32)
+    k_clip_pruned(ClipParams P, SubGrid g, const int2* __restrict__ table, int table_n, int table_r,
+                  const uint32_t* __restrict__ cells, int64_t ncells) {
+    using PT = typename PointOf<D>::type;
+    __shared__ WarpCell cells_sm[CLIP_WARPS];
+    __shared__ int4 stack_sm[CLIP_WARPS][PRUNE_STACK];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t t = (int64_t)blockIdx.x * CLIP_WARPS + w;
+    if (t >= ncells) return;  // warp-uniform
+    WarpCell& W = cells_sm[w];
+    int4* stk = stack_sm[w];
+    const PT* spts = (const PT*)P.spts;
+    const uint32_t s = cells[t];
+    const uint32_t e = P.perm[s];
+    const PT sp = spts[s];
+    const double sx = sp.x, sy = sp.y, sz = pz(sp);
+
+    // ---- the bounding box cell, as in k_clip (cell.cpp:42-104)
+    const double beps = 1e-14;
+    const double xmin = -beps, xmax = 1.0 + beps;
+    if (lane < 2 * D) {
+        double4 pl;
+        switch (lane) {
+            case 0: pl = make_double4(1.0, 0.0, 0.0, -xmin); break;
+            case 1: pl = make_double4(-1.0, 0.0, 0.0, xmax); break;
+            case 2: pl = make_double4(0.0, 1.0, 0.0, -xmin); break;
+            case 3: pl = make_double4(0.0, -1.0, 0.0, xmax); break;
+            case 4: pl = make_double4(0.0, 0.0, 1.0, -xmin); break;
+            default: pl = make_double4(0.0, 0.0, -1.0, xmax); break;
+        }
+        W.hp[lane] = pl;
+        W.vid[lane] = -1;
+    }
+    if (D == 3) {
+        W.u.b.emask[lane] = 0ull;
+        W.u.b.emask[lane + 32] = 0ull;
+    }
+    const int ntri0 = D == 2 ? 4 : 8;
+    if (lane < ntri0) {
+        uint32_t tv;
+        if (D == 2) {
+            const uint32_t t2[4] = {pack3(2, 0, 0), pack3(1, 2, 0), pack3(3, 1, 0), pack3(0, 3, 0)};
+            tv = t2[lane & 3];
+        } else {
+            const uint32_t t3[8] = {pack3(2, 5, 0), pack3(5, 3, 0), pack3(1, 5, 2), pack3(5, 1, 3),
+                                    pack3(4, 2, 0), pack3(4, 0, 3), pack3(2, 4, 1), pack3(4, 3, 1)};
+            tv = t3[lane & 7];
+        }
+        W.tri[lane] = tv;
+    }
+    __syncwarp();
+    if (lane < ntri0) {
+        double x, y, z;
+        vertex_pos<D>(W.hp, W.tri[lane], x, y, z);
+        W.vd2[lane] = seed_d2(x, y, z, sx, sy, sz);
+    }
+    __syncwarp();
+    int nb_v = 2 * D, nb_t = ntri0;
+    int status = ST_SUCCESS;
+    double v_dist = max_vd2(W, nb_t, lane, nullptr);
+    double fail_vdist = 0.0;
+
+    // vertex positions of this lane's vertices (lane, lane + 32, lane + 64)
+    double vx[3], vy[3], vz[3];
+    auto refresh = [&]() {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int i = lane + 32 * j;
+            if (i < nb_t) vertex_pos<D>(W.hp, W.tri[i], vx[j], vy[j], vz[j]);
+        }
+    };
+    refresh();
+    // true when no point of the box can cut the cell (with a relative margin for rounding)
+    auto prunable = [&](const double (&lo)[3], double side) -> bool {
+        bool ok = true;
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int i = lane + 32 * j;
+            if (i < nb_t) ok = ok && pt_box_d2<D>(vx[j], vy[j], vz[j], lo, side) > W.vd2[i] * (1.0 + 1e-9);
+        }
+        return __all_sync(FULL, ok);
+    };
+    const int G = g.G;
+    const double h0 = 1.0 / (double)G;
+    // clips by the points of level-L box (x, y, z), descending refined bins depth first
+    auto visit = [&](int x0, int y0, int z0) -> bool {
+        int sp_ = 0;
+        if (lane == 0) stk[0] = make_int4(x0, y0, z0, 0);
+        sp_ = 1;
+        __syncwarp();
+        while (sp_ > 0) {
+            const int4 b = stk[--sp_];
+            __syncwarp();
+            const int L = b.w;
+            const int cx = b.x >> L, cy = b.y >> L, cz = b.z >> L;
+            const uint32_t m = morton<D>(cx, cy, cz);
+            const int Lb = g.lvl[m];
+            if (L < Lb) {
+                // children nearest first: pushed farthest first
+                const double side = 1.0 / (double)(G << (L + 1));
+                double cd[1 << D];
+                int order[1 << D];
+#pragma unroll
+                for (int ch = 0; ch < (1 << D); ch++) {
+                    const double lo[3] = {(2 * b.x + (ch & 1)) * side, (2 * b.y + ((ch >> 1) & 1)) * side,
+                                          D == 3 ? (2 * b.z + ((ch >> 2) & 1)) * side : 0.0};
+                    cd[ch] = pt_box_d2<D>(sx, sy, sz, lo, side);
+                    order[ch] = ch;
+                }
+                for (int a = 1; a < (1 << D); a++)  // insertion sort, descending distance
+                    for (int q = a; q > 0 && cd[order[q]] > cd[order[q - 1]]; q--) {
+                        const int tmp = order[q];
+                        order[q] = order[q - 1];
+                        order[q - 1] = tmp;
+                    }
+                for (int a = 0; a < (1 << D); a++) {
+                    const int ch = order[a];
+                    if (cd[ch] * (1.0 - 1e-12) > 4 * v_dist) continue;
+                    const int nx = 2 * b.x + (ch & 1), ny = 2 * b.y + ((ch >> 1) & 1),
+                              nz = D == 3 ? 2 * b.z + ((ch >> 2) & 1) : 0;
+                    const double lo[3] = {nx * side, ny * side, nz * side};
+                    if (prunable(lo, side)) continue;
+                    if (sp_ >= PRUNE_STACK) return false;
+                    if (lane == 0) stk[sp_] = make_int4(nx, ny, nz, L + 1);
+                    sp_++;
+                }
+                __syncwarp();
+                continue;
+            }
+            // a leaf: one sub-bin of the bin's own level
+            const uint32_t slot = g.sub_off[m] + (L > 0 ? morton<D>(b.x - (cx << L), b.y - (cy << L), b.z - (cz << L)) : 0u);
+            const uint32_t a0 = g.sub_start[slot], a1 = g.sub_start[slot + 1];
+            for (uint32_t q = a0; q < a1; q++) {
+                if (q == s) continue;
+                const PT B = spts[q];
+                const double bx = B.x, by = B.y, bz = pz(B);
+                if (seed_d2(bx, by, bz, sx, sy, sz) > 4 * v_dist) continue;
+                const int r = clip_by<D, true>(W, lane, P.perm[q], bx, by, bz, sx, sy, sz, P.robust, nb_v, nb_t,
+                                               status, v_dist, fail_vdist);
+                if (r == CLIP_FAIL) return false;
+                if (r == CLIP_CUT) refresh();
+            }
+        }
+        return true;
+    };
+    // coarse bins around the seed's: the offset table (ascending lower bound), then rings
+    const int bc[3] = {bin_coord(sx, G), bin_coord(sy, G), D == 3 ? bin_coord(sz, G) : 0};
+    const double pc[3] = {sx, sy, sz};
+    bool alive = true;
+    for (int ci = 0; ci < table_n && alive; ci++) {
+        const int2 ent = table[ci];
+        if ((double)ent.y * h0 * h0 * (1.0 - 1e-12) > 4 * v_dist) break;
+        const int x = bc[0] + (int)(signed char)(ent.x & 255), y = bc[1] + (int)(signed char)((ent.x >> 8) & 255),
+                  z = D == 3 ? bc[2] + (int)(signed char)((ent.x >> 16) & 255) : 0;
+        if (x < 0 || x >= G || y < 0 || y >= G || (D == 3 && (z < 0 || z >= G))) continue;
+        const double lo[3] = {x * h0, y * h0, z * h0};
+        if (pt_box_d2<D>(sx, sy, sz, lo, h0) * (1.0 - 1e-12) > 4 * v_dist) continue;
+        if (prunable(lo, h0)) continue;
+        alive = visit(x, y, z);
+    }
+    // a vertex without a position (three planes through one line, w = 0) makes v_dist
+    // NaN and no radius bounds the walk: such a cell stays uncertified, as in k_clip
+    if (v_dist != v_dist) alive = false;
+    for (int r = table_r + 1; alive; r++) {
+        double lb = CUDART_INF;
+        bool all = true;
+#pragma unroll
+        for (int a = 0; a < D; a++) {
+            const int lo = bc[a] - (r - 1), hi = bc[a] + (r - 1);
+            if (lo > 0) {
+                all = false;
+                lb = fmin(lb, pc[a] - (double)lo * h0);
+            }
+            if (hi < G - 1) {
+                all = false;
+                lb = fmin(lb, (double)(hi + 1) * h0 - pc[a]);
+            }
+        }
+        if (all || r > G + 1) break;
+        if (lb > 0.0 && 4 * v_dist < lb * lb * (1.0 - 1e-12)) break;
+        if (v_dist != v_dist) {
+            alive = false;
+            break;
+        }
+        const int w1 = 2 * r + 1;
+        const int ncube = D == 2 ? w1 * w1 : w1 * w1 * w1;
+        for (int ci = 0; ci < ncube && alive; ci++) {
+            const int dx = ci % w1 - r, rest = ci / w1;
+            const int dy = rest % w1 - r, dz = D == 3 ? rest / w1 - r : 0;
+            if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
+            const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
+            if (x < 0 || x >= G || y < 0 || y >= G || (D == 3 && (z < 0 || z >= G))) continue;
+            const double lo[3] = {x * h0, y * h0, z * h0};
+            if (pt_box_d2<D>(sx, sy, sz, lo, h0) * (1.0 - 1e-12) > 4 * v_dist) continue;
+            if (prunable(lo, h0)) continue;
+            alive = visit(x, y, z);
+        }
+    }
+    if (!alive || v_dist != v_dist) {
+        store_failed(P, lane, e, status == ST_SUCCESS ? ST_SECURITY_RADIUS_NOT_REACHED : status);
+        return;
+    }
+    // every point within the security radius was clipped or excluded: certified
+    extract_and_store<D>(W, P, w, lane, nb_v, nb_t, e, P.K + 1, sx, sy, sz);
+}
 
 // ============================================================================
 // FP32 local-frame clipping (BASELINE's precision form).  The cell is clipped
@@ -1273,7 +1541,8 @@ cudaError_t select_cells(pgpu_ctx* c, int code, bool hydro_only, bool as_slots, 
 // reset: start a fresh face array (else faces are appended to the current one).
 cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const uint32_t* knn, bool reset,
                       unsigned long long* fc, unsigned* overflow, unsigned* uncert, bool fp32 = false,
-                      unsigned* reclip = nullptr, const uint32_t* slots = nullptr, const uint16_t* kq = nullptr) {
+                      unsigned* reclip = nullptr, const uint32_t* slots = nullptr, const uint16_t* kq = nullptr,
+                      bool pruned = false) {
     const int D = c->prm.dim;
     cudaError_t e = cudaSuccess;
     DevScalars* sc = (DevScalars*)c->scalars.p;
@@ -1314,7 +1583,17 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     P.face_cap = c->face_cap;
     if (nq > 0) {
         const unsigned blocks = (unsigned)((nq + CLIP_WARPS - 1) / CLIP_WARPS);
-        if (fp32) {
+        if (pruned) {
+            const SubGrid g = {c->grid_G, (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
+                               (const uint32_t*)c->sub_start.p};
+            const int2* tab = (const int2*)c->knn_table.p;
+            if (D == 2)
+                k_clip_pruned<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P, g, tab, c->knn_table_n,
+                                                                            c->knn_table_r, qs, nq);
+            else
+                k_clip_pruned<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P, g, tab, c->knn_table_n,
+                                                                            c->knn_table_r, qs, nq);
+        } else if (fp32) {
             if (D == 2)
                 k_clip32<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
             else
@@ -1414,6 +1693,28 @@ cudaError_t launch_fallback(pgpu_ctx* c, int K2) {
     c->num_faces = (int64_t)fc;
     c->n_uncertified = unc;
     c->n_refit = nf;
+    return cudaSuccess;
+}
+
+// Hydro cells still uncertified after the neighbour lists: clipped again by the
+// grid walk of k_clip_pruned, faces appended.
+cudaError_t launch_pruned(pgpu_ctx* c) {
+    cudaError_t e = cudaSuccess;
+    const int64_t nq = c->n_query;
+    uint32_t* fq = ensure<uint32_t>(c->fb_qs, nq + 1, &e);
+    if (e) return e;
+    uint32_t nf = 0;
+    c->n_pruned = 0;
+    if ((e = select_cells(c, ST_SECURITY_RADIUS_NOT_REACHED, true, false, fq, &nf))) return e;
+    if (nf == 0) return cudaSuccess;
+    unsigned long long fc = 0;
+    unsigned of = 0, unc = 0;
+    if ((e = clip_pass(c, fq, nf, c->prm.k, nullptr, false, &fc, &of, &unc, false, nullptr, nullptr, nullptr, true)))
+        return e;
+    if (of) return cudaErrorMemoryAllocation;
+    c->num_faces = (int64_t)fc;
+    c->n_uncertified = unc;
+    c->n_pruned = nf;
     return cudaSuccess;
 }
 

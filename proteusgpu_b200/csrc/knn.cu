@@ -218,12 +218,48 @@ __device__ __forceinline__ double box_d2(const double* pc, int x, int y, int z, 
     return bd2;
 }
 
+// Sorted-point range of the level-Lq box (x, y, z) for a query whose own box is
+// qb.  In a bin refined at least as finely the box is an aligned block of
+// Morton-consecutive sub-bins.  In a coarser bin the box lies inside one larger
+// sub-bin S, which is scanned whole, once: from the box of S nearest the query
+// (the query's box clamped into S), whose box distance is S's own.
+template <int D>
+__device__ __forceinline__ bool box_range(const SubGrid& g, int Lq, int x, int y, int z, const int (&qb)[3],
+                                          uint32_t& start, uint32_t& cnt) {
+    const int cx = x >> Lq, cy = y >> Lq, cz = z >> Lq;
+    const uint32_t m = morton<D>(cx, cy, cz);
+    const int Lb = g.lvl[m];
+    const uint32_t base = g.sub_off[m];
+    uint32_t a, b;
+    if (Lb >= Lq) {
+        const int sh = Lb - Lq;
+        const uint32_t first = morton<D>(x - (cx << Lq), y - (cy << Lq), z - (cz << Lq)) << (D * sh);
+        a = base + first;
+        b = a + (1u << (D * sh));
+    } else {
+        const int sh = Lq - Lb;
+        const int sx = x >> sh, sy = y >> sh, sz = z >> sh;
+        const int bxs[3] = {x, y, z}, sxs[3] = {sx, sy, sz};
+#pragma unroll
+        for (int k = 0; k < D; k++) {
+            const int lo = sxs[k] << sh, hi = lo + (1 << sh) - 1;
+            const int nearest = qb[k] < lo ? lo : (qb[k] > hi ? hi : qb[k]);
+            if (bxs[k] != nearest) return false;
+        }
+        a = base + morton<D>(sx - (cx << Lb), sy - (cy << Lb), sz - (cz << Lb));
+        b = a + 1;
+    }
+    start = g.sub_start[a];
+    cnt = g.sub_start[b] - start;
+    return true;
+}
+
 template <int D>
 __global__ void __launch_bounds__(KNN_WARPS * 32)
-    k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm,
-          const uint32_t* __restrict__ bin_start, int G, const int2* __restrict__ table, int table_n, int table_r,
-          const uint32_t* __restrict__ qs, int64_t nq, int K, const uint16_t* __restrict__ kq, int stride,
-          uint32_t* __restrict__ out, unsigned long long* __restrict__ cand_counter) {
+    k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
+          const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
+          int K, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
+          unsigned long long* __restrict__ cand_counter) {
     __shared__ KnnSmem S;
     using PT = typename PointOf<D>::type;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -240,7 +276,11 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
     const PT p = spts[s];
     const uint32_t qid = perm[s];
     const double pc[3] = {p.x, p.y, pz(p)};
-    const int bc[3] = {bin_coord(p.x, G), bin_coord(p.y, G), D == 3 ? bin_coord(pz(p), G) : 0};
+    // the query searches at its own bin's level: boxes of side 1 / (G << Lq)
+    const int G0 = grid.G;
+    const int Lq = grid.lvl[morton<D>(bin_coord(p.x, G0), bin_coord(p.y, G0), D == 3 ? bin_coord(pz(p), G0) : 0)];
+    const int G = G0 << Lq;
+    const int bc[3] = {sub_coord(p.x, G0, Lq), sub_coord(p.y, G0, Lq), D == 3 ? sub_coord(pz(p), G0, Lq) : 0};
     const double h = 1.0 / (double)G;
     double thr_d = CUDART_INF;
     uint32_t thr_i = NO_NEIGHBOR;
@@ -251,10 +291,10 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
     // 1. offsets in order of their lower bound
     for (int c0 = 0; c0 < table_n; c0 += 32) {
         const int2 first = table[c0];
-        if (thr_i != NO_NEIGHBOR && (double)first.y * h * h * (1.0 - 1e-12) > thr_d) {
-            done = true;  // every remaining bin is farther than the K-th neighbour
-            break;
-        }
+        // every remaining table bin is farther than the K-th neighbour; bins beyond the
+        // table (which may be nearer than the table's last entries) are left to the
+        // ring search, whose first test ends it at once when they are all too far
+        if (thr_i != NO_NEIGHBOR && (double)first.y * h * h * (1.0 - 1e-12) > thr_d) break;
         const int ci = c0 + lane;
         uint32_t bstart = 0, bcnt = 0;
         if (ci < table_n) {
@@ -264,11 +304,7 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
             const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
             bool ok = x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G));
             if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
-            if (ok) {
-                const uint32_t key = morton<D>(x, y, z);
-                bstart = bin_start[key];
-                bcnt = bin_start[key + 1] - bstart;
-            }
+            if (ok && !box_range<D>(grid, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
         }
         scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, w, lane, nrows, K, qn, thr_d, thr_i, ncand);
         // the bound is tested at chunk boundaries: merge what is queued
@@ -307,11 +343,7 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
                 const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
                 bool ok = cheb == r && x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G));
                 if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
-                if (ok) {
-                    const uint32_t key = morton<D>(x, y, z);
-                    bstart = bin_start[key];
-                    bcnt = bin_start[key + 1] - bstart;
-                }
+                if (ok && !box_range<D>(grid, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
             }
             scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, w, lane, nrows, K, qn, thr_d, thr_i, ncand);
         }
@@ -369,14 +401,15 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
     DevScalars* sc = (DevScalars*)c->scalars.p;
     const unsigned blocks = (unsigned)((nq + KNN_WARPS - 1) / KNN_WARPS);
     const uint32_t* perm = (const uint32_t*)c->perm.p;
-    const uint32_t* bs = (const uint32_t*)c->bin_start.p;
+    const SubGrid grid = {c->grid_G, (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
+                       (const uint32_t*)c->sub_start.p};
     const int2* tab = (const int2*)c->knn_table.p;
     if (c->prm.dim == 2)
-        k_knn<2><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double2*)c->spts.p, perm, bs, c->grid_G, tab,
+        k_knn<2><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double2*)c->spts.p, perm, grid, tab,
                                                            c->knn_table_n, c->knn_table_r, qs, nq, K, kq, stride,
                                                            out, &sc->knn_cand);
     else
-        k_knn<3><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double4*)c->spts.p, perm, bs, c->grid_G, tab,
+        k_knn<3><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double4*)c->spts.p, perm, grid, tab,
                                                            c->knn_table_n, c->knn_table_r, qs, nq, K, kq, stride,
                                                            out, &sc->knn_cand);
     count_launches(1);

@@ -111,6 +111,74 @@ __global__ void k_bin_count(const typename PointOf<D>::type* __restrict__ ext, i
     atomicAdd(&cnt[k], 1u);
 }
 
+// Refinement level of each coarse bin: dense bins (clustered inputs) are split
+// into (2^L)^D sub-bins so that the search works at the local point spacing.
+template <int D>
+__global__ void k_bin_levels(const uint32_t* __restrict__ cnt, int64_t M, uint8_t* __restrict__ lvl,
+                             uint32_t* __restrict__ size) {
+    const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const uint32_t c = cnt[m];
+    int L = 0;
+    if (c > SUB_SPLIT)
+        while (L < SUB_LMAX && (uint64_t)c > (uint64_t)SUB_FILL << (D * L)) L++;
+    lvl[m] = (uint8_t)L;
+    size[m] = 1u << (D * L);
+}
+
+// Sub-bin slot of every point (overwrites its coarse key) and the slot counts.
+template <int D>
+__global__ void k_sub_count(const typename PointOf<D>::type* __restrict__ ext, int64_t n, int G,
+                            const uint8_t* __restrict__ lvl, const uint32_t* __restrict__ sub_off,
+                            uint32_t* __restrict__ key, uint32_t* __restrict__ sub_cnt) {
+    const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= n) return;
+    const typename PointOf<D>::type p = ext[e];
+    const uint32_t b = key[e];
+    const int L = lvl[b];
+    uint32_t slot = sub_off[b];
+    if (L > 0) {
+        const int lx = sub_coord(p.x, G, L) - (bin_coord(p.x, G) << L);
+        const int ly = sub_coord(p.y, G, L) - (bin_coord(p.y, G) << L);
+        const int lz = D == 3 ? sub_coord(pz(p), G, L) - (bin_coord(pz(p), G) << L) : 0;
+        slot += morton<D>(lx, ly, lz);
+    }
+    key[e] = slot;
+    atomicAdd(&sub_cnt[slot], 1u);
+}
+
+// Points of each sub-bin in ascending extended id (the scatter's atomics leave
+// them in arbitrary order), so that every walk over a sub-bin is deterministic.
+template <int D>
+__global__ void k_sub_sort(const uint32_t* __restrict__ sub_start, int64_t T,
+                           typename PointOf<D>::type* __restrict__ spts, uint32_t* __restrict__ perm,
+                           uint32_t* __restrict__ inv) {
+    const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (slot >= T) return;
+    const uint32_t a = sub_start[slot], b = sub_start[slot + 1];
+    if (b - a < 2) return;
+    for (uint32_t i = a + 1; i < b; i++) {
+        const uint32_t id = perm[i];
+        const typename PointOf<D>::type pt = spts[i];
+        uint32_t j = i;
+        while (j > a && perm[j - 1] > id) {
+            perm[j] = perm[j - 1];
+            spts[j] = spts[j - 1];
+            j--;
+        }
+        perm[j] = id;
+        spts[j] = pt;
+    }
+    for (uint32_t i = a; i < b; i++) inv[perm[i]] = i;
+}
+
+// Point range of each coarse bin from the sub-bin starts.
+__global__ void k_bin_from_sub(const uint32_t* __restrict__ sub_off, const uint32_t* __restrict__ sub_start,
+                               int64_t M, uint32_t* __restrict__ bin_start) {
+    const int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (m <= M) bin_start[m] = sub_start[sub_off[m]];
+}
+
 template <int D>
 __global__ void k_bin_scatter(const typename PointOf<D>::type* __restrict__ ext, int64_t n,
                               const uint32_t* __restrict__ key, const uint32_t* __restrict__ start,
@@ -204,6 +272,9 @@ static int grid_resolution(int64_t n, int D) {
     return G > gmax ? gmax : G;
 }
 
+// Two-level counting sort: coarse Morton bins, each split into Morton-ordered
+// sub-bins when dense, so that every coarse bin and every aligned block of its
+// sub-bins is one contiguous range of the sorted points.
 cudaError_t launch_grid_sort(pgpu_ctx* c) {
     const int D = c->prm.dim;
     const int64_t n = c->n_ext;
@@ -217,6 +288,8 @@ cudaError_t launch_grid_sort(pgpu_ctx* c) {
     uint32_t* cnt = ensure<uint32_t>(c->bin_cnt, M + 1, &e);
     uint32_t* start = ensure<uint32_t>(c->bin_start, M + 1, &e);
     uint32_t* key = ensure<uint32_t>(c->bin_key, n + 1, &e);
+    uint8_t* lvl = ensure<uint8_t>(c->bin_lvl, M + 1, &e);
+    uint32_t* soff = ensure<uint32_t>(c->sub_off, M + 1, &e);
     const size_t pt_bytes = D == 2 ? 16 : 32;
     if (e || (e = ensure_bytes(c->spts, (size_t)(n + 1) * pt_bytes))) return e;
     uint32_t* perm = ensure<uint32_t>(c->perm, n + 1, &e);
@@ -228,18 +301,46 @@ cudaError_t launch_grid_sort(pgpu_ctx* c) {
             k_bin_count<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, G, key, cnt);
         else
             k_bin_count<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, G, key, cnt);
+        count_launches(1);
     }
-    if (n > 0) count_launches(1);
-    if ((e = exclusive_scan_u32(cnt, start, M, c->scan_tmp, c->stream))) return e;
-    if ((e = cudaMemsetAsync(cnt, 0, (M + 1) * sizeof(uint32_t), c->stream))) return e;
+    // levels, sub-table offsets (one slot per coarse bin at level 0)
+    if (D == 2)
+        k_bin_levels<2><<<nblk(M, 256), 256, 0, c->stream>>>(cnt, M, lvl, start);
+    else
+        k_bin_levels<3><<<nblk(M, 256), 256, 0, c->stream>>>(cnt, M, lvl, start);
+    count_launches(1);
+    if ((e = exclusive_scan_u32(start, soff, M, c->scan_tmp, c->stream))) return e;
+    uint32_t T = 0;
+    if ((e = cudaMemcpyAsync(&T, soff + M, sizeof(T), cudaMemcpyDeviceToHost, c->stream))) return e;
+    if ((e = cudaStreamSynchronize(c->stream))) return e;
+    c->sub_slots = T;
+    uint32_t* scnt = ensure<uint32_t>(c->sub_cnt, (size_t)T + 1, &e);
+    uint32_t* sstart = ensure<uint32_t>(c->sub_start, (size_t)T + 1, &e);
+    if (e) return e;
+    if ((e = cudaMemsetAsync(scnt, 0, ((size_t)T + 1) * sizeof(uint32_t), c->stream))) return e;
     if (n > 0) {
         if (D == 2)
-            k_bin_scatter<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, key, start, cnt,
+            k_sub_count<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, G, lvl, soff, key, scnt);
+        else
+            k_sub_count<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, G, lvl, soff, key, scnt);
+        count_launches(1);
+    }
+    if ((e = exclusive_scan_u32(scnt, sstart, T, c->scan_tmp, c->stream))) return e;
+    k_bin_from_sub<<<nblk(M + 1, 256), 256, 0, c->stream>>>(soff, sstart, M, start);
+    count_launches(1);
+    if ((e = cudaMemsetAsync(scnt, 0, ((size_t)T + 1) * sizeof(uint32_t), c->stream))) return e;
+    if (n > 0) {
+        if (D == 2)
+            k_bin_scatter<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, key, sstart, scnt,
                                                                   (double2*)c->spts.p, perm, inv);
         else
-            k_bin_scatter<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, key, start, cnt,
+            k_bin_scatter<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, key, sstart, scnt,
                                                                   (double4*)c->spts.p, perm, inv);
-        count_launches(1);
+        if (D == 2)
+            k_sub_sort<2><<<nblk(T, 256), 256, 0, c->stream>>>(sstart, T, (double2*)c->spts.p, perm, inv);
+        else
+            k_sub_sort<3><<<nblk(T, 256), 256, 0, c->stream>>>(sstart, T, (double4*)c->spts.p, perm, inv);
+        count_launches(2);
     }
     return cudaGetLastError();
 }

@@ -97,6 +97,29 @@ __device__ __forceinline__ int bin_coord(double x, int G) {
     return i < 0 ? 0 : (i > G - 1 ? G - 1 : i);
 }
 
+// Sub-bins of dense coarse bins: a bin with more than SUB_SPLIT points gets the
+// smallest level L (<= SUB_LMAX) with at most SUB_FILL points per sub-bin on
+// average.  Coordinates at level L run over [0, G << L); a point's level-L
+// coordinate is clamped into its own coarse bin so both levels agree.
+constexpr int SUB_SPLIT = 16;
+constexpr int SUB_FILL = 4;
+constexpr int SUB_LMAX = 5;
+// The grid as the search kernels see it: coarse Morton bins, dense ones split
+// into Morton-ordered sub-bins.
+struct SubGrid {
+    int G;                      // coarse bins per axis
+    const uint8_t* lvl;         // refinement level per coarse bin
+    const uint32_t* sub_off;    // first sub-bin slot per coarse bin
+    const uint32_t* sub_start;  // first sorted point per sub-bin slot (one past the last: n)
+};
+
+__device__ __forceinline__ int sub_coord(double x, int G, int L) {
+    const int b = bin_coord(x, G);
+    const int i = (int)floor(x * (double)(G << L));
+    const int lo = b << L, hi = lo + (1 << L) - 1;
+    return i < lo ? lo : (i > hi ? hi : i);
+}
+
 // ---- hydro: the reference's HLL solver (src/hydro/riemann.cpp:7-124) ----
 struct Prim {
     double rho, vx, vy, vz, E;

@@ -78,6 +78,7 @@ struct pgpu_ctx {
     std::string err;
     bool timing = false;
     cudaEvent_t ev[6] = {};
+    unsigned ev_mask = 0;      // events recorded since the last build began
     float stage_ms[5] = {};
 
     // sizes of the current mesh
@@ -95,6 +96,10 @@ struct pgpu_ctx {
     pgpu::DevBuf ghost_src;    // u32: hydro id copied by each ghost
     pgpu::DevBuf ghost_code;   // u32: image code of each ghost
     pgpu::DevBuf bin_cnt, bin_start, bin_key;  // grid bins (Morton slots) and per-point key
+    pgpu::DevBuf bin_lvl;      // u8 per coarse bin: refinement level L ((2^L)^D sub-bins)
+    pgpu::DevBuf sub_off;      // u32 per coarse bin: first sub-bin slot (M + 1 entries)
+    pgpu::DevBuf sub_cnt, sub_start;  // per sub-bin slot: counts, first sorted point (T + 1)
+    int64_t sub_slots = 0;     // T
     pgpu::DevBuf spts, perm, inv;  // sorted points, sorted->ext id, ext id->sorted
     pgpu::DevBuf qflag, qoff, qs;  // query list (sorted positions of the cells to compute)
     pgpu::DevBuf knn;          // n_query rows of knn_stride ext ids
@@ -118,6 +123,7 @@ struct pgpu_ctx {
     int64_t n_uncertified = 0;  // hydro cells of the last clip with SECURITY_RADIUS_NOT_REACHED
     int64_t n_refit = 0;        // cells recomputed with the fallback budget in the last step
     int64_t n_reclip = 0;       // cells the FP32 clip handed to the FP64 clip in the last step
+    int64_t n_pruned = 0;       // cells certified by the grid walk in the last step
     pgpu::DevBuf fb_qs, fb_knn; // fallback query list and lists
     pgpu::KBudget kb;           // learned neighbour budget (optional form)
 };
@@ -143,6 +149,8 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
 cudaError_t launch_clip(pgpu_ctx* c);
 // uncertified hydro cells of the last clip: KNN and clipping again with budget K2
 cudaError_t launch_fallback(pgpu_ctx* c, int K2);
+// uncertified hydro cells of the last clip: clipped by walking the grid (no neighbour budget)
+cudaError_t launch_pruned(pgpu_ctx* c);
 // kbudget.cu
 cudaError_t kb_init_weights(pgpu_ctx* c);
 cudaError_t kb_features(pgpu_ctx* c);                 // before the step's clip (reads the previous mesh)

@@ -54,6 +54,16 @@ def assert_same_topology(g, o, failure_codes_may_differ=False):
     assert np.array_equal(np.asarray(g.neighbor), np.asarray(o.neighbor)), "neighbour lists differ"
 
 
+def faces_of(m, cells):
+    """Concatenated face indices of the given cells (each cell's faces in stored order)."""
+    fp = np.asarray(m.face_ptr, np.int64)
+    fc = np.asarray(m.face_counts, np.int64)
+    cells = np.asarray(cells, np.int64)
+    if len(cells) == 0:
+        return np.zeros(0, np.int64)
+    return np.concatenate([np.arange(fp[c], fp[c] + fc[c]) for c in cells])
+
+
 def cell_faces(m, c):
     s = int(m.face_ptr[c])
     return slice(s, s + int(m.face_counts[c]))

@@ -50,3 +50,43 @@ def test_knn_sorted_order_is_a_permutation():
     assert sorted(perm.tolist()) == list(range(5000))
     assert np.array_equal(sp, pts[perm])
     assert ng >= 1
+
+
+def _dense_blob(n_blob, n_bg, dim, sigma, seed):
+    rng = np.random.default_rng(seed)
+    blob = 0.5 + sigma * rng.standard_normal((n_blob, dim))
+    pts = np.concatenate([np.clip(blob, 0.0, 1.0 - 1e-12), rng.random((n_bg, dim))])
+    return np.ascontiguousarray(pts)
+
+
+@pytest.mark.parametrize("dim,k", [(3, 64), (3, 190), (2, 32)])
+def test_knn_refined_bins(dim, k):
+    """A blob thousands of times denser than the background: its coarse bins are
+    split into sub-bins (up to the deepest level) and queries search at the
+    blob's spacing; queries at the blob's edge mix levels."""
+    pts = _dense_blob(30000, 8000, dim, 0.002 if dim == 3 else 0.001, 11 + dim)
+    with Context(dim=dim, k=k) as ctx:
+        g = ctx.knn(pts)
+    assert np.array_equal(g, om.knn(pts, k))
+
+
+def test_knn_refined_lattice_on_box_edges():
+    """Unjittered points on the sub-bin grid lines of a refined region (coordinates
+    that are exact multiples of the sub-bin side) next to a sparse background."""
+    rng = np.random.default_rng(21)
+    side = 1.0 / 2048
+    g1 = (np.arange(40) * side + 0.25)
+    lat = np.stack(np.meshgrid(g1, g1, indexing="ij"), -1).reshape(-1, 2)
+    pts = np.ascontiguousarray(np.concatenate([lat, rng.random((3000, 2))]))
+    with Context(dim=2, k=24) as ctx:
+        g = ctx.knn(pts)
+    assert np.array_equal(g, om.knn(pts, 24))
+
+
+def test_knn_many_duplicates_in_one_bin():
+    rng = np.random.default_rng(22)
+    base = rng.random((2000, 3))
+    pts = np.ascontiguousarray(np.concatenate([base, np.repeat(base[:3], 400, axis=0)]))
+    with Context(dim=3, k=32) as ctx:
+        g = ctx.knn(pts)
+    assert np.array_equal(g, om.knn(pts, 32))
