@@ -37,6 +37,8 @@ UNIT = "cell-updates/s"
 # Workloads.  sedov3d_1m is the configuration the metric is quoted on for one GPU
 # (3D Sedov, plain method); the others are smaller cases (profiling, smoke).
 CONFIGS = {
+    "clustered3d_16m": dict(dim=3, n=16_777_216, seed=4, k=190, buff=0.04, boundary="periodic", cfl=0.3,
+                            ic="clustered"),
     "sedov3d_1m": dict(dim=3, n=1_048_576, seed=2, k=190, buff=0.04, boundary="periodic", cfl=0.3),
     "sedov3d_256k": dict(dim=3, n=262_144, seed=2, k=190, buff=0.04 * 4 ** (1 / 3), boundary="periodic", cfl=0.3),
     "sod2d_10k": dict(dim=2, n=10_000, seed=1, k=16, buff=0.04, boundary="reflective", cfl=0.3),
@@ -72,6 +74,8 @@ def parse():
 
 def make_ic(cfg):
     from proteusgpu_b200 import ics
+    if cfg.get("ic") == "clustered":
+        return ics.clustered_3d(n=cfg["n"], seed=cfg["seed"])
     if cfg["dim"] == 3:
         return ics.sedov_3d(n=cfg["n"], seed=cfg["seed"])
     return ics.sod_2d(n_side=int(round(cfg["n"] ** 0.5)), seed=cfg["seed"])

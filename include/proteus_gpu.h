@@ -213,6 +213,7 @@ typedef struct {
     int64_t reclip_cells;       /* cells the FP32 clip handed to the FP64 clip in the last step */
     int64_t pruned_cells;       /* moving-mesh steps: hydro cells whose certificate needed more than the
                                    neighbour budget(s), clipped by walking the grid instead (extension) */
+    int64_t walk_points, walk_boxes; /* that walk's work: points clipped, grid boxes visited */
 } pgpu_stats;
 
 /* Statistics of the last step (synchronises the stream). */

@@ -42,7 +42,8 @@ class Stats(C.Structure):
                 ("knn_candidates", C.c_int64), ("last_dt", C.c_double), ("total_mass", C.c_double),
                 ("total_energy", C.c_double), ("total_mom", C.c_double * 3), ("cert_k_max", C.c_int32),
                 ("n_grid", C.c_int32), ("refit_cells", C.c_int64), ("uncertified_cells", C.c_int64),
-                ("reclip_cells", C.c_int64), ("pruned_cells", C.c_int64)]
+                ("reclip_cells", C.c_int64), ("pruned_cells", C.c_int64), ("walk_points", C.c_int64),
+                ("walk_boxes", C.c_int64)]
 
 
 class KBudgetInfo(C.Structure):

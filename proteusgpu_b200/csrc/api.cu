@@ -128,8 +128,10 @@ int build_mesh(pgpu_ctx* c, int64_t n, bool no_ghosts, bool all_cells) {
         // cells whose certificate did not close within k: KNN and clipping again with the fallback budget
         CK(pgpu::launch_fallback(c, c->prm.k_fallback));
     }
-    if (!all_cells && c->n_uncertified > 0) {
-        // cells whose security sphere reaches past every budget (beside dense clumps): grid walk
+    c->n_pruned = 0;
+    if (!all_cells) {
+        // cells whose security sphere reaches past every budget (beside dense clumps), or that
+        // failed otherwise: grid walk in the seed's local frame
         CK(pgpu::launch_pruned(c));
     }
     if (kb_on && !kb.trained) {
@@ -634,6 +636,8 @@ int pgpu_sim_stats(pgpu_ctx* c, pgpu_stats* out) {
     out->reclip_cells = c->n_reclip;
     out->uncertified_cells = c->n_uncertified;
     out->pruned_cells = c->n_pruned;
+    out->walk_points = (int64_t)h.walk_points;
+    out->walk_boxes = (int64_t)h.walk_boxes;
     return PGPU_OK;
 }
 

@@ -186,6 +186,7 @@ struct ClipParams {
     uint32_t* f_own;
     double4* f_geo;
     unsigned long long* face_counter;
+    unsigned long long* walk_stats;  // grid walk: points clipped, boxes visited
     unsigned int* overflow;
     unsigned long long face_cap;
 };
@@ -221,7 +222,9 @@ __device__ __forceinline__ void compute_vpos(WarpCell& W, int lane, int nb_t) {
 template <int D>
 __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams& P, int w, int lane, int nb_v, int nb_t,
                                                   uint32_t e, int certk, double sx, double sy, double sz,
-                                                  bool vpos_ready = false) {
+                                                  bool vpos_ready = false, double ox = 0.0, double oy = 0.0,
+                                                  double oz = 0.0) {
+    // (ox, oy, oz): origin of the frame the cell was clipped in, added to the centroid
     if (!vpos_ready) compute_vpos<D>(W, lane, nb_t);
 
     double cell_vol = 0.0, cen[3] = {0.0, 0.0, 0.0};
@@ -422,9 +425,9 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
         P.fcnt[e] = fits ? (uint32_t)nf : 0u;
         P.status[e] = ST_SUCCESS;
         P.certk[e] = certk;
-        P.centroid[3 * (size_t)e] = (cen[0] - 0.5) * P.scale + 0.5;
-        P.centroid[3 * (size_t)e + 1] = (cen[1] - 0.5) * P.scale + 0.5;
-        P.centroid[3 * (size_t)e + 2] = D == 3 ? (cen[2] - 0.5) * P.scale + 0.5 : 0.0;
+        P.centroid[3 * (size_t)e] = (cen[0] + ox - 0.5) * P.scale + 0.5;
+        P.centroid[3 * (size_t)e + 1] = (cen[1] + oy - 0.5) * P.scale + 0.5;
+        P.centroid[3 * (size_t)e + 2] = D == 3 ? (cen[2] + oz - 0.5) * P.scale + 0.5 : 0.0;
     }
 }
 
@@ -764,10 +767,15 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
 // vertex v is nearer to q than to the seed, so a box whose distance to every
 // vertex exceeds that vertex's distance to the seed holds no cutting point.
 // When the walk ends every point within the security radius has been clipped
-// or excluded, which is the certificate.  Points of a sub-bin are clipped in
+// or excluded, which is the certificate.  The walk also takes the cells that
+// failed for other reasons (predicates the absolute-frame determinants cannot
+// decide, plane or vertex overflow): it clips in the seed's local frame and
+// reuses plane slots, which removes most of those causes.  Points of a sub-bin are clipped in
 // their sorted order (by extended id within the sub-bin), so the result is
 // deterministic.
 constexpr int PRUNE_STACK = 64;
+constexpr int WALK_MAX_BOXES = 1 << 17;   // boxes popped per cell
+constexpr int WALK_MAX_POINTS = 1 << 15;  // points clipped per cell
 
 // squared distance from (x, y, z) to the box [lo, lo + side)^D
 template <int D>
@@ -799,20 +807,26 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
     const uint32_t s = cells[t];
     const uint32_t e = P.perm[s];
     const PT sp = spts[s];
+    // absolute seed; the cell is clipped in the frame centred on it (planes (-b, |b|^2 / 2)
+    // for b = B - seed), which keeps clump cells far from the origin well conditioned
     const double sx = sp.x, sy = sp.y, sz = pz(sp);
+    if (!(isfinite(sx) && isfinite(sy) && isfinite(sz))) {
+        store_failed(P, lane, e, ST_SECURITY_RADIUS_NOT_REACHED);
+        return;
+    }
 
-    // ---- the bounding box cell, as in k_clip (cell.cpp:42-104)
+    // ---- the bounding box cell (cell.cpp:42-104) in the local frame: w' = w + n . seed
     const double beps = 1e-14;
     const double xmin = -beps, xmax = 1.0 + beps;
     if (lane < 2 * D) {
         double4 pl;
         switch (lane) {
-            case 0: pl = make_double4(1.0, 0.0, 0.0, -xmin); break;
-            case 1: pl = make_double4(-1.0, 0.0, 0.0, xmax); break;
-            case 2: pl = make_double4(0.0, 1.0, 0.0, -xmin); break;
-            case 3: pl = make_double4(0.0, -1.0, 0.0, xmax); break;
-            case 4: pl = make_double4(0.0, 0.0, 1.0, -xmin); break;
-            default: pl = make_double4(0.0, 0.0, -1.0, xmax); break;
+            case 0: pl = make_double4(1.0, 0.0, 0.0, sx - xmin); break;
+            case 1: pl = make_double4(-1.0, 0.0, 0.0, xmax - sx); break;
+            case 2: pl = make_double4(0.0, 1.0, 0.0, sy - xmin); break;
+            case 3: pl = make_double4(0.0, -1.0, 0.0, xmax - sy); break;
+            case 4: pl = make_double4(0.0, 0.0, 1.0, sz - xmin); break;
+            default: pl = make_double4(0.0, 0.0, -1.0, xmax - sz); break;
         }
         W.hp[lane] = pl;
         W.vid[lane] = -1;
@@ -838,7 +852,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
     if (lane < ntri0) {
         double x, y, z;
         vertex_pos<D>(W.hp, W.tri[lane], x, y, z);
-        W.vd2[lane] = seed_d2(x, y, z, sx, sy, sz);
+        W.vd2[lane] = seed_d2(x, y, z, 0.0, 0.0, 0.0);
     }
     __syncwarp();
     int nb_v = 2 * D, nb_t = ntri0;
@@ -858,16 +872,19 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
     refresh();
     // true when no point of the box can cut the cell (with a relative margin for rounding)
     auto prunable = [&](const double (&lo)[3], double side) -> bool {
+        const double ll[3] = {lo[0] - sx, lo[1] - sy, lo[2] - sz};  // the box in the local frame
         bool ok = true;
 #pragma unroll
         for (int j = 0; j < 3; j++) {
             const int i = lane + 32 * j;
-            if (i < nb_t) ok = ok && pt_box_d2<D>(vx[j], vy[j], vz[j], lo, side) > W.vd2[i] * (1.0 + 1e-9);
+            if (i < nb_t) ok = ok && pt_box_d2<D>(vx[j], vy[j], vz[j], ll, side) > W.vd2[i] * (1.0 + 1e-9);
         }
         return __all_sync(FULL, ok);
     };
     const int G = g.G;
     const double h0 = 1.0 / (double)G;
+    // work bounds: a cell that needs more is left uncertified (reported, not hung)
+    int boxes = 0, points = 0;
     // clips by the points of level-L box (x, y, z), descending refined bins depth first
     auto visit = [&](int x0, int y0, int z0) -> bool {
         int sp_ = 0;
@@ -878,6 +895,13 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
             const int4 b = stk[--sp_];
             __syncwarp();
             const int L = b.w;
+            if (++boxes > WALK_MAX_BOXES || v_dist != v_dist) return false;
+            if (L > 0) {  // pushed while the cell was larger: test again
+                const double side = 1.0 / (double)(G << L);
+                const double lo[3] = {b.x * side, b.y * side, b.z * side};
+                if (pt_box_d2<D>(sx, sy, sz, lo, side) * (1.0 - 1e-12) > 4 * v_dist) continue;
+                if (prunable(lo, side)) continue;
+            }
             const int cx = b.x >> L, cy = b.y >> L, cz = b.z >> L;
             const uint32_t m = morton<D>(cx, cy, cz);
             const int Lb = g.lvl[m];
@@ -919,9 +943,10 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
             for (uint32_t q = a0; q < a1; q++) {
                 if (q == s) continue;
                 const PT B = spts[q];
-                const double bx = B.x, by = B.y, bz = pz(B);
-                if (seed_d2(bx, by, bz, sx, sy, sz) > 4 * v_dist) continue;
-                const int r = clip_by<D, true>(W, lane, P.perm[q], bx, by, bz, sx, sy, sz, P.robust, nb_v, nb_t,
+                const double bx = B.x - sx, by = B.y - sy, bz = pz(B) - sz;
+                if (seed_d2(bx, by, bz, 0.0, 0.0, 0.0) > 4 * v_dist) continue;
+                if (++points > WALK_MAX_POINTS) return false;
+                const int r = clip_by<D, true>(W, lane, P.perm[q], bx, by, bz, 0.0, 0.0, 0.0, P.robust, nb_v, nb_t,
                                                status, v_dist, fail_vdist);
                 if (r == CLIP_FAIL) return false;
                 if (r == CLIP_CUT) refresh();
@@ -974,6 +999,10 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
             const int dx = ci % w1 - r, rest = ci / w1;
             const int dy = rest % w1 - r, dz = D == 3 ? rest / w1 - r : 0;
             if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
+            if (++boxes > WALK_MAX_BOXES) {
+                alive = false;
+                break;
+            }
             const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
             if (x < 0 || x >= G || y < 0 || y >= G || (D == 3 && (z < 0 || z >= G))) continue;
             const double lo[3] = {x * h0, y * h0, z * h0};
@@ -982,12 +1011,16 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
             alive = visit(x, y, z);
         }
     }
+    if (lane == 0) {
+        atomicAdd(&P.walk_stats[0], (unsigned long long)points);
+        atomicAdd(&P.walk_stats[1], (unsigned long long)boxes);
+    }
     if (!alive || v_dist != v_dist) {
         store_failed(P, lane, e, status == ST_SUCCESS ? ST_SECURITY_RADIUS_NOT_REACHED : status);
         return;
     }
     // every point within the security radius was clipped or excluded: certified
-    extract_and_store<D>(W, P, w, lane, nb_v, nb_t, e, P.K + 1, sx, sy, sz);
+    extract_and_store<D>(W, P, w, lane, nb_v, nb_t, e, P.K + 1, 0.0, 0.0, 0.0, false, sx, sy, sz);
 }
 
 // ============================================================================
@@ -1514,7 +1547,10 @@ __global__ void k_flag_status(const uint32_t* __restrict__ qs, const uint32_t* _
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= nq) return;
     const uint32_t e = perm[qs[t]];
-    flag[t] = ((!hydro_only || e < (uint32_t)n_hydro) && status[e] == code) ? 1u : 0u;
+    const int st = status[e];
+    // code < 0: any failure (not SUCCESS, not skipped, not waiting for the FP64 re-clip)
+    const bool match = code >= 0 ? st == code : (st != ST_SUCCESS && st != ST_NOT_COMPUTED && st != ST_RECLIP);
+    flag[t] = ((!hydro_only || e < (uint32_t)n_hydro) && match) ? 1u : 0u;
 }
 
 // Compacts the cells whose status is `code` into `out` (query slots, or sorted
@@ -1579,6 +1615,7 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     P.f_own = (uint32_t*)c->f_own.p;
     P.f_geo = (double4*)c->f_geo.p;
     P.face_counter = &sc->face_count;
+    P.walk_stats = &sc->walk_points;
     P.overflow = &sc->overflow;
     P.face_cap = c->face_cap;
     if (nq > 0) {
@@ -1696,8 +1733,8 @@ cudaError_t launch_fallback(pgpu_ctx* c, int K2) {
     return cudaSuccess;
 }
 
-// Hydro cells still uncertified after the neighbour lists: clipped again by the
-// grid walk of k_clip_pruned, faces appended.
+// Hydro cells still failed after the neighbour lists (uncertified, or any other
+// failure): clipped again by the grid walk of k_clip_pruned, faces appended.
 cudaError_t launch_pruned(pgpu_ctx* c) {
     cudaError_t e = cudaSuccess;
     const int64_t nq = c->n_query;
@@ -1705,7 +1742,9 @@ cudaError_t launch_pruned(pgpu_ctx* c) {
     if (e) return e;
     uint32_t nf = 0;
     c->n_pruned = 0;
-    if ((e = select_cells(c, ST_SECURITY_RADIUS_NOT_REACHED, true, false, fq, &nf))) return e;
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    if ((e = cudaMemsetAsync(&sc->walk_points, 0, 2 * sizeof(unsigned long long), c->stream))) return e;
+    if ((e = select_cells(c, -1, true, false, fq, &nf))) return e;
     if (nf == 0) return cudaSuccess;
     unsigned long long fc = 0;
     unsigned of = 0, unc = 0;

@@ -151,17 +151,26 @@ __global__ void k_prim_dt(const double* __restrict__ mass, const double* __restr
     if (i < n) {
         const double V = vol[i];
         const double m = mass[i];
-        Prim s;
-        s.rho = m / V;
-        s.vx = mom[i * D] / m;
-        s.vy = mom[i * D + 1] / m;
-        s.vz = D == 3 ? mom[i * D + 2] / m : 0.0;
-        s.E = en[i] / V;
-        w4[i] = make_double4(s.rho, s.vx, s.vy, s.vz);
-        we[i] = s.E;
-        d = dt_cell<D>(s, V, cfl, gamma);
-        if (status[i] != ST_SUCCESS) atomicAdd(&sc->failed, 1u);
-        else atomicMax(&sc->cert_k_max, certk[i]);
+        if (status[i] != ST_SUCCESS || !(V > 0.0)) {
+            // a cell without a mesh cell this step keeps its conserved state: density -1
+            // marks it for k_flux_update (no fluxes, its faces are walls), it drifts with
+            // its velocity and takes no part in the time step
+            const double im = m > 0.0 ? 1.0 / m : 0.0;
+            w4[i] = make_double4(-1.0, mom[i * D] * im, mom[i * D + 1] * im, D == 3 ? mom[i * D + 2] * im : 0.0);
+            we[i] = 0.0;
+            atomicAdd(&sc->failed, 1u);
+        } else {
+            Prim s;
+            s.rho = m / V;
+            s.vx = mom[i * D] / m;
+            s.vy = mom[i * D + 1] / m;
+            s.vz = D == 3 ? mom[i * D + 2] / m : 0.0;
+            s.E = en[i] / V;
+            w4[i] = make_double4(s.rho, s.vx, s.vy, s.vz);
+            we[i] = s.E;
+            d = dt_cell<D>(s, V, cfl, gamma);
+            atomicMax(&sc->cert_k_max, certk[i]);
+        }
     }
     d = block_min(d);
     if (threadIdx.x == 0) atomicMin(&sc->dt_bits, dbits(d));
@@ -179,7 +188,8 @@ __global__ void k_flux_update(const double4* __restrict__ w4, const double* __re
     const double4 wi = w4[i];
     const Prim si = {wi.x, wi.y, wi.z, wi.w, we[i]};
     double tr = 0, tx = 0, ty = 0, tz = 0, te = 0;
-    const uint32_t fp = fptr[i], nf = fcnt[i];
+    const bool alive = wi.x >= 0.0;  // density -1: no mesh cell this step
+    const uint32_t fp = fptr[i], nf = alive ? fcnt[i] : 0u;
     unsigned nbox = 0, nunp = 0;
     for (uint32_t q = 0; q < nf; q++) {
         const uint32_t own = f_own[fp + q];
@@ -203,10 +213,11 @@ __global__ void k_flux_update(const double4* __restrict__ w4, const double* __re
                         found = true;
                         break;
                     }
-                if (!found) nunp++;
+                if (!found && w4[h].x >= 0.0) nunp++;
             }
         }
         const double4 wj4 = w4[h];
+        if (wj4.x < 0.0) continue;  // the neighbour has no mesh cell this step: a wall
         Prim sj = {wj4.x, wj4.y, wj4.z, wj4.w, we[h]};
         if (MIRROR && code) {
             uint32_t cd = code;

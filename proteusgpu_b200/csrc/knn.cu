@@ -275,6 +275,10 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
     const uint32_t s = qs[t];
     const PT p = spts[s];
     const uint32_t qid = perm[s];
+    if (!(isfinite(p.x) && isfinite(p.y) && isfinite(pz(p)))) {  // no neighbours for a point without a position
+        for (int idx = lane; idx < K; idx += 32) out[t * stride + idx] = NO_NEIGHBOR;
+        return;
+    }
     const double pc[3] = {p.x, p.y, pz(p)};
     // the query searches at its own bin's level: boxes of side 1 / (G << Lq)
     const int G0 = grid.G;

@@ -39,6 +39,8 @@ struct DevScalars {
     unsigned int reclip;            // cells the FP32 clip could not decide
     double dt;                      // the step's dt (device copy)
     double sums[5];                 // mass, mom x/y/z, energy
+    unsigned long long walk_points; // grid walk: points clipped (statistics; after the
+    unsigned long long walk_boxes;  //   per-step counters, which are cleared up to dt)
 };
 
 // Learned neighbour budget: a per-cell MLP (8 features -> 32 -> 32 -> 6 classes,

@@ -130,10 +130,10 @@ def test_robust_predicates_reflective(dim):
         assert_same_topology(g, o)
         check_fields(g, o, dim)
         return
-    # In 3D a few wall cells do not certify within K (the oracle reports them); the
-    # moving-mesh build walks the grid for those (cert_k = K + 1) and certifies most.
+    # In 3D a few wall cells fail within K (the oracle reports them); the moving-mesh
+    # build walks the grid for those (cert_k = K + 1) and certifies most.
     gs, os_ = np.asarray(g.status), np.asarray(o.status)
-    walked = (os_ == 3) & (gs == 4)
+    walked = (os_ != 4) & (gs == 4)
     assert walked.sum() > 0 and (np.asarray(g.cert_k)[walked] == k + 1).all()
     assert np.array_equal((gs == 4)[~walked], (os_ == 4)[~walked])
     okc = np.where(os_ == 4)[0]
