@@ -1,10 +1,10 @@
 #!/usr/bin/env python
 """Benchmark of the per-timestep mesh-and-flux path (one JSON line on stdout).
 
-A step is one full moving-mesh step of the 3D Sedov-Taylor workload
-(1,048,576 uniform points): ghost layer, Morton grid sort, KNN, clipping with
-the security-radius certificate, extraction, CFL time step, HLL flux +
-conserved update + drift.  The metric is hydro cell-updates per second (one
+A step is one full moving-mesh step of the clustered 3D Sedov-Taylor workload
+(16,777,216 points, 70 % of them in 64 Gaussian clumps): ghost layer, two-level
+Morton grid sort, KNN, clipping with the security-radius certificate,
+extraction, CFL time step, HLL flux + conserved update + drift.  The metric is hydro cell-updates per second (one
 hydro cell advanced one full step) of the learned-K + FP32-clipping form, with
 the plain fixed-K (190) FP64 form timed beside it on the same states.
 
@@ -34,11 +34,14 @@ sys.path.insert(0, ROOT)
 METRIC = "Voronoi cell-updates/s per B200: learned-K+FP32 vs plain GPU, at matched L1 err"
 UNIT = "cell-updates/s"
 
-# Workloads.  sedov3d_1m is the configuration the metric is quoted on for one GPU
-# (3D Sedov, plain method); the others are smaller cases (profiling, smoke).
+# Workloads.  clustered3d_16m is the configuration the metric is quoted on (3D
+# clustered Sedov, 16,777,216 points: 70 % in 64 Gaussian clumps, seed 4); the
+# others are the uniform 3D Sedov (1M points) and smaller profiling/smoke cases.
 CONFIGS = {
     "clustered3d_16m": dict(dim=3, n=16_777_216, seed=4, k=190, buff=0.04, boundary="periodic", cfl=0.3,
                             ic="clustered"),
+    "clustered3d_1m": dict(dim=3, n=1_048_576, seed=4, k=190, buff=0.04 * 16 ** (1 / 3), boundary="periodic",
+                           cfl=0.3, ic="clustered"),
     "sedov3d_1m": dict(dim=3, n=1_048_576, seed=2, k=190, buff=0.04, boundary="periodic", cfl=0.3),
     "sedov3d_256k": dict(dim=3, n=262_144, seed=2, k=190, buff=0.04 * 4 ** (1 / 3), boundary="periodic", cfl=0.3),
     "sod2d_10k": dict(dim=2, n=10_000, seed=1, k=16, buff=0.04, boundary="reflective", cfl=0.3),
@@ -64,7 +67,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--config", choices=sorted(CONFIGS), default="sedov3d_1m")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="clustered3d_16m")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
     ap.add_argument("--skip-e2e", action="store_true", help="omit the end-to-end leg")
     ap.add_argument("--skip-forms", action="store_true",
@@ -144,16 +147,18 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU reference
-def cpu_reference_step_rate(steps: int, n_sample: int = 20000, nthreads: int | None = None):
+def cpu_reference_step_rate(steps: int, cfg: dict, n_sample: int = 20000, nthreads: int | None = None):
     """Cell-updates/s of the reference's own CPU code (oracle/_ref, compiled from its sources) on a
-    bounded sample of the 3D Sedov workload: per step compute_periodic_mesh (KNN + clipping + extraction)
-    + dt_CFL + hydro_step; ghost layer widened so that it spans the same number of cells as buff = 0.04
-    does at 1,048,576 points.  Falls back to the C restatement (oracle/liboracle.so) if _ref is absent."""
+    bounded sample of the workload (same distribution, n_sample points): per step compute_periodic_mesh
+    (KNN + clipping + extraction) + dt_CFL + hydro_step; the ghost layer is widened so that it spans
+    the same number of (mean) cells as the workload's buff does at its full size, at most 0.15.  Falls
+    back to the C restatement (oracle/liboracle.so) if _ref is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from proteusgpu_b200 import ics
     nthreads = nthreads or os.cpu_count() or 1
-    ic = ics.sedov_3d(n=n_sample, seed=2)
-    buff = 0.04 * (1_048_576 / n_sample) ** (1 / 3)
+    clustered = cfg.get("ic") == "clustered"
+    ic = ics.clustered_3d(n=n_sample, seed=cfg["seed"]) if clustered else ics.sedov_3d(n=n_sample, seed=2)
+    buff = min(cfg["buff"] * (cfg["n"] / n_sample) ** (1 / 3), 0.15)
     kind = "reference"
     try:
         import refbuild as rb
@@ -181,8 +186,8 @@ def cpu_reference_step_rate(steps: int, n_sample: int = 20000, nthreads: int | N
             rho, vel, E, _ = om.hydro_step_ref(m, dt, ic.gamma, rho, vel, E)
         times.append(time.perf_counter() - t0)
     t = float(np.mean(times))
-    sample = (f"3D Sedov, {n_sample} uniform points (seed 2), K=190, buff {buff:.3f}, {steps} step(s) of "
-              "compute_periodic_mesh + dt_CFL + hydro_step")
+    sample = (f"3D Sedov, {n_sample} {'clustered' if clustered else 'uniform'} points, K=190, buff {buff:.3f}, "
+              f"{steps} step(s) of compute_periodic_mesh + dt_CFL + hydro_step")
     return n_sample / t, kind, nthreads, sample, t
 
 
@@ -199,8 +204,8 @@ FORMS = {
 HEADLINE, BASELINE_FORM = "learned_fp32", "plain_fp64"
 
 # DRAM bytes per cell of one k_clip32 launch, from the ncu capture summarised in
-# profiles/k_clip32_sedov3d_256k.md (read + write / cells), used for `traffic`.
-CLIP32_DRAM_BYTES_PER_CELL = (143.396608e6 + 161.378048e6) / 262_144
+# profiles/k_clip32_clustered3d_1m.md (read + write / cells), used for `traffic`.
+CLIP32_DRAM_BYTES_PER_CELL = (713.581312e6 + 822.387968e6) / 1_048_576
 
 
 def _barrier(dist):
@@ -229,7 +234,7 @@ def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks
                   gamma=ic.gamma, device=local_rank, precision=spec["precision"])
     if spec["kbudget"]:
         # the warm-up steps but the last train the proposal; the last one already uses it
-        ctx.kbudget_enable(train_steps=max(1, args.warmup - 1), iters_per_step=64, quantile=0.99, seed=1)
+        ctx.kbudget_enable(train_steps=max(1, args.warmup - 1), iters_per_step=256, quantile=0.98, seed=1)
     ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
     for _ in range(max(args.warmup, 0)):
         ctx.sim_step(cfg["cfl"], want_dt=False)
@@ -345,7 +350,8 @@ def run_ours(args, rank, world, local_rank):
         roof = {"kernel": "k_clip32 (+ FP64 re-clip of undecided cells)", "bound": "fp32", "achieved": ach,
                 "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
                 "traffic": CLIP32_DRAM_BYTES_PER_CELL * n_query,
-                "traffic_note": "DRAM bytes per launch, ncu capture at 262,144 cells scaled by cells",
+                "traffic_note": "DRAM bytes per launch: ncu capture of the clustered 1,048,576-cell case "
+                                "(K = 190 lists) scaled by cells",
                 "peak_source": "FP32 FMA rate measured in this run (pgpu_fp32_peak)",
                 "work": f"{W['clip_flop_per_cell']:.0f} algorithmic flop per cell x {n_query} cells"}
     elif dom == "knn":
@@ -366,10 +372,11 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if not args.skip_cpu and world == 1:
-        v, kind, cores, sample, t_step = cpu_reference_step_rate(steps=2)
+        v, kind, cores, sample, t_step = cpu_reference_step_rate(steps=2, cfg=cfg)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
                "s_per_step": t_step}
-    wl = (f"{args.config}: 3D Sedov-Taylor blast, {cfg['n']} uniform points (seed {cfg['seed']}), "
+    dist_name = "clustered (70% in 64 Gaussian clumps)" if cfg.get("ic") == "clustered" else "uniform"
+    wl = (f"{args.config}: 3D Sedov-Taylor blast, {cfg['n']} {dist_name} points (seed {cfg['seed']}), "
           f"moving mesh, {cfg['boundary']} box" if D == 3 else args.config)
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -404,9 +411,9 @@ def run_reference(args, rank):
     v_all = []
     kind = cores = sample = None
     if warm:
-        cpu_reference_step_rate(steps=1)
+        cpu_reference_step_rate(steps=1, cfg=CONFIGS[args.config])
     for _ in range(steps):
-        v, kind, cores, sample, _t = cpu_reference_step_rate(steps=1)
+        v, kind, cores, sample, _t = cpu_reference_step_rate(steps=1, cfg=CONFIGS[args.config])
         v_all.append(v)
     v = float(np.mean(v_all))
     cfg = CONFIGS[args.config]
