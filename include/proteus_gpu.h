@@ -219,6 +219,22 @@ typedef struct {
 /* Statistics of the last step (synchronises the stream). */
 int pgpu_sim_stats(pgpu_ctx *ctx, pgpu_stats *out);
 
+/* ---------------------------------------------------------- batches ---
+ * Extension (the reference runs one simulation per process).  n_inst
+ * independent moving-mesh simulations of uneven sizes advanced together: their
+ * points are concatenated (instance b owns hydro ids [sum counts[<b], +counts[b])
+ * of pos/rho/v/E/deposit, each in its own unit box) and every stage of a step is
+ * one launch over all of them.  Each instance keeps its own ghost layer (buff),
+ * gamma, boundary (PGPU_PERIODIC / PGPU_REFLECTIVE), grid and CFL time step, so
+ * its mesh and state are the ones it gets when run alone.  Faces and neighbour
+ * ids refer to the concatenated ids.  Needs flux_mode PGPU_FLUX_PHYSICAL; then
+ * pgpu_sim_step / sim_get / sim_set / download_mesh work on the whole batch
+ * (the step's dt_out is the smallest instance dt; pgpu_batch_dt gives each). */
+int pgpu_batch_init(pgpu_ctx *ctx, int n_inst, const int64_t *counts, const double *buff, const double *gamma,
+                    const int *boundary, const double *pos, const double *rho, const double *v, const double *E,
+                    const double *deposit);
+int pgpu_batch_dt(pgpu_ctx *ctx, double *dt_per_instance);
+
 /* ------------------------------------------- learned neighbour budget ---
  * Extension (the reference uses one compile-time _K_ for every cell, Config.sh,
  * src/knn/knn.cpp:225-315).  When enabled, every mesh build of a moving-mesh

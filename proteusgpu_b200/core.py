@@ -198,6 +198,28 @@ class Context:
         check(self._h, self._L.pgpu_sim_init(self._h, _ptr(pos), _ptr(rho), _ptr(v), _ptr(E), _ptr(dep), len(pos)),
               "pgpu_sim_init")
 
+    def batch_init(self, counts, buff, gamma, boundary, pos, rho, v, E, deposit=None) -> None:
+        """Independent simulations advanced together (extension): instance b owns the
+        next counts[b] rows of pos/rho/v/E; buff, gamma, boundary ("periodic" or
+        "reflective") per instance."""
+        counts = np.ascontiguousarray(counts, np.int64)
+        nb = len(counts)
+        bf = np.ascontiguousarray(np.broadcast_to(np.asarray(buff, np.float64), (nb,)))
+        gm = np.ascontiguousarray(np.broadcast_to(np.asarray(gamma, np.float64), (nb,)))
+        bd = np.ascontiguousarray([_lib.BOUNDARY[b] if isinstance(b, str) else int(b) for b in
+                                   np.broadcast_to(np.asarray(boundary, object), (nb,))], np.int32)
+        pos, rho, v, E = _c64(pos), _c64(rho), _c64(v), _c64(E)
+        dep = None if deposit is None else _c64(deposit)
+        check(self._h, self._L.pgpu_batch_init(self._h, nb, _ptr(counts), _ptr(bf), _ptr(gm), _ptr(bd), _ptr(pos),
+                                               _ptr(rho), _ptr(v), _ptr(E), _ptr(dep)), "pgpu_batch_init")
+        self._n_inst = nb
+
+    def batch_dt(self) -> np.ndarray:
+        """Each instance's dt of the last step."""
+        out = np.zeros(getattr(self, "_n_inst", 1))
+        check(self._h, self._L.pgpu_batch_dt(self._h, _ptr(out)), "pgpu_batch_dt")
+        return out
+
     def sim_step(self, cfl: float = 0.3, fixed_dt: float = 0.0, want_dt: bool = True) -> float | None:
         dt = C.c_double()
         check(self._h, self._L.pgpu_sim_step(self._h, cfl, fixed_dt, C.byref(dt) if want_dt else None),

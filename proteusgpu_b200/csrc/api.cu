@@ -270,6 +270,7 @@ int pgpu_knn(pgpu_ctx* c, const double* pts, int64_t n, uint32_t* out) {
     if (r) return r;
     if ((!pts && n > 0) || n < 0) return fail(c, PGPU_EINVAL, "pgpu_knn: bad points");
     if ((r = upload_points(c, pts, n))) return r;
+    CK(pgpu::set_single_instance(c, n));
     mark(c, 0);
     CK(pgpu::launch_ghosts(c, (const double*)c->pos.p, n, true));
     mark(c, 1);
@@ -317,6 +318,7 @@ int pgpu_periodic_mesh(pgpu_ctx* c, const double* pts, int64_t n, int64_t* n_see
     if (r) return r;
     if ((!pts && n > 0) || n < 0) return fail(c, PGPU_EINVAL, "pgpu_periodic_mesh: bad points");
     if ((r = upload_points(c, pts, n))) return r;
+    CK(pgpu::set_single_instance(c, n));
     if ((r = build_mesh(c, n, false, true))) return r;
     mark(c, 5);
     c->have_sim = false;
@@ -330,6 +332,7 @@ int pgpu_compute_mesh(pgpu_ctx* c, const double* pts, int64_t n, int64_t* num_fa
     if (r) return r;
     if ((!pts && n > 0) || n < 0) return fail(c, PGPU_EINVAL, "pgpu_compute_mesh: bad points");
     if ((r = upload_points(c, pts, n))) return r;
+    CK(pgpu::set_single_instance(c, n));
     if ((r = build_mesh(c, n, true, true))) return r;
     mark(c, 5);
     c->have_sim = false;
@@ -519,11 +522,54 @@ int pgpu_hydro_step(pgpu_ctx* c, double dt) {
 }
 
 // ------------------------------------------------------------------ moving mesh
+static int sim_init_common(pgpu_ctx* c, const double* pos, const double* rho, const double* v, const double* E,
+                           const double* deposit, int64_t n);
+
 int pgpu_sim_init(pgpu_ctx* c, const double* pos, const double* rho, const double* v, const double* E,
                   const double* deposit, int64_t n) {
     int r = check_ctx(c);
     if (r) return r;
     if (n <= 0 || !pos || !rho || !v || !E) return fail(c, PGPU_EINVAL, "pgpu_sim_init: bad arguments");
+    CK(pgpu::set_single_instance(c, n));
+    return sim_init_common(c, pos, rho, v, E, deposit, n);
+}
+
+int pgpu_batch_init(pgpu_ctx* c, int n_inst, const int64_t* counts, const double* buff, const double* gamma,
+                    const int* boundary, const double* pos, const double* rho, const double* v, const double* E,
+                    const double* deposit) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (n_inst < 1 || n_inst > 65535 || !counts || !buff || !gamma || !boundary || !pos || !rho || !v || !E)
+        return fail(c, PGPU_EINVAL, "pgpu_batch_init: bad arguments");
+    int64_t n = 0;
+    for (int b = 0; b < n_inst; b++) {
+        if (counts[b] <= 0 || !(buff[b] > 0.0 && buff[b] < 0.5) || !(gamma[b] > 1.0) ||
+            (boundary[b] != PGPU_PERIODIC && boundary[b] != PGPU_REFLECTIVE))
+            return fail(c, PGPU_EINVAL, "pgpu_batch_init: bad instance parameters");
+        n += counts[b];
+    }
+    if (c->prm.flux_mode != PGPU_FLUX_PHYSICAL)
+        return fail(c, PGPU_EINVAL, "pgpu_batch_init: batches use PGPU_FLUX_PHYSICAL");
+    CK(pgpu::set_instances(c, n_inst, counts, buff, gamma, boundary));
+    return sim_init_common(c, pos, rho, v, E, deposit, n);
+}
+
+int pgpu_batch_dt(pgpu_ctx* c, double* dt) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!dt) return PGPU_EINVAL;
+    if (!c->have_sim) return fail(c, PGPU_ESTATE, "pgpu_batch_dt: no simulation");
+    std::vector<unsigned long long> bits(c->inst.n);
+    CK(cudaMemcpyAsync(bits.data(), c->inst.d_dt.p, c->inst.n * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    std::memcpy(dt, bits.data(), c->inst.n * sizeof(double));
+    return PGPU_OK;
+}
+
+static int sim_init_common(pgpu_ctx* c, const double* pos, const double* rho, const double* v, const double* E,
+                           const double* deposit, int64_t n) {
+    int r = 0;
     if ((r = upload_points(c, pos, n))) return r;
     c->have_mesh = false;
     if ((r = build_mesh(c, n, false, false))) return r;

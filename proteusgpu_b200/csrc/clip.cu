@@ -175,7 +175,8 @@ struct ClipParams {
     int robust;
     unsigned int* uncertified;  // hydro cells ending with SECURITY_RADIUS_NOT_REACHED
     unsigned int* reclip;       // cells the FP32 kernel hands to the FP64 kernel
-    double vscale, ascale, scale;  // unit box -> physical
+    const InstPar* ip;      // per instance: unit box -> physical scale (scale_out)
+    const uint16_t* inst;   // instance of each extended id
     double* vol;
     uint32_t* fptr;
     uint32_t* fcnt;
@@ -390,6 +391,10 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
         cen[1] = sy + cen[1] / sv;
         cen[2] = sz + cen[2] / sv;
     }
+    // unit box -> physical: the cell's instance's 1 + 2 buff
+    const double uscale = P.ip[P.inst[e]].scale_out;
+    const double vscale = D == 2 ? uscale * uscale : uscale * uscale * uscale;
+    const double ascale = D == 2 ? uscale : uscale * uscale;
     unsigned long long base = 0;
     if (lane == 0) base = atomicAdd(P.face_counter, (unsigned long long)nf);
     base = __shfl_sync(FULL, base, 0);
@@ -416,18 +421,18 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
                     own = pack_owner(P.ghost_src[nbr - P.n_hydro], P.ghost_code[nbr - P.n_hydro]);
             }
             P.f_own[f] = own;
-            P.f_geo[f] = make_double4(pe.x / nlen, pe.y / nlen, pe.z / nlen, P.ascale * area[pass]);
+            P.f_geo[f] = make_double4(pe.x / nlen, pe.y / nlen, pe.z / nlen, ascale * area[pass]);
         }
     }
     if (lane == 0) {
-        P.vol[e] = P.vscale * cell_vol;
+        P.vol[e] = vscale * cell_vol;
         P.fptr[e] = fits ? (uint32_t)base : 0u;
         P.fcnt[e] = fits ? (uint32_t)nf : 0u;
         P.status[e] = ST_SUCCESS;
         P.certk[e] = certk;
-        P.centroid[3 * (size_t)e] = (cen[0] + ox - 0.5) * P.scale + 0.5;
-        P.centroid[3 * (size_t)e + 1] = (cen[1] + oy - 0.5) * P.scale + 0.5;
-        P.centroid[3 * (size_t)e + 2] = D == 3 ? (cen[2] + oz - 0.5) * P.scale + 0.5 : 0.0;
+        P.centroid[3 * (size_t)e] = (cen[0] + ox - 0.5) * uscale + 0.5;
+        P.centroid[3 * (size_t)e + 1] = (cen[1] + oy - 0.5) * uscale + 0.5;
+        P.centroid[3 * (size_t)e + 2] = D == 3 ? (cen[2] + oz - 0.5) * uscale + 0.5 : 0.0;
     }
 }
 
@@ -881,7 +886,9 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
         }
         return __all_sync(FULL, ok);
     };
-    const int G = g.G;
+    const InstPar& ipc = g.ip[g.inst[e]];  // the cell's instance: its grid
+    const int G = ipc.G;
+    const uint32_t slot0 = ipc.slot0;
     const double h0 = 1.0 / (double)G;
     // work bounds: a cell that needs more is left uncertified (reported, not hung)
     int boxes = 0, points = 0;
@@ -903,7 +910,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
                 if (prunable(lo, side)) continue;
             }
             const int cx = b.x >> L, cy = b.y >> L, cz = b.z >> L;
-            const uint32_t m = morton<D>(cx, cy, cz);
+            const uint32_t m = slot0 + morton<D>(cx, cy, cz);
             const int Lb = g.lvl[m];
             if (L < Lb) {
                 // children nearest first: pushed farthest first
@@ -1602,9 +1609,8 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     P.robust = c->prm.predicates == PGPU_PRED_ROBUST;
     P.uncertified = &sc->uncertified;
     P.reclip = &sc->reclip;
-    P.scale = c->unit_scale;
-    P.vscale = D == 2 ? P.scale * P.scale : P.scale * P.scale * P.scale;
-    P.ascale = D == 2 ? P.scale : P.scale * P.scale;
+    P.ip = (const InstPar*)c->inst.d_par.p;
+    P.inst = (const uint16_t*)c->inst.d_inst_e.p;
     P.vol = (double*)c->vol.p;
     P.fptr = (uint32_t*)c->fptr.p;
     P.fcnt = (uint32_t*)c->fcnt.p;
@@ -1621,7 +1627,8 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     if (nq > 0) {
         const unsigned blocks = (unsigned)((nq + CLIP_WARPS - 1) / CLIP_WARPS);
         if (pruned) {
-            const SubGrid g = {c->grid_G, (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
+            const SubGrid g = {(const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
+                               (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
                                (const uint32_t*)c->sub_start.p};
             const int2* tab = (const int2*)c->knn_table.p;
             if (D == 2)

@@ -38,9 +38,11 @@ __global__ void k_gather_faces(const uint32_t* __restrict__ fptr, const uint32_t
 // others hold the scaled-back zero.
 template <int D>
 __global__ void k_seeds(const typename PointOf<D>::type* __restrict__ ext, const int* __restrict__ status,
-                        int64_t n, double scale, int no_scale, double* __restrict__ out) {
+                        int64_t n, const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst, int no_scale,
+                        double* __restrict__ out) {
     int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
+    const double scale = ip[inst[e]].scale_out;
     const typename PointOf<D>::type p = ext[e];
     const bool ok = status[e] == ST_SUCCESS;
     double c[3] = {ok ? p.x : 0.0, ok ? p.y : 0.0, ok ? pz(p) : 0.0};
@@ -83,9 +85,13 @@ cudaError_t launch_seeds(pgpu_ctx* c, double* out, bool no_scale) {
     const int64_t n = c->n_ext;
     if (n <= 0) return cudaSuccess;
     if (c->prm.dim == 2)
-        k_seeds<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, (const int*)c->status.p, n, c->unit_scale, no_scale, out);
+        k_seeds<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, (const int*)c->status.p, n,
+                                                        (const InstPar*)c->inst.d_par.p,
+                                                        (const uint16_t*)c->inst.d_inst_e.p, no_scale, out);
     else
-        k_seeds<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, (const int*)c->status.p, n, c->unit_scale, no_scale, out);
+        k_seeds<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, (const int*)c->status.p, n,
+                                                        (const InstPar*)c->inst.d_par.p,
+                                                        (const uint16_t*)c->inst.d_inst_e.p, no_scale, out);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -144,11 +144,14 @@ template <int D>
 __global__ void k_prim_dt(const double* __restrict__ mass, const double* __restrict__ mom,
                           const double* __restrict__ en, const double* __restrict__ vol,
                           const int* __restrict__ status, const int* __restrict__ certk, int64_t n, double cfl,
-                          double gamma, double4* __restrict__ w4, double* __restrict__ we,
-                          DevScalars* __restrict__ sc) {
+                          const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst,
+                          unsigned long long* __restrict__ dt_inst, double4* __restrict__ w4,
+                          double* __restrict__ we, DevScalars* __restrict__ sc) {
     int64_t i = (int64_t)blockIdx.x * HT + threadIdx.x;
     double d = 1e100;
+    const int b = i < n ? inst[i] : -1;
     if (i < n) {
+        const double gamma = ip[b].gamma;
         const double V = vol[i];
         const double m = mass[i];
         if (status[i] != ST_SUCCESS || !(V > 0.0)) {
@@ -172,19 +175,40 @@ __global__ void k_prim_dt(const double* __restrict__ mass, const double* __restr
             atomicMax(&sc->cert_k_max, certk[i]);
         }
     }
-    d = block_min(d);
-    if (threadIdx.x == 0) atomicMin(&sc->dt_bits, dbits(d));
+    // each instance has its own time step; a block inside one instance reduces first
+    __shared__ int s_b0;
+    if (threadIdx.x == 0) s_b0 = b;
+    __syncthreads();
+    const int b0 = s_b0;
+    const bool uniform = __syncthreads_and(b == b0 || b < 0) != 0;
+    if (uniform) {
+        const double m = block_min(d);
+        if (threadIdx.x == 0) {
+            atomicMin(&sc->dt_bits, dbits(m));
+            if (b0 >= 0) atomicMin(&dt_inst[b0], dbits(m));
+        }
+    } else {
+        const double m = block_min(d);
+        if (threadIdx.x == 0) atomicMin(&sc->dt_bits, dbits(m));
+        if (b >= 0) atomicMin(&dt_inst[b], dbits(d));
+    }
 }
 
-template <int D, bool PHYSICAL, bool MIRROR>
+template <int D, bool PHYSICAL, int MIRROR>
 __global__ void k_flux_update(const double4* __restrict__ w4, const double* __restrict__ we,
                               const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fcnt,
                               const uint32_t* __restrict__ f_own, const double4* __restrict__ f_geo, int64_t n,
-                              double gamma, double fixed_dt, double* __restrict__ mass, double* __restrict__ mom,
-                              double* __restrict__ en, double* __restrict__ pos, DevScalars* __restrict__ sc) {
+                              const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst,
+                              const unsigned long long* __restrict__ dt_inst, double fixed_dt,
+                              double* __restrict__ mass, double* __restrict__ mom, double* __restrict__ en,
+                              double* __restrict__ pos, DevScalars* __restrict__ sc) {
     int64_t i = (int64_t)blockIdx.x * HT + threadIdx.x;
     if (i >= n) return;
-    const double dt = fixed_dt > 0 ? fixed_dt : __longlong_as_double((long long)sc->dt_bits);
+    const int b = inst[i];
+    const double gamma = ip[b].gamma;
+    // MIRROR 0 / 1: every instance periodic / walled; 2: per instance
+    const bool mirror = MIRROR == 2 ? ip[b].mirror != 0 : MIRROR == 1;
+    const double dt = fixed_dt > 0 ? fixed_dt : __longlong_as_double((long long)dt_inst[b]);
     const double4 wi = w4[i];
     const Prim si = {wi.x, wi.y, wi.z, wi.w, we[i]};
     double tr = 0, tx = 0, ty = 0, tz = 0, te = 0;
@@ -204,7 +228,7 @@ __global__ void k_flux_update(const double4* __restrict__ w4, const double* __re
             code = own >> OWNER_BITS;
             if (PHYSICAL && h < (uint32_t)i) {
                 // the lower hydro id's value of this face's area
-                const uint32_t want = pack_owner((uint32_t)i, reverse_code(code, D, !MIRROR));
+                const uint32_t want = pack_owner((uint32_t)i, reverse_code(code, D, !mirror));
                 const uint32_t hp = fptr[h], hn = fcnt[h];
                 bool found = false;
                 for (uint32_t r = 0; r < hn; r++)
@@ -219,7 +243,7 @@ __global__ void k_flux_update(const double4* __restrict__ w4, const double* __re
         const double4 wj4 = w4[h];
         if (wj4.x < 0.0) continue;  // the neighbour has no mesh cell this step: a wall
         Prim sj = {wj4.x, wj4.y, wj4.z, wj4.w, we[h]};
-        if (MIRROR && code) {
+        if (mirror && code) {
             uint32_t cd = code;
             if (cd % 3) sj.vx = -sj.vx;
             cd /= 3;
@@ -246,7 +270,7 @@ __global__ void k_flux_update(const double4* __restrict__ w4, const double* __re
 #pragma unroll
     for (int a = 0; a < D; a++) {
         double p = pos[i * D + a] + vv[a] * dt;
-        if (!MIRROR) {
+        if (!mirror) {
             if (p < 0.0) p += 1.0;
             if (p >= 1.0) p -= 1.0;
         } else {
@@ -371,10 +395,14 @@ cudaError_t launch_prim_dt(pgpu_ctx* c, double cfl, double fixed_dt) {
     double* we = ensure<double>(c->we, n + 1, &e);
     if (e) return e;
     DevScalars* sc = (DevScalars*)c->scalars.p;
-    // reset the per-step statistics and the dt accumulator (1e100 as the reference's start value)
+    // reset the per-step statistics and the dt accumulators (1e100 as the reference's start value)
     DevScalars init{};
     init.dt_bits = 0x54B249AD2594C37Dull;
     if ((e = cudaMemcpyAsync(&sc->dt_bits, &init.dt_bits, sizeof(init.dt_bits), cudaMemcpyHostToDevice, c->stream)))
+        return e;
+    c->inst.dt_init.assign(c->inst.n, init.dt_bits);
+    if ((e = cudaMemcpyAsync(c->inst.d_dt.p, c->inst.dt_init.data(), c->inst.n * sizeof(unsigned long long),
+                             cudaMemcpyHostToDevice, c->stream)))
         return e;
     if ((e = cudaMemsetAsync(&sc->overflow, 0, offsetof(DevScalars, dt) - offsetof(DevScalars, overflow),
                              c->stream)))
@@ -385,12 +413,16 @@ cudaError_t launch_prim_dt(pgpu_ctx* c, double cfl, double fixed_dt) {
             k_prim_dt<2><<<nblk(n, HT), HT, 0, c->stream>>>((const double*)c->mass.p, (const double*)c->mom.p,
                                                             (const double*)c->en.p, (const double*)c->vol.p,
                                                             (const int*)c->status.p, (const int*)c->certk.p, n, cfl,
-                                                            c->prm.gamma, w4, we, sc);
+                                                            (const InstPar*)c->inst.d_par.p,
+                                                            (const uint16_t*)c->inst.d_inst_h.p,
+                                                            (unsigned long long*)c->inst.d_dt.p, w4, we, sc);
         else
             k_prim_dt<3><<<nblk(n, HT), HT, 0, c->stream>>>((const double*)c->mass.p, (const double*)c->mom.p,
                                                             (const double*)c->en.p, (const double*)c->vol.p,
                                                             (const int*)c->status.p, (const int*)c->certk.p, n, cfl,
-                                                            c->prm.gamma, w4, we, sc);
+                                                            (const InstPar*)c->inst.d_par.p,
+                                                            (const uint16_t*)c->inst.d_inst_h.p,
+                                                            (unsigned long long*)c->inst.d_dt.p, w4, we, sc);
         count_launches(1);
     }
     return cudaGetLastError();
@@ -402,25 +434,31 @@ cudaError_t launch_flux_update(pgpu_ctx* c, double fixed_dt) {
     if (n <= 0) return cudaSuccess;
     DevScalars* sc = (DevScalars*)c->scalars.p;
     const bool phys = c->prm.flux_mode == PGPU_FLUX_PHYSICAL;
-    const bool mir = c->prm.boundary == PGPU_REFLECTIVE;
+    // walls: 0 all periodic, 1 all reflective, 2 mixed across the instances of a batch
+    int mir = c->inst.par[0].mirror;
+    for (const auto& q : c->inst.par)
+        if (q.mirror != c->inst.par[0].mirror) mir = 2;
 #define PGPU_FLUX(DD, PH, MI)                                                                                     \
     k_flux_update<DD, PH, MI><<<nblk(n, HT), HT, 0, c->stream>>>(                                                \
         (const double4*)c->w4.p, (const double*)c->we.p, (const uint32_t*)c->fptr.p, (const uint32_t*)c->fcnt.p, \
-        (const uint32_t*)c->f_own.p, (const double4*)c->f_geo.p, n, c->prm.gamma, fixed_dt, (double*)c->mass.p,  \
-        (double*)c->mom.p, (double*)c->en.p, (double*)c->pos.p, sc)
+        (const uint32_t*)c->f_own.p, (const double4*)c->f_geo.p, n, (const InstPar*)c->inst.d_par.p,              \
+        (const uint16_t*)c->inst.d_inst_h.p, (const unsigned long long*)c->inst.d_dt.p, fixed_dt,                 \
+        (double*)c->mass.p, (double*)c->mom.p, (double*)c->en.p, (double*)c->pos.p, sc)
+#define PGPU_FLUX_M(DD, PH) \
+    do {                    \
+        if (mir == 0)       \
+            PGPU_FLUX(DD, PH, 0); \
+        else if (mir == 1)  \
+            PGPU_FLUX(DD, PH, 1); \
+        else                \
+            PGPU_FLUX(DD, PH, 2); \
+    } while (0)
     if (D == 2) {
-        if (phys) {
-            if (mir) PGPU_FLUX(2, true, true); else PGPU_FLUX(2, true, false);
-        } else {
-            if (mir) PGPU_FLUX(2, false, true); else PGPU_FLUX(2, false, false);
-        }
+        if (phys) PGPU_FLUX_M(2, true); else PGPU_FLUX_M(2, false);
     } else {
-        if (phys) {
-            if (mir) PGPU_FLUX(3, true, true); else PGPU_FLUX(3, true, false);
-        } else {
-            if (mir) PGPU_FLUX(3, false, true); else PGPU_FLUX(3, false, false);
-        }
+        if (phys) PGPU_FLUX_M(3, true); else PGPU_FLUX_M(3, false);
     }
+#undef PGPU_FLUX_M
 #undef PGPU_FLUX
     count_launches(1);
     return cudaGetLastError();

@@ -446,7 +446,8 @@ __global__ void k_mlp_bf16_all(const float* __restrict__ w, uint16_t* __restrict
 template <int D>
 __global__ void k_kb_features(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ perm,
                               const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ bin_start,
-                              int G, int64_t nq, int64_t n_hydro, const int* __restrict__ certk,
+                              const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst, int64_t nq,
+                              int64_t n_hydro, const int* __restrict__ certk,
                               const double* __restrict__ vol, const uint32_t* __restrict__ fcnt,
                               const double* __restrict__ centroid, const double* __restrict__ pos,
                               float* __restrict__ hist_vol, uint8_t* __restrict__ miss, float* __restrict__ feat) {
@@ -457,8 +458,10 @@ __global__ void k_kb_features(const uint32_t* __restrict__ qs, const uint32_t* _
     float f[KB_FEATURES] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (e < (uint32_t)n_hydro) {
         const typename PointOf<D>::type p = spts[s];
+        const InstPar& par = ip[inst[e]];
+        const int G = par.G;
         const int bx = bin_coord(p.x, G), by = bin_coord(p.y, G), bz = D == 3 ? bin_coord(pz(p), G) : 0;
-        const uint32_t own = morton<D>(bx, by, bz);
+        const uint32_t own = par.slot0 + morton<D>(bx, by, bz);
         const uint32_t occ = bin_start[own + 1] - bin_start[own];
         uint32_t occ_nb = 0;
         for (int dz = (D == 3 ? -1 : 0); dz <= (D == 3 ? 1 : 0); dz++)
@@ -466,7 +469,7 @@ __global__ void k_kb_features(const uint32_t* __restrict__ qs, const uint32_t* _
                 for (int dx = -1; dx <= 1; dx++) {
                     const int x = bx + dx, y = by + dy, z = bz + dz;
                     if (x < 0 || x >= G || y < 0 || y >= G || (D == 3 && (z < 0 || z >= G))) continue;
-                    const uint32_t k = morton<D>(x, y, z);
+                    const uint32_t k = par.slot0 + morton<D>(x, y, z);
                     occ_nb += bin_start[k + 1] - bin_start[k];
                 }
         const double V = vol[e];
@@ -476,7 +479,7 @@ __global__ void k_kb_features(const uint32_t* __restrict__ qs, const uint32_t* _
         f[1] = log2f(1.0f + (float)occ) * 0.25f;
         f[2] = log2f(1.0f + (float)occ_nb) * 0.125f;
         f[3] = (Vp > 0.0f && V > 0.0) ? 4.0f * fminf(fmaxf((float)((V - (double)Vp) / V), -1.0f), 1.0f) : 0.0f;
-        f[4] = V > 0.0 ? 0.25f * log2f((float)(V * (double)n_hydro)) : -2.0f;
+        f[4] = V > 0.0 ? 0.25f * log2f((float)(V * (double)par.count)) : -2.0f;
         f[5] = miss[e] ? 1.0f : 0.0f;
         miss[e] = 0;
         if (V > 0.0) {
@@ -586,12 +589,14 @@ cudaError_t kb_features(pgpu_ctx* c) {
     if (c->prm.dim == 2)
         k_kb_features<2><<<nblk(nq, 256), 256, 0, c->stream>>>(
             (const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p, (const double2*)c->spts.p,
-            (const uint32_t*)c->bin_start.p, c->grid_G, nq, nh, (const int*)c->certk.p, (const double*)c->vol.p,
+            (const uint32_t*)c->bin_start.p, (const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
+            nq, nh, (const int*)c->certk.p, (const double*)c->vol.p,
             (const uint32_t*)c->fcnt.p, (const double*)c->centroid.p, (const double*)c->pos.p, hv, ms, feat);
     else
         k_kb_features<3><<<nblk(nq, 256), 256, 0, c->stream>>>(
             (const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p, (const double4*)c->spts.p,
-            (const uint32_t*)c->bin_start.p, c->grid_G, nq, nh, (const int*)c->certk.p, (const double*)c->vol.p,
+            (const uint32_t*)c->bin_start.p, (const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
+            nq, nh, (const int*)c->certk.p, (const double*)c->vol.p,
             (const uint32_t*)c->fcnt.p, (const double*)c->centroid.p, (const double*)c->pos.p, hv, ms, feat);
     count_launches(1);
     return cudaGetLastError();

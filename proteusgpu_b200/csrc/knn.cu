@@ -224,10 +224,10 @@ __device__ __forceinline__ double box_d2(const double* pc, int x, int y, int z, 
 // sub-bin S, which is scanned whole, once: from the box of S nearest the query
 // (the query's box clamped into S), whose box distance is S's own.
 template <int D>
-__device__ __forceinline__ bool box_range(const SubGrid& g, int Lq, int x, int y, int z, const int (&qb)[3],
-                                          uint32_t& start, uint32_t& cnt) {
+__device__ __forceinline__ bool box_range(const SubGrid& g, uint32_t slot0, int Lq, int x, int y, int z,
+                                          const int (&qb)[3], uint32_t& start, uint32_t& cnt) {
     const int cx = x >> Lq, cy = y >> Lq, cz = z >> Lq;
-    const uint32_t m = morton<D>(cx, cy, cz);
+    const uint32_t m = slot0 + morton<D>(cx, cy, cz);
     const int Lb = g.lvl[m];
     const uint32_t base = g.sub_off[m];
     uint32_t a, b;
@@ -280,9 +280,12 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
         return;
     }
     const double pc[3] = {p.x, p.y, pz(p)};
-    // the query searches at its own bin's level: boxes of side 1 / (G << Lq)
-    const int G0 = grid.G;
-    const int Lq = grid.lvl[morton<D>(bin_coord(p.x, G0), bin_coord(p.y, G0), D == 3 ? bin_coord(pz(p), G0) : 0)];
+    // the query searches its own instance's grid at its own bin's level: boxes of side 1 / (G << Lq)
+    const InstPar& ipq = grid.ip[grid.inst[qid]];
+    const int G0 = ipq.G;
+    const uint32_t slot0 = ipq.slot0;
+    const int Lq =
+        grid.lvl[slot0 + morton<D>(bin_coord(p.x, G0), bin_coord(p.y, G0), D == 3 ? bin_coord(pz(p), G0) : 0)];
     const int G = G0 << Lq;
     const int bc[3] = {sub_coord(p.x, G0, Lq), sub_coord(p.y, G0, Lq), D == 3 ? sub_coord(pz(p), G0, Lq) : 0};
     const double h = 1.0 / (double)G;
@@ -308,7 +311,7 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
             const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
             bool ok = x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G));
             if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
-            if (ok && !box_range<D>(grid, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
+            if (ok && !box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
         }
         scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, w, lane, nrows, K, qn, thr_d, thr_i, ncand);
         // the bound is tested at chunk boundaries: merge what is queued
@@ -347,7 +350,7 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
                 const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
                 bool ok = cheb == r && x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G));
                 if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
-                if (ok && !box_range<D>(grid, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
+                if (ok && !box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
             }
             scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, w, lane, nrows, K, qn, thr_d, thr_i, ncand);
         }
@@ -405,8 +408,9 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
     DevScalars* sc = (DevScalars*)c->scalars.p;
     const unsigned blocks = (unsigned)((nq + KNN_WARPS - 1) / KNN_WARPS);
     const uint32_t* perm = (const uint32_t*)c->perm.p;
-    const SubGrid grid = {c->grid_G, (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
-                       (const uint32_t*)c->sub_start.p};
+    const SubGrid grid = {(const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
+                          (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
+                          (const uint32_t*)c->sub_start.p};
     const int2* tab = (const int2*)c->knn_table.p;
     if (c->prm.dim == 2)
         k_knn<2><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double2*)c->spts.p, perm, grid, tab,

@@ -44,9 +44,11 @@ __device__ __forceinline__ bool in_region(const double* p, int r, double buff) {
 }
 
 template <int D>
-__global__ void k_ghost_count(const double* __restrict__ pos, int64_t n, double buff, uint32_t* __restrict__ cnt) {
+__global__ void k_ghost_count(const double* __restrict__ pos, int64_t n, const uint16_t* __restrict__ inst,
+                              const InstPar* __restrict__ ip, uint32_t* __restrict__ cnt) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const double buff = ip[inst[i]].buff;
     double p[D];
 #pragma unroll
     for (int a = 0; a < D; a++) p[a] = pos[i * D + a];
@@ -57,15 +59,20 @@ __global__ void k_ghost_count(const double* __restrict__ pos, int64_t n, double 
 }
 
 template <int D>
-__global__ void k_ghost_write(const double* __restrict__ pos, int64_t n, double buff, double scale, int mirror,
-                              int no_ghosts, const uint32_t* __restrict__ goff,
+__global__ void k_ghost_write(const double* __restrict__ pos, int64_t n, const uint16_t* __restrict__ inst,
+                              const InstPar* __restrict__ ip, int no_ghosts, const uint32_t* __restrict__ goff,
                               typename PointOf<D>::type* __restrict__ ext, uint32_t* __restrict__ gsrc,
-                              uint32_t* __restrict__ gcode) {
+                              uint32_t* __restrict__ gcode, uint16_t* __restrict__ inst_e) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const uint16_t b = inst[i];
+    const InstPar par = ip[b];
+    const double buff = par.buff, scale = par.scale_in;
+    const int mirror = par.mirror;
     double p[D];
 #pragma unroll
     for (int a = 0; a < D; a++) p[a] = pos[i * D + a];
+    inst_e[i] = b;
     if (no_ghosts) {  // compute_mesh: points are used as given
         ext[i] = make_pt<D>(p[0], p[1], D == 3 ? p[D - 1] : 0.0);
         return;
@@ -94,6 +101,7 @@ __global__ void k_ghost_write(const double* __restrict__ pos, int64_t n, double 
 #pragma unroll
         for (int a = 0; a < D; a++) g[a] = scale * (g[a] - 0.5) + 0.5;
         ext[n + k] = make_pt<D>(g[0], g[1], g[2]);
+        inst_e[n + k] = b;
         gsrc[k] = (uint32_t)i;
         gcode[k] = code;
         k++;
@@ -101,12 +109,15 @@ __global__ void k_ghost_write(const double* __restrict__ pos, int64_t n, double 
 }
 
 template <int D>
-__global__ void k_bin_count(const typename PointOf<D>::type* __restrict__ ext, int64_t n, int G,
+__global__ void k_bin_count(const typename PointOf<D>::type* __restrict__ ext, int64_t n,
+                            const uint16_t* __restrict__ inst_e, const InstPar* __restrict__ ip,
                             uint32_t* __restrict__ key, uint32_t* __restrict__ cnt) {
     int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
     typename PointOf<D>::type p = ext[e];
-    uint32_t k = morton<D>(bin_coord(p.x, G), bin_coord(p.y, G), D == 3 ? bin_coord(pz(p), G) : 0);
+    const InstPar& par = ip[inst_e[e]];
+    const int G = par.G;
+    uint32_t k = par.slot0 + morton<D>(bin_coord(p.x, G), bin_coord(p.y, G), D == 3 ? bin_coord(pz(p), G) : 0);
     key[e] = k;
     atomicAdd(&cnt[k], 1u);
 }
@@ -128,12 +139,14 @@ __global__ void k_bin_levels(const uint32_t* __restrict__ cnt, int64_t M, uint8_
 
 // Sub-bin slot of every point (overwrites its coarse key) and the slot counts.
 template <int D>
-__global__ void k_sub_count(const typename PointOf<D>::type* __restrict__ ext, int64_t n, int G,
+__global__ void k_sub_count(const typename PointOf<D>::type* __restrict__ ext, int64_t n,
+                            const uint16_t* __restrict__ inst_e, const InstPar* __restrict__ ip,
                             const uint8_t* __restrict__ lvl, const uint32_t* __restrict__ sub_off,
                             uint32_t* __restrict__ key, uint32_t* __restrict__ sub_cnt) {
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= n) return;
     const typename PointOf<D>::type p = ext[e];
+    const int G = ip[inst_e[e]].G;
     const uint32_t b = key[e];
     const int L = lvl[b];
     uint32_t slot = sub_off[b];
@@ -214,51 +227,147 @@ __global__ void k_iota(uint32_t* __restrict__ q, int64_t n) {
 
 inline unsigned nblk(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
+__global__ void k_fill_inst(uint16_t* __restrict__ inst, const int64_t* __restrict__ hydro0, int nb, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int lo = 0, hi = nb - 1;  // last instance whose first hydro id is <= i
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (hydro0[mid] <= i) lo = mid; else hi = mid - 1;
+    }
+    inst[i] = (uint16_t)lo;
+}
+
+__global__ void k_gather_u32(const uint32_t* __restrict__ src, const int64_t* __restrict__ idx, int n,
+                             uint32_t* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = src[idx[i]];
+}
+
 }  // namespace
+
+static cudaError_t upload_par(pgpu_ctx* c) {
+    Instances& I = c->inst;
+    cudaError_t e = cudaSuccess;
+    InstPar* d = ensure<InstPar>(I.d_par, I.n, &e);
+    if (e) return e;
+    return cudaMemcpyAsync(d, I.par.data(), I.n * sizeof(InstPar), cudaMemcpyHostToDevice, c->stream);
+}
+
+static cudaError_t setup_instances(pgpu_ctx* c, int nb, const int64_t* counts, const double* buff,
+                                   const double* gamma, const int* mirror) {
+    Instances& I = c->inst;
+    I.n = nb;
+    I.count.assign(counts, counts + nb);
+    I.hydro0.assign(nb + 1, 0);
+    for (int b = 0; b < nb; b++) I.hydro0[b + 1] = I.hydro0[b] + counts[b];
+    I.par.assign(nb, InstPar{});
+    for (int b = 0; b < nb; b++) {
+        InstPar& q = I.par[b];
+        q.buff = buff[b];
+        q.scale_in = 1. / (1. + (2 * buff[b]));
+        q.scale_out = 1. + (2 * buff[b]);
+        q.gamma = gamma[b];
+        q.mirror = mirror[b];
+        q.count = (uint32_t)counts[b];
+    }
+    const int64_t n = I.hydro0[nb];
+    cudaError_t e = cudaSuccess;
+    uint16_t* ih = ensure<uint16_t>(I.d_inst_h, n + 1, &e);
+    ensure<unsigned long long>(I.d_dt, nb + 1, &e);
+    if (e) return e;
+    if (nb == 1) {
+        if ((e = cudaMemsetAsync(ih, 0, (n + 1) * sizeof(uint16_t), c->stream))) return e;
+    } else if (n > 0) {
+        int64_t* h0 = ensure<int64_t>(I.d_gather, nb + 1, &e);
+        if (e) return e;
+        if ((e = cudaMemcpyAsync(h0, I.hydro0.data(), (nb + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c->stream)))
+            return e;
+        k_fill_inst<<<nblk(n, 256), 256, 0, c->stream>>>(ih, h0, nb, n);
+        count_launches(1);
+        if ((e = cudaStreamSynchronize(c->stream))) return e;  // d_gather is reused below
+    }
+    return upload_par(c);
+}
+
+cudaError_t set_single_instance(pgpu_ctx* c, int64_t n) {
+    const int mir = c->prm.boundary == PGPU_REFLECTIVE;
+    return setup_instances(c, 1, &n, &c->prm.buff, &c->prm.gamma, &mir);
+}
+
+cudaError_t set_instances(pgpu_ctx* c, int nb, const int64_t* counts, const double* buff, const double* gamma,
+                          const int* boundary) {
+    std::vector<int> mir(nb);
+    for (int b = 0; b < nb; b++) mir[b] = boundary[b] == PGPU_REFLECTIVE;
+    return setup_instances(c, nb, counts, buff, gamma, mir.data());
+}
 
 cudaError_t launch_ghosts(pgpu_ctx* c, const double* pos_dev, int64_t n, bool no_ghosts) {
     const int D = c->prm.dim;
     cudaError_t e = cudaSuccess;
-    const double buff = c->prm.buff;
-    const double scale = 1. / (1. + (2 * buff));
+    Instances& I = c->inst;
+    if (I.hydro0.empty() || I.hydro0[I.n] != n) return cudaErrorInvalidValue;  // instances not set for n points
+    const InstPar* ip = (const InstPar*)I.d_par.p;
+    const uint16_t* ih = (const uint16_t*)I.d_inst_h.p;
     int64_t ng = 0;
+    std::vector<int64_t> ext_count(I.count);
     if (!no_ghosts) {
         uint32_t* cnt = ensure<uint32_t>(c->gcnt, n + 1, &e);
         uint32_t* off = ensure<uint32_t>(c->goff, n + 1, &e);
         if (e) return e;
         if (n > 0) {
             if (D == 2)
-                k_ghost_count<2><<<nblk(n, 256), 256, 0, c->stream>>>(pos_dev, n, buff, cnt);
+                k_ghost_count<2><<<nblk(n, 256), 256, 0, c->stream>>>(pos_dev, n, ih, ip, cnt);
             else
-                k_ghost_count<3><<<nblk(n, 256), 256, 0, c->stream>>>(pos_dev, n, buff, cnt);
+                k_ghost_count<3><<<nblk(n, 256), 256, 0, c->stream>>>(pos_dev, n, ih, ip, cnt);
         }
         if (n > 0) count_launches(1);
         if ((e = exclusive_scan_u32(cnt, off, n, c->scan_tmp, c->stream))) return e;
-        uint32_t total = 0;
-        if ((e = cudaMemcpyAsync(&total, off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream))) return e;
+        // ghost offsets at every instance's first point (the last entry is the total)
+        std::vector<uint32_t> at(I.n + 1, 0);
+        if (I.n == 1) {
+            if ((e = cudaMemcpyAsync(&at[1], off + n, sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream))) return e;
+        } else {
+            int64_t* idx = ensure<int64_t>(I.d_gather, 2 * (I.n + 1) + 2, &e);
+            if (e) return e;
+            uint32_t* outv = (uint32_t*)(idx + I.n + 1);
+            if ((e = cudaMemcpyAsync(idx, I.hydro0.data(), (I.n + 1) * sizeof(int64_t), cudaMemcpyHostToDevice,
+                                     c->stream)))
+                return e;
+            k_gather_u32<<<nblk(I.n + 1, 256), 256, 0, c->stream>>>(off, idx, I.n + 1, outv);
+            count_launches(1);
+            if ((e = cudaMemcpyAsync(at.data(), outv, (I.n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost,
+                                     c->stream)))
+                return e;
+        }
         if ((e = cudaStreamSynchronize(c->stream))) return e;
-        ng = total;
+        ng = at[I.n];
+        for (int b = 0; b < I.n; b++) ext_count[b] += (int64_t)at[b + 1] - (int64_t)at[b];
     }
     c->n_hydro = n;
     c->n_ext = n + ng;
+    I.ext_count = ext_count;
     const size_t pt_bytes = D == 2 ? 16 : 32;
     if ((e = ensure_bytes(c->ext, (size_t)(c->n_ext + 1) * pt_bytes))) return e;
     ensure<uint32_t>(c->ghost_src, ng + 1, &e);
     ensure<uint32_t>(c->ghost_code, ng + 1, &e);
+    uint16_t* ie = ensure<uint16_t>(I.d_inst_e, c->n_ext + 1, &e);
     if (e) return e;
     if (n > 0) {
         const uint32_t* off = (const uint32_t*)c->goff.p;
         if (D == 2)
-            k_ghost_write<2><<<nblk(n, 256), 256, 0, c->stream>>>(
-                pos_dev, n, buff, scale, c->prm.boundary == PGPU_REFLECTIVE, no_ghosts, off, (double2*)c->ext.p,
-                (uint32_t*)c->ghost_src.p, (uint32_t*)c->ghost_code.p);
+            k_ghost_write<2><<<nblk(n, 256), 256, 0, c->stream>>>(pos_dev, n, ih, ip, no_ghosts, off,
+                                                                  (double2*)c->ext.p, (uint32_t*)c->ghost_src.p,
+                                                                  (uint32_t*)c->ghost_code.p, ie);
         else
-            k_ghost_write<3><<<nblk(n, 256), 256, 0, c->stream>>>(
-                pos_dev, n, buff, scale, c->prm.boundary == PGPU_REFLECTIVE, no_ghosts, off, (double4*)c->ext.p,
-                (uint32_t*)c->ghost_src.p, (uint32_t*)c->ghost_code.p);
+            k_ghost_write<3><<<nblk(n, 256), 256, 0, c->stream>>>(pos_dev, n, ih, ip, no_ghosts, off,
+                                                                  (double4*)c->ext.p, (uint32_t*)c->ghost_src.p,
+                                                                  (uint32_t*)c->ghost_code.p, ie);
     }
     if (n > 0) count_launches(1);
-    c->unit_scale = no_ghosts ? 1.0 : 1. + (2 * buff);
+    if (no_ghosts)
+        for (auto& q : I.par) q.scale_out = 1.0;  // compute_mesh: no unit-box scaling
+    c->unit_scale = I.par[0].scale_out;
     return cudaGetLastError();
 }
 
@@ -279,11 +388,22 @@ cudaError_t launch_grid_sort(pgpu_ctx* c) {
     const int D = c->prm.dim;
     const int64_t n = c->n_ext;
     cudaError_t e = cudaSuccess;
-    int G = grid_resolution(n, D);
-    int64_t P = 1;
-    while (P < G) P <<= 1;
-    int64_t M = D == 2 ? P * P : P * P * P;
-    c->grid_G = G;
+    // one grid per instance, sized by its own point count; their Morton slots follow each other
+    Instances& I = c->inst;
+    int64_t M = 0;
+    for (int b = 0; b < I.n; b++) {
+        const int Gb = grid_resolution(I.ext_count[b], D);
+        int64_t P = 1;
+        while (P < Gb) P <<= 1;
+        I.par[b].G = Gb;
+        I.par[b].slot0 = (uint32_t)M;
+        M += D == 2 ? P * P : P * P * P;
+    }
+    if (M >= (1ll << 32)) return cudaErrorInvalidValue;
+    if ((e = upload_par(c))) return e;
+    const InstPar* ip = (const InstPar*)I.d_par.p;
+    const uint16_t* ie = (const uint16_t*)I.d_inst_e.p;
+    c->grid_G = I.par[0].G;
     c->morton_slots = M;
     uint32_t* cnt = ensure<uint32_t>(c->bin_cnt, M + 1, &e);
     uint32_t* start = ensure<uint32_t>(c->bin_start, M + 1, &e);
@@ -298,9 +418,9 @@ cudaError_t launch_grid_sort(pgpu_ctx* c) {
     if ((e = cudaMemsetAsync(cnt, 0, (M + 1) * sizeof(uint32_t), c->stream))) return e;
     if (n > 0) {
         if (D == 2)
-            k_bin_count<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, G, key, cnt);
+            k_bin_count<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, ie, ip, key, cnt);
         else
-            k_bin_count<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, G, key, cnt);
+            k_bin_count<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, ie, ip, key, cnt);
         count_launches(1);
     }
     // levels, sub-table offsets (one slot per coarse bin at level 0)
@@ -320,9 +440,11 @@ cudaError_t launch_grid_sort(pgpu_ctx* c) {
     if ((e = cudaMemsetAsync(scnt, 0, ((size_t)T + 1) * sizeof(uint32_t), c->stream))) return e;
     if (n > 0) {
         if (D == 2)
-            k_sub_count<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, G, lvl, soff, key, scnt);
+            k_sub_count<2><<<nblk(n, 256), 256, 0, c->stream>>>((const double2*)c->ext.p, n, ie, ip, lvl, soff, key,
+                                                                scnt);
         else
-            k_sub_count<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, G, lvl, soff, key, scnt);
+            k_sub_count<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, ie, ip, lvl, soff, key,
+                                                                scnt);
         count_launches(1);
     }
     if ((e = exclusive_scan_u32(scnt, sstart, T, c->scan_tmp, c->stream))) return e;

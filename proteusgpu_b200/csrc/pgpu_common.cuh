@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "pgpu_ctx.h"
+
 namespace pgpu {
 
 constexpr int MAX_P = 64;   // clipping planes per cell (reference _MAX_P_, Config.sh:37)
@@ -104,10 +106,11 @@ __device__ __forceinline__ int bin_coord(double x, int G) {
 constexpr int SUB_SPLIT = 16;
 constexpr int SUB_FILL = 4;
 constexpr int SUB_LMAX = 5;
-// The grid as the search kernels see it: coarse Morton bins, dense ones split
-// into Morton-ordered sub-bins.
+// The grid as the search kernels see it: per instance, coarse Morton bins, dense
+// ones split into Morton-ordered sub-bins.
 struct SubGrid {
-    int G;                      // coarse bins per axis
+    const InstPar* ip;          // per instance: G, first slot
+    const uint16_t* inst;       // instance of each extended id
     const uint8_t* lvl;         // refinement level per coarse bin
     const uint32_t* sub_off;    // first sub-bin slot per coarse bin
     const uint32_t* sub_start;  // first sorted point per sub-bin slot (one past the last: n)

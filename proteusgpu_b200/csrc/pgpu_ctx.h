@@ -6,10 +6,27 @@
 
 #include <string>
 #include <utility>
+#include <vector>
 
 #include "../../include/proteus_gpu.h"
 
 namespace pgpu {
+
+// Per-simulation parameters.  A context advances one simulation, or a batch of
+// independent ones whose points are concatenated (hydro points of every
+// instance first, then every instance's ghosts); each instance keeps its own
+// unit box, ghost layer, grid, gamma, boundary and time step, so that its
+// results are those of a run on its own.
+struct InstPar {
+    double buff;       // ghost layer width
+    double scale_in;   // 1 / (1 + 2 buff): physical -> unit box
+    double scale_out;  // 1 + 2 buff: unit box -> physical
+    double gamma;
+    int mirror;        // reflective walls
+    int G;             // coarse grid bins per axis
+    uint32_t slot0;    // first coarse Morton slot of this instance's grid
+    uint32_t count;    // hydro points
+};
 
 // A device allocation that only grows.  Contents are not preserved on growth.
 struct DevBuf {
@@ -55,6 +72,21 @@ constexpr int KB_PART = 1544;  // per-warp partial gradient row (parameters, los
 // BF16 operand copies (u16): W1[32][8], W2[32][32], W2^T, W3[8][32] (rows 6-7 zero), W3^T[32][8]
 constexpr int KB_BW1 = 0, KB_BW2 = 256, KB_BW2T = 1280, KB_BW3 = 2304, KB_BW3T = 2560, KB_NBF = 2816;
 constexpr int KB_GRAD_BLOCKS = 148, KB_GRAD_WARPS = 4;
+
+// The simulations a context advances (one unless pgpu_batch_init made a batch).
+struct Instances {
+    int n = 1;
+    std::vector<int64_t> count;      // hydro points per instance
+    std::vector<int64_t> hydro0;     // first hydro id (n + 1 entries)
+    std::vector<int64_t> ext_count;  // hydro + ghost points per instance (last mesh)
+    std::vector<InstPar> par;        // host copy of the parameters
+    DevBuf d_par;                    // InstPar[n]
+    DevBuf d_inst_h;                 // u16 per hydro id
+    DevBuf d_inst_e;                 // u16 per extended id
+    DevBuf d_dt;                     // u64 dt bits per instance
+    std::vector<unsigned long long> dt_init;  // staging for their reset
+    DevBuf d_gather;                 // u32 scratch for per-instance ghost totals
+};
 
 struct KBudget {
     bool enabled = false;
@@ -128,6 +160,7 @@ struct pgpu_ctx {
     int64_t n_pruned = 0;       // cells certified by the grid walk in the last step
     pgpu::DevBuf fb_qs, fb_knn; // fallback query list and lists
     pgpu::KBudget kb;           // learned neighbour budget (optional form)
+    pgpu::Instances inst;       // the simulation(s) of this context
 };
 
 namespace pgpu {
@@ -139,6 +172,11 @@ void count_launches(int n);
 // scan.cu
 cudaError_t exclusive_scan_u32(const uint32_t* in, uint32_t* out, int64_t n, DevBuf& tmp, cudaStream_t s);
 // mesh_prep.cu
+// one instance from the context's parameters, n hydro points
+cudaError_t set_single_instance(pgpu_ctx* c, int64_t n);
+// a batch: counts[b] points per instance, with their own buff, gamma and boundary
+cudaError_t set_instances(pgpu_ctx* c, int nb, const int64_t* counts, const double* buff, const double* gamma,
+                          const int* boundary);
 cudaError_t launch_ghosts(pgpu_ctx* c, const double* pos_dev, int64_t n, bool scale_only);
 cudaError_t launch_grid_sort(pgpu_ctx* c);
 cudaError_t launch_query_list(pgpu_ctx* c, bool all_cells);
