@@ -45,6 +45,10 @@ CONFIGS = {
     "sedov3d_1m": dict(dim=3, n=1_048_576, seed=2, k=190, buff=0.04, boundary="periodic", cfl=0.3),
     "sedov3d_256k": dict(dim=3, n=262_144, seed=2, k=190, buff=0.04 * 4 ** (1 / 3), boundary="periodic", cfl=0.3),
     "sod2d_10k": dict(dim=2, n=10_000, seed=1, k=16, buff=0.04, boundary="reflective", cfl=0.3),
+    # 256 independent 2D simulations (Sod with walls / Sedov / Kelvin-Helmholtz, gamma 1.4 or 5/3),
+    # point counts log-uniform in [1e3, 2e5], advanced together
+    "batched2d_256": dict(dim=2, n=None, seed=5, k=32, buff=None, boundary="mixed", cfl=0.3, batch=True,
+                          n_inst=256),
 }
 
 # Algorithmic work per unit ("Roofline"): counted with the oracle's
@@ -77,6 +81,8 @@ def parse():
 
 def make_ic(cfg):
     from proteusgpu_b200 import ics
+    if cfg.get("batch"):
+        return ics.batch_2d(cfg["n_inst"], cfg["seed"])
     if cfg.get("ic") == "clustered":
         return ics.clustered_3d(n=cfg["n"], seed=cfg["seed"])
     if cfg["dim"] == 3:
@@ -149,46 +155,64 @@ class ClockSampler:
 # ---------------------------------------------------------------- CPU reference
 def cpu_reference_step_rate(steps: int, cfg: dict, n_sample: int = 20000, nthreads: int | None = None):
     """Cell-updates/s of the reference's own CPU code (oracle/_ref, compiled from its sources) on a
-    bounded sample of the workload (same distribution, n_sample points): per step compute_periodic_mesh
-    (KNN + clipping + extraction) + dt_CFL + hydro_step; the ghost layer is widened so that it spans
-    the same number of (mean) cells as the workload's buff does at its full size, at most 0.15.  Falls
-    back to the C restatement (oracle/liboracle.so) if _ref is absent."""
+    bounded sample of the workload: per step and simulation compute_periodic_mesh (KNN + clipping +
+    extraction) + dt_CFL + hydro_step.  3D: n_sample points of the same distribution, the ghost layer
+    widened so that it spans the same number of mean cells as the workload's buff does at its full
+    size (at most 0.15).  Batches: the first instances of the batch up to n_sample points in all, each
+    with its own buff and gamma (the reference knows periodic boxes only, so walled instances run
+    periodic).  Falls back to the C restatement (oracle/liboracle.so) if _ref is absent."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from proteusgpu_b200 import ics
     nthreads = nthreads or os.cpu_count() or 1
-    clustered = cfg.get("ic") == "clustered"
-    ic = ics.clustered_3d(n=n_sample, seed=cfg["seed"]) if clustered else ics.sedov_3d(n=n_sample, seed=2)
-    buff = min(cfg["buff"] * (cfg["n"] / n_sample) ** (1 / 3), 0.15)
+    dim, K = cfg["dim"], cfg["k"]
+    if cfg.get("batch"):
+        B = ics.batch_2d(cfg["n_inst"], cfg["seed"])
+        items, tot = [], 0
+        for ic, bf in zip(B.instances, B.buff):
+            if tot >= n_sample:
+                break
+            items.append((ic, float(bf)))
+            tot += ic.n
+        desc = f"first {len(items)} instances of the batch ({tot} 2D points, periodic), K={K}"
+    else:
+        clustered = cfg.get("ic") == "clustered"
+        ic = ics.clustered_3d(n=n_sample, seed=cfg["seed"]) if clustered else ics.sedov_3d(n=n_sample, seed=2)
+        buff = min(cfg["buff"] * (cfg["n"] / n_sample) ** (1 / 3), 0.15)
+        items, tot = [(ic, buff)], n_sample
+        desc = (f"3D Sedov, {n_sample} {'clustered' if clustered else 'uniform'} points, K={K}, "
+                f"buff {buff:.3f}")
     kind = "reference"
     try:
         import refbuild as rb
-        rb.load(3, 190)
+        rb.load(dim, K)
     except (FileNotFoundError, OSError):
         kind = "port"
+    state = [(ic.pos.copy(), ic.rho.copy(), ic.vel.copy(), ic.energy.copy()) for ic, _ in items]
     times = []
-    x = ic.pos.copy()
-    rho, vel, E = ic.rho.copy(), ic.vel.copy(), ic.energy.copy()
     for s in range(steps):
         t0 = time.perf_counter()
-        if kind == "reference":
-            m = rb.periodic_mesh(x, 190, buff=buff, gamma=ic.gamma, keep_handle=True, nthreads=nthreads)
-            if s == 0:
-                E = E + ic.deposit / np.where(m.volumes[:n_sample] > 0, m.volumes[:n_sample], 1.0)
-            dt = rb.dt_cfl(3, 190, m.handle, 0.3, rho, vel, E, ic.gamma)
-            rho, vel, E = rb.hydro_step(3, 190, m.handle, dt, rho, vel, E, ic.gamma)
-            rb.free_handle(3, 190, m.handle)
-        else:
-            import oracle as om
-            m = om.build_mesh(x, 190, buff=buff)
-            if s == 0:
-                E = E + ic.deposit / np.where(m.volumes[:n_sample] > 0, m.volumes[:n_sample], 1.0)
-            dt = om.dt_cfl(m, 0.3, ic.gamma, rho, vel, E)
-            rho, vel, E, _ = om.hydro_step_ref(m, dt, ic.gamma, rho, vel, E)
+        for j, (ic, buff) in enumerate(items):
+            x, rho, vel, E = state[j]
+            n = ic.n
+            if kind == "reference":
+                m = rb.periodic_mesh(x, K, buff=buff, gamma=ic.gamma, keep_handle=True, nthreads=nthreads)
+                if s == 0 and ic.deposit is not None:
+                    E = E + ic.deposit / np.where(m.volumes[:n] > 0, m.volumes[:n], 1.0)
+                dt = rb.dt_cfl(dim, K, m.handle, 0.3, rho, vel, E, ic.gamma)
+                rho, vel, E = rb.hydro_step(dim, K, m.handle, dt, rho, vel, E, ic.gamma)
+                rb.free_handle(dim, K, m.handle)
+            else:
+                import oracle as om
+                m = om.build_mesh(x, K, buff=buff)
+                if s == 0 and ic.deposit is not None:
+                    E = E + ic.deposit / np.where(m.volumes[:n] > 0, m.volumes[:n], 1.0)
+                dt = om.dt_cfl(m, 0.3, ic.gamma, rho, vel, E)
+                rho, vel, E, _ = om.hydro_step_ref(m, dt, ic.gamma, rho, vel, E)
+            state[j] = (x, rho, vel, E)
         times.append(time.perf_counter() - t0)
     t = float(np.mean(times))
-    sample = (f"3D Sedov, {n_sample} {'clustered' if clustered else 'uniform'} points, K=190, buff {buff:.3f}, "
-              f"{steps} step(s) of compute_periodic_mesh + dt_CFL + hydro_step")
-    return n_sample / t, kind, nthreads, sample, t
+    sample = f"{desc}, {steps} step(s) of compute_periodic_mesh + dt_CFL + hydro_step"
+    return tot / t, kind, nthreads, sample, t
 
 
 # ---------------------------------------------------------------- our arm
@@ -230,12 +254,19 @@ def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks
     from proteusgpu_b200 import Context, _lib
     L = _lib.load()
     spec = FORMS[form]
-    ctx = Context(dim=cfg["dim"], k=cfg["k"], buff=cfg["buff"], boundary=cfg["boundary"], flux="physical",
-                  gamma=ic.gamma, device=local_rank, precision=spec["precision"])
+    batch = bool(cfg.get("batch"))
+    ctx = Context(dim=cfg["dim"], k=cfg["k"], buff=0.04 if batch else cfg["buff"],
+                  boundary="periodic" if batch else cfg["boundary"], flux="physical",
+                  gamma=1.4 if batch else ic.gamma, device=local_rank, precision=spec["precision"],
+                  predicates="robust" if batch else "reference")
     if spec["kbudget"]:
         # the warm-up steps but the last train the proposal; the last one already uses it
         ctx.kbudget_enable(train_steps=max(1, args.warmup - 1), iters_per_step=256, quantile=0.98, seed=1)
-    ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+    if batch:
+        ctx.batch_init(ic.counts, ic.buff, ic.gamma, ic.boundary, ic.concat("pos"), ic.concat("rho"),
+                       ic.concat("vel"), ic.concat("energy"), ic.concat("deposit"))
+    else:
+        ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
     for _ in range(max(args.warmup, 0)):
         ctx.sim_step(cfg["cfl"], want_dt=False)
     ctx.enable_timing(True)
@@ -349,7 +380,7 @@ def run_ours(args, rank, world, local_rank):
         ach = n_query * W["clip_flop_per_cell"] / (stage[3] * 1e-3) / 1e12
         roof = {"kernel": "k_clip32 (+ FP64 re-clip of undecided cells)", "bound": "fp32", "achieved": ach,
                 "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
-                "traffic": CLIP32_DRAM_BYTES_PER_CELL * n_query,
+                "traffic": CLIP32_DRAM_BYTES_PER_CELL * n_query if D == 3 else None,
                 "traffic_note": "DRAM bytes per launch: ncu capture of the clustered 1,048,576-cell case "
                                 "(K = 190 lists) scaled by cells",
                 "peak_source": "FP32 FMA rate measured in this run (pgpu_fp32_peak)",
@@ -376,14 +407,21 @@ def run_ours(args, rank, world, local_rank):
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
                "s_per_step": t_step}
     dist_name = "clustered (70% in 64 Gaussian clumps)" if cfg.get("ic") == "clustered" else "uniform"
-    wl = (f"{args.config}: 3D Sedov-Taylor blast, {cfg['n']} {dist_name} points (seed {cfg['seed']}), "
-          f"moving mesh, {cfg['boundary']} box" if D == 3 else args.config)
+    if cfg.get("batch"):
+        wl = (f"{args.config}: {cfg['n_inst']} independent 2D simulations (Sod with walls / Sedov / "
+              f"Kelvin-Helmholtz, gamma 1.4 or 5/3, seed {cfg['seed']}), {n} points in all, point counts "
+              "log-uniform in [1e3, 2e5], one launch per stage")
+    elif D == 3:
+        wl = (f"{args.config}: 3D Sedov-Taylor blast, {cfg['n']} {dist_name} points (seed {cfg['seed']}), "
+              f"moving mesh, {cfg['boundary']} box")
+    else:
+        wl = args.config
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": wl, "n_points": cfg["n"], "k": cfg["k"], "buff": cfg["buff"],
+        "config": {"workload": wl, "n_points": n, "k": cfg["k"], "buff": cfg["buff"],
                    "form": "learned-K (BF16 MLP proposal, plain-K fallback) + FP32 local-frame clipping "
                            "(FP64 re-clip, FP64 extraction, hydro and sums)",
                    "baseline_form": f"plain: fixed K={cfg['k']}, FP64 clipping",
