@@ -269,6 +269,8 @@ def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks
         ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
     for _ in range(max(args.warmup, 0)):
         ctx.sim_step(cfg["cfl"], want_dt=False)
+    # launch shapes for this workload, timed on mesh builds of the current state (nothing advances)
+    tuning = ctx.autotune()
     ctx.enable_timing(True)
     ctx.sim_step(cfg["cfl"], want_dt=False)
     stage = ctx.stage_times()
@@ -295,7 +297,7 @@ def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks
     launches = L.pgpu_launch_count() - l0
     kb_after = ctx.kbudget_stats() if spec["kbudget"] else None
     out = {"ms": ms, "stage": stage, "stats": stats, "launches": launches, "clocks": clk.summary(),
-           "kbudget": kb_after or kb}
+           "kbudget": kb_after or kb, "tuning": tuning}
     if want_e2e:
         # end to end: the same step through the C ABI with the state in pinned host
         # memory, copied to the device before and back after every step
@@ -351,7 +353,8 @@ def run_ours(args, rank, world, local_rank):
     for f, r in res.items():
         forms[f] = {"value": rate(r), "ms_per_step": r["ms"] / args.steps,
                     "stages_ms": dict(zip(STAGES, r["stage"])), "reclip_cells": r["stats"]["reclip_cells"],
-                    "speedup_vs_plain": rate(r) / rate(base)}
+                    "speedup_vs_plain": rate(r) / rate(base),
+                    "tuning": {k: r["tuning"][k] for k in ("ppb", "knn_warps", "clip_warps", "ms_default", "ms_tuned")}}
         if r["kbudget"]:
             kb = r["kbudget"]
             forms[f]["learned_k"] = {"mean_k": kb["mean_k"], "plain_k": cfg["k"], "cells": kb["cells"],

@@ -235,6 +235,21 @@ int pgpu_batch_init(pgpu_ctx *ctx, int n_inst, const int64_t *counts, const doub
                     const double *deposit);
 int pgpu_batch_dt(pgpu_ctx *ctx, double *dt_per_instance);
 
+/* -------------------------------------------------------- autotuner ---
+ * Extension.  Times mesh builds of the current simulation state (nothing
+ * advances) and picks the coarse grid's mean points per bin (1.5, 2, 3, 4), the
+ * KNN block size (2, 4, 8 queries) and the clipping block size (2, 4 cells), one
+ * after the other; the choice is cached for the process by (dim, log2 n, batch,
+ * precision, learned K, k) and reused without timing.  Results do not depend on
+ * the launch shapes. */
+typedef struct {
+    double ppb;
+    int32_t knn_warps, clip_warps;
+    float ms_default, ms_tuned;  /* ghosts + sort + KNN + clip of one build, before and after */
+    int32_t from_cache;
+} pgpu_tuning;
+int pgpu_autotune(pgpu_ctx *ctx, pgpu_tuning *out);
+
 /* ------------------------------------------- learned neighbour budget ---
  * Extension (the reference uses one compile-time _K_ for every cell, Config.sh,
  * src/knn/knn.cpp:225-315).  When enabled, every mesh build of a moving-mesh

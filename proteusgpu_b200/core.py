@@ -214,6 +214,13 @@ class Context:
                                                _ptr(rho), _ptr(v), _ptr(E), _ptr(dep)), "pgpu_batch_init")
         self._n_inst = nb
 
+    def autotune(self) -> dict:
+        """Launch shapes for this workload (grid bin size, KNN and clipping block sizes),
+        timed on mesh builds of the current state; cached per workload class."""
+        t = _lib.Tuning()
+        check(self._h, self._L.pgpu_autotune(self._h, C.byref(t)), "pgpu_autotune")
+        return {f: getattr(t, f) for f, _ in t._fields_}
+
     def batch_dt(self) -> np.ndarray:
         """Each instance's dt of the last step."""
         out = np.zeros(getattr(self, "_n_inst", 1))

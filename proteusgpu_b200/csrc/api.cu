@@ -2,6 +2,10 @@
 // of the stage launches, and host transfers.  No computation happens here.
 #include <algorithm>
 #include <atomic>
+#include <cmath>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -786,6 +790,91 @@ int pgpu_mlp_grad(pgpu_ctx* c, const float* feat, const int32_t* labels, int64_t
     if (grad) CK(cudaMemcpyAsync(grad, g, pgpu::KB_NPARAM * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     if (loss) CK(cudaMemcpyAsync(loss, g + pgpu::KB_NPARAM, sizeof(float), cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+// ------------------------------------------------------------------ autotuner
+// Launch shapes per workload class, shared by the contexts of this process.
+using TuneKey = std::tuple<int, int, int, int, int, int>;  // dim, log2 n, batch, precision, learned K, k
+static std::mutex g_tune_mu;
+static std::map<TuneKey, pgpu::Tuning> g_tune_cache;
+
+static TuneKey tune_key(const pgpu_ctx* c) {
+    const int lg = c->n_hydro > 0 ? (int)std::lround(std::log2((double)c->n_hydro)) : 0;
+    return TuneKey(c->prm.dim, lg, c->inst.n > 1, c->prm.precision, c->kb.enabled && c->kb.trained, c->prm.k);
+}
+
+// One mesh build of the current simulation state with stage timing; returns the
+// summed stage times selected by mask (bit i: stage i of ghosts, sort, knn, clip).
+static int timed_build(pgpu_ctx* c, unsigned mask, float* ms) {
+    int r = build_mesh(c, c->n_hydro, false, false);
+    if (r) return r;
+    collect_times(c);
+    float t = 0.0f;
+    for (int i = 0; i < 4; i++)
+        if (mask & (1u << i)) t += c->stage_ms[i];
+    *ms = t;
+    return PGPU_OK;
+}
+
+int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_sim) return fail(c, PGPU_ESTATE, "pgpu_autotune: needs a simulation (pgpu_sim_init or pgpu_batch_init)");
+    const TuneKey key = tune_key(c);
+    pgpu_tuning res{};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            c->tune = it->second;
+            res.from_cache = 1;
+        }
+    }
+    if (!res.from_cache) {
+        const bool timing = c->timing;
+        const bool kb_enabled = c->kb.enabled;
+        if (kb_enabled && !c->kb.trained) c->kb.enabled = false;  // tune without training steps
+        c->timing = true;
+        pgpu::Tuning best = c->tune;
+        float t = 0.0f;
+        if ((r = timed_build(c, 0xF, &t))) return r;
+        res.ms_default = t;
+        // 1. grid bin size: sort + KNN + clip
+        float bt = 1e30f;
+        for (double ppb : {1.5, 2.0, 3.0, 4.0}) {
+            c->tune.ppb = ppb;
+            if ((r = timed_build(c, 0xE, &t))) return r;
+            if (t < bt) bt = t, best.ppb = ppb;
+        }
+        c->tune.ppb = best.ppb;
+        // 2. KNN block size
+        bt = 1e30f;
+        for (int kw : {2, 4, 8}) {
+            c->tune.knn_warps = kw;
+            if ((r = timed_build(c, 0x4, &t))) return r;
+            if (t < bt) bt = t, best.knn_warps = kw;
+        }
+        c->tune.knn_warps = best.knn_warps;
+        // 3. clipping block size
+        bt = 1e30f;
+        for (int cw : {2, 4}) {
+            c->tune.clip_warps = cw;
+            if ((r = timed_build(c, 0x8, &t))) return r;
+            if (t < bt) bt = t, best.clip_warps = cw;
+        }
+        c->tune = best;
+        if ((r = timed_build(c, 0xF, &t))) return r;
+        res.ms_tuned = t;
+        c->timing = timing;
+        c->kb.enabled = kb_enabled;
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        g_tune_cache[key] = best;
+    }
+    res.ppb = c->tune.ppb;
+    res.knn_warps = c->tune.knn_warps;
+    res.clip_warps = c->tune.clip_warps;
+    if (out) *out = res;
     return PGPU_OK;
 }
 

@@ -665,12 +665,12 @@ __device__ __forceinline__ int clip_by(WarpCell& W, int lane, uint32_t z, double
     return CLIP_CUT;
 }
 
-template <int D>
-__global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip(ClipParams P) {
+template <int D, int CW>
+__global__ void __launch_bounds__(CW * 32) k_clip(ClipParams P) {
     using PT = typename PointOf<D>::type;
-    __shared__ WarpCell cells[CLIP_WARPS];
+    __shared__ WarpCell cells[CW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t t = (int64_t)blockIdx.x * CLIP_WARPS + w;
+    const int64_t t = (int64_t)blockIdx.x * CW + w;
     if (t >= P.nq) return;  // warp-uniform
     WarpCell& W = cells[w];
     const PT* spts = (const PT*)P.spts;
@@ -1212,12 +1212,12 @@ __device__ __forceinline__ double4 plane64(int p, int vid, const typename PointO
     return make_double4(dx, dy, dz, -dot / 2.0);
 }
 
-template <int D>
-__global__ void __launch_bounds__(CLIP_WARPS * 32) k_clip32(ClipParams P) {
+template <int D, int CW>
+__global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
     using PT = typename PointOf<D>::type;
-    __shared__ WarpCell cells[CLIP_WARPS];
+    __shared__ WarpCell cells[CW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t t = (int64_t)blockIdx.x * CLIP_WARPS + w;
+    const int64_t t = (int64_t)blockIdx.x * CW + w;
     if (t >= P.nq) return;  // warp-uniform
     WarpCell& W = cells[w];
     float4* hp = W.u.b.hp32;
@@ -1626,6 +1626,8 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     P.face_cap = c->face_cap;
     if (nq > 0) {
         const unsigned blocks = (unsigned)((nq + CLIP_WARPS - 1) / CLIP_WARPS);
+        const int CW = c->tune.clip_warps;  // cells (warps) per block: autotuned, 2 or 4
+        const unsigned blocks_cw = (unsigned)((nq + CW - 1) / CW);
         if (pruned) {
             const SubGrid g = {(const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
                                (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
@@ -1638,15 +1640,21 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
                 k_clip_pruned<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P, g, tab, c->knn_table_n,
                                                                             c->knn_table_r, qs, nq);
         } else if (fp32) {
-            if (D == 2)
-                k_clip32<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
-            else
-                k_clip32<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+            if (D == 2) {
+                if (CW == 2) k_clip32<2, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
+                else k_clip32<2, 4><<<blocks_cw, 128, 0, c->stream>>>(P);
+            } else {
+                if (CW == 2) k_clip32<3, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
+                else k_clip32<3, 4><<<blocks_cw, 128, 0, c->stream>>>(P);
+            }
         } else {
-            if (D == 2)
-                k_clip<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
-            else
-                k_clip<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P);
+            if (D == 2) {
+                if (CW == 2) k_clip<2, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
+                else k_clip<2, 4><<<blocks_cw, 128, 0, c->stream>>>(P);
+            } else {
+                if (CW == 2) k_clip<3, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
+                else k_clip<3, 4><<<blocks_cw, 128, 0, c->stream>>>(P);
+            }
         }
         count_launches(1);
     }

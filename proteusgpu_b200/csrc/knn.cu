@@ -34,7 +34,6 @@
 namespace pgpu {
 namespace {
 
-constexpr int KNN_WARPS = 4;
 constexpr int MAX_ROWS = MAX_K / 32;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int TABLE_R3 = 8;   // offsets with |d|_inf <= 8 in 3D (17^3 entries)
@@ -87,13 +86,15 @@ __device__ __forceinline__ void bitonic_merge32(double& d, uint32_t& id, int lan
     }
 }
 
-struct KnnSmem {
-    double row_d[KNN_WARPS][MAX_ROWS * 32];
-    uint32_t row_i[KNN_WARPS][MAX_ROWS * 32];
-    double q_d[KNN_WARPS][32];
-    uint32_t q_i[KNN_WARPS][32];
-    uint32_t b_start[KNN_WARPS][32];
-    uint32_t b_excl[KNN_WARPS][32];
+// One warp's shared memory: the K best (rows of 32), the survivor queue and the
+// chunk's bin table.
+struct WarpKnn {
+    double row_d[MAX_ROWS * 32];
+    uint32_t row_i[MAX_ROWS * 32];
+    double q_d[32];
+    uint32_t q_i[32];
+    uint32_t b_start[32];
+    uint32_t b_excl[32];
 };
 
 // Merges qn queued keys into the warp's ascending rows (rows of 32 in shared
@@ -132,7 +133,7 @@ __device__ __noinline__ void merge_queue(double* rd, uint32_t* ri, const double*
 template <int D>
 __device__ __forceinline__ void scan_bins(const typename PointOf<D>::type* __restrict__ spts,
                                           const uint32_t* __restrict__ perm, uint32_t bstart, uint32_t bcnt,
-                                          const typename PointOf<D>::type& p, uint32_t qid, KnnSmem& S, int w,
+                                          const typename PointOf<D>::type& p, uint32_t qid, WarpKnn& S,
                                           int lane, int nrows, int K, int& qn, double& thr_d, uint32_t& thr_i,
                                           unsigned long long& ncand) {
     using PT = typename PointOf<D>::type;
@@ -140,8 +141,8 @@ __device__ __forceinline__ void scan_bins(const typename PointOf<D>::type* __res
     const uint32_t total = __shfl_sync(FULL, incl, 31);
     if (total == 0) return;
     __syncwarp();
-    S.b_start[w][lane] = bstart;
-    S.b_excl[w][lane] = incl - bcnt;
+    S.b_start[lane] = bstart;
+    S.b_excl[lane] = incl - bcnt;
     __syncwarp();
     ncand += total;
     for (uint32_t k0 = 0; k0 < total; k0 += 32) {
@@ -153,8 +154,8 @@ __device__ __forceinline__ void scan_bins(const typename PointOf<D>::type* __res
             int j = 0;
 #pragma unroll
             for (int step = 16; step > 0; step >>= 1)
-                if (j + step < 32 && S.b_excl[w][j + step] <= tt) j += step;
-            const uint32_t sidx = S.b_start[w][j] + (tt - S.b_excl[w][j]);
+                if (j + step < 32 && S.b_excl[j + step] <= tt) j += step;
+            const uint32_t sidx = S.b_start[j] + (tt - S.b_excl[j]);
             eid = perm[sidx];
             if (eid == qid) {
                 valid = false;
@@ -175,33 +176,33 @@ __device__ __forceinline__ void scan_bins(const typename PointOf<D>::type* __res
         if (bal == 0) continue;
         if (qn + __popc(bal) > 32) {
             __syncwarp();
-            merge_queue(S.row_d[w], S.row_i[w], S.q_d[w], S.q_i[w], qn, nrows, lane);
+            merge_queue(S.row_d, S.row_i, S.q_d, S.q_i, qn, nrows, lane);
             qn = 0;
             __syncwarp();
-            thr_d = S.row_d[w][K - 1];
-            thr_i = S.row_i[w][K - 1];
+            thr_d = S.row_d[K - 1];
+            thr_i = S.row_i[K - 1];
             surv = surv && key_less(d2, eid, thr_d, thr_i);
             bal = __ballot_sync(FULL, surv);
         }
         if (surv) {
             const int pos = qn + __popc(bal & ((1u << lane) - 1u));
-            S.q_d[w][pos] = d2;
-            S.q_i[w][pos] = eid;
+            S.q_d[pos] = d2;
+            S.q_i[pos] = eid;
         }
         qn += __popc(bal);
         __syncwarp();
     }
 }
 
-__device__ __forceinline__ void flush_queue(KnnSmem& S, int w, int lane, int nrows, int K, int& qn, double& thr_d,
+__device__ __forceinline__ void flush_queue(WarpKnn& S, int lane, int nrows, int K, int& qn, double& thr_d,
                                             uint32_t& thr_i) {
     if (qn == 0) return;
     __syncwarp();
-    merge_queue(S.row_d[w], S.row_i[w], S.q_d[w], S.q_i[w], qn, nrows, lane);
+    merge_queue(S.row_d, S.row_i, S.q_d, S.q_i, qn, nrows, lane);
     qn = 0;
     __syncwarp();
-    thr_d = S.row_d[w][K - 1];
-    thr_i = S.row_i[w][K - 1];
+    thr_d = S.row_d[K - 1];
+    thr_i = S.row_i[K - 1];
 }
 
 // Squared distance from p to the box of bin (x, y, z).
@@ -254,22 +255,23 @@ __device__ __forceinline__ bool box_range(const SubGrid& g, uint32_t slot0, int 
     return true;
 }
 
-template <int D>
-__global__ void __launch_bounds__(KNN_WARPS * 32)
+template <int D, int KW>
+__global__ void __launch_bounds__(KW * 32)
     k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
           const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
           int K, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
           unsigned long long* __restrict__ cand_counter) {
-    __shared__ KnnSmem S;
+    __shared__ WarpKnn S_all[KW];
     using PT = typename PointOf<D>::type;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t t = (int64_t)blockIdx.x * KNN_WARPS + w;
+    const int64_t t = (int64_t)blockIdx.x * KW + w;
     if (t >= nq) return;  // warp-uniform
+    WarpKnn& S = S_all[w];
     if (kq) K = kq[t];
     const int nrows = (K + 31) >> 5;
     for (int r = 0; r < nrows; r++) {
-        S.row_d[w][r * 32 + lane] = CUDART_INF;
-        S.row_i[w][r * 32 + lane] = NO_NEIGHBOR;
+        S.row_d[r * 32 + lane] = CUDART_INF;
+        S.row_i[r * 32 + lane] = NO_NEIGHBOR;
     }
     __syncwarp();
     const uint32_t s = qs[t];
@@ -313,9 +315,9 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
             if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
             if (ok && !box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
         }
-        scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, w, lane, nrows, K, qn, thr_d, thr_i, ncand);
+        scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, lane, nrows, K, qn, thr_d, thr_i, ncand);
         // the bound is tested at chunk boundaries: merge what is queued
-        flush_queue(S, w, lane, nrows, K, qn, thr_d, thr_i);
+        flush_queue(S, lane, nrows, K, qn, thr_d, thr_i);
     }
 
     // 2. beyond the table: Chebyshev rings table_r + 1, table_r + 2, ... (sparse regions)
@@ -352,12 +354,12 @@ __global__ void __launch_bounds__(KNN_WARPS * 32)
                 if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
                 if (ok && !box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
             }
-            scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, w, lane, nrows, K, qn, thr_d, thr_i, ncand);
+            scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, lane, nrows, K, qn, thr_d, thr_i, ncand);
         }
-        flush_queue(S, w, lane, nrows, K, qn, thr_d, thr_i);
+        flush_queue(S, lane, nrows, K, qn, thr_d, thr_i);
     }
     __syncwarp();
-    for (int idx = lane; idx < K; idx += 32) out[t * stride + idx] = S.row_i[w][idx];
+    for (int idx = lane; idx < K; idx += 32) out[t * stride + idx] = S.row_i[idx];
     if (cand_counter && lane == 0) atomicAdd(cand_counter, ncand);
 }
 
@@ -406,20 +408,22 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
     cudaError_t e = cudaSuccess;
     if (c->knn_table_n == 0 && (e = build_knn_table(c))) return e;
     DevScalars* sc = (DevScalars*)c->scalars.p;
-    const unsigned blocks = (unsigned)((nq + KNN_WARPS - 1) / KNN_WARPS);
+    const int KW = c->tune.knn_warps;  // warps (queries) per block: autotuned, 2, 4 or 8
+    const unsigned blocks = (unsigned)((nq + KW - 1) / KW);
     const uint32_t* perm = (const uint32_t*)c->perm.p;
     const SubGrid grid = {(const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
                           (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
                           (const uint32_t*)c->sub_start.p};
     const int2* tab = (const int2*)c->knn_table.p;
-    if (c->prm.dim == 2)
-        k_knn<2><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double2*)c->spts.p, perm, grid, tab,
-                                                           c->knn_table_n, c->knn_table_r, qs, nq, K, kq, stride,
-                                                           out, &sc->knn_cand);
-    else
-        k_knn<3><<<blocks, KNN_WARPS * 32, 0, c->stream>>>((const double4*)c->spts.p, perm, grid, tab,
-                                                           c->knn_table_n, c->knn_table_r, qs, nq, K, kq, stride,
-                                                           out, &sc->knn_cand);
+#define PGPU_KNN(DD, PT, WW)                                                                                 \
+    k_knn<DD, WW><<<blocks, WW * 32, 0, c->stream>>>((const PT*)c->spts.p, perm, grid, tab, c->knn_table_n,     \
+                                                      c->knn_table_r, qs, nq, K, kq, stride, out, &sc->knn_cand)
+    if (c->prm.dim == 2) {
+        if (KW == 2) PGPU_KNN(2, double2, 2); else if (KW == 8) PGPU_KNN(2, double2, 8); else PGPU_KNN(2, double2, 4);
+    } else {
+        if (KW == 2) PGPU_KNN(3, double4, 2); else if (KW == 8) PGPU_KNN(3, double4, 8); else PGPU_KNN(3, double4, 4);
+    }
+#undef PGPU_KNN
     count_launches(1);
     return cudaGetLastError();
 }

@@ -371,9 +371,8 @@ cudaError_t launch_ghosts(pgpu_ctx* c, const double* pos_dev, int64_t n, bool no
     return cudaGetLastError();
 }
 
-// Grid resolution: about GRID_PPB points per bin.
-static int grid_resolution(int64_t n, int D) {
-    const double ppb = D == 2 ? 2.0 : 2.0;
+// Grid resolution: about ppb points per coarse bin (autotuned; 2 by default).
+static int grid_resolution(int64_t n, int D, double ppb) {
     double g = D == 2 ? sqrt((double)n / ppb) : cbrt((double)n / ppb);
     int G = (int)(g + 0.5);
     if (G < 1) G = 1;
@@ -392,7 +391,7 @@ cudaError_t launch_grid_sort(pgpu_ctx* c) {
     Instances& I = c->inst;
     int64_t M = 0;
     for (int b = 0; b < I.n; b++) {
-        const int Gb = grid_resolution(I.ext_count[b], D);
+        const int Gb = grid_resolution(I.ext_count[b], D, c->tune.ppb);
         int64_t P = 1;
         while (P < Gb) P <<= 1;
         I.par[b].G = Gb;

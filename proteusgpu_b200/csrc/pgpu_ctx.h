@@ -88,6 +88,13 @@ struct Instances {
     DevBuf d_gather;                 // u32 scratch for per-instance ghost totals
 };
 
+// Launch shapes chosen by pgpu_autotune (defaults until it runs).
+struct Tuning {
+    double ppb = 2.0;    // mean points per coarse grid bin
+    int knn_warps = 4;   // queries (warps) per KNN block: 2, 4 or 8
+    int clip_warps = 4;  // cells (warps) per clipping block: 2 or 4
+};
+
 struct KBudget {
     bool enabled = false;
     bool trained = false;
@@ -161,6 +168,7 @@ struct pgpu_ctx {
     pgpu::DevBuf fb_qs, fb_knn; // fallback query list and lists
     pgpu::KBudget kb;           // learned neighbour budget (optional form)
     pgpu::Instances inst;       // the simulation(s) of this context
+    pgpu::Tuning tune;          // launch shapes (pgpu_autotune)
 };
 
 namespace pgpu {
