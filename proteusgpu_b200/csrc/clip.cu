@@ -61,6 +61,8 @@ struct WarpCell {
             unsigned long long emask[MAX_P];
             unsigned char nxt[MAX_P];
             float4 hp32[MAX_P];   // FP32 local-frame planes (k_clip32)
+            uint32_t stage[MAX_P];  // new vertices of the current cut, in their final order
+            double stage_d2[MAX_P]; // and their squared distances to the seed (FP64 clip)
         } b;
         double vpos[MAX_T][3];
     } u;
@@ -504,9 +506,7 @@ __device__ __forceinline__ int clip_by(WarpCell& W, int lane, uint32_t z, double
     const int kept = nb_t - nb_r;
     int n_new = 0;
     bool bad = false;
-    uint32_t my_new[9];
-    int my_new_pos[9];
-    int my_new_cnt = 0;
+    uint32_t* stage = W.u.b.stage;  // new vertices, written at their final position
     if (D == 2) {
         uint32_t lo = 0, hi = 0;  // XOR of the lines of removed vertices
 #pragma unroll
@@ -536,9 +536,7 @@ __device__ __forceinline__ int clip_by(WarpCell& W, int lane, uint32_t z, double
                 int j = lane == 0 ? b0 : b1;
                 const double4 hi_ = W.hp[cur], hj = W.hp[j];
                 double rw = det2(hi_.x, hi_.y, hj.x, hj.y);  // new_vertex orientation (cell.cpp:351-359)
-                my_new[0] = rw > 0 ? pack3(j, cur, 0) : pack3(cur, j, 0);
-                my_new_pos[0] = lane;
-                my_new_cnt = 1;
+                stage[lane] = rw > 0 ? pack3(j, cur, 0) : pack3(cur, j, 0);
             }
         }
     } else {
@@ -569,9 +567,8 @@ __device__ __forceinline__ int clip_by(WarpCell& W, int lane, uint32_t z, double
                 bool isb = rem && !((em[y] >> x) & 1ull);
                 unsigned bal = __ballot_sync(FULL, isb);
                 if (isb) {
-                    my_new[my_new_cnt] = pack3(cur, x, y);
-                    my_new_pos[my_new_cnt] = base + __popc(bal & ((1u << lane) - 1u));
-                    my_new_cnt++;
+                    const int pos = base + __popc(bal & ((1u << lane) - 1u));
+                    if (pos < MAX_P) stage[pos] = pack3(cur, x, y);
                     src |= 1ull << x;
                     W.u.b.nxt[x] = (unsigned char)y;
                 }
@@ -615,14 +612,16 @@ __device__ __forceinline__ int clip_by(WarpCell& W, int lane, uint32_t z, double
         fail_vdist = max_vd2(W, nb_t, lane, km);
         return CLIP_FAIL;
     }
-    // 3. new vertices and their certificate distances
-    double nd2[9];
+    // 3. new vertices and their certificate distances, one lane each
+    __syncwarp();
     double newmax = 0.0;
-    for (int q = 0; q < my_new_cnt; q++) {
+    const int n_st = n_new < MAX_P ? n_new : MAX_P;
+    for (int q = lane; q < n_st; q += 32) {
         double x, y, zz;
-        vertex_pos<D>(W.hp, my_new[q], x, y, zz);
-        nd2[q] = seed_d2(x, y, zz, sx, sy, sz);
-        newmax = nan_max(newmax, nd2[q]);
+        vertex_pos<D>(W.hp, stage[q], x, y, zz);
+        const double d2 = seed_d2(x, y, zz, sx, sy, sz);
+        W.u.b.stage_d2[q] = d2;
+        newmax = nan_max(newmax, d2);
     }
     if (kept + n_new >= MAX_T) {  // new_vertex overflow (cell.cpp:347-350)
         status = ST_TRIANGLE_OVERFLOW;
@@ -653,9 +652,9 @@ __device__ __forceinline__ int clip_by(WarpCell& W, int lane, uint32_t z, double
             W.tri[kp[j]] = kt[j];
             W.vd2[kp[j]] = kd[j];
         }
-    for (int q = 0; q < my_new_cnt; q++) {
-        W.tri[kept + my_new_pos[q]] = my_new[q];
-        W.vd2[kept + my_new_pos[q]] = nd2[q];
+    for (int q = lane; q < n_new; q += 32) {
+        W.tri[kept + q] = stage[q];
+        W.vd2[kept + q] = W.u.b.stage_d2[q];
     }
     if (lane == 0) W.vid[cur] = (int)z;
     if (cur == nb_v) nb_v++;
@@ -1319,9 +1318,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
         const int kept = nb_t - nb_r;
         int n_new = 0;
         bool bad = false;
-        uint32_t my_new[9];
-        int my_new_pos[9];
-        int my_new_cnt = 0;
+        uint32_t* stage = W.u.b.stage;  // new vertices, written at their final position
         if (D == 2) {
             uint32_t lo = 0, hi = 0;
 #pragma unroll
@@ -1353,9 +1350,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
                     const float4 hi_ = hp[cur], hj = hp[j];
                     const float rw = det2f(hi_.x, hi_.y, hj.x, hj.y);
                     und = !(fabsf(rw) > F32_BOUND * per2f(hi_.x, hi_.y, hj.x, hj.y));
-                    my_new[0] = rw > 0 ? pack3(j, cur, 0) : pack3(cur, j, 0);
-                    my_new_pos[0] = lane;
-                    my_new_cnt = 1;
+                    stage[lane] = rw > 0 ? pack3(j, cur, 0) : pack3(cur, j, 0);
                 }
                 if (__any_sync(FULL, und)) bad = true;
             }
@@ -1387,9 +1382,8 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
                     const bool isb = rem && !((em[y] >> x) & 1ull);
                     const unsigned bal = __ballot_sync(FULL, isb);
                     if (isb) {
-                        my_new[my_new_cnt] = pack3(cur, x, y);
-                        my_new_pos[my_new_cnt] = base + __popc(bal & ((1u << lane) - 1u));
-                        my_new_cnt++;
+                        const int pos = base + __popc(bal & ((1u << lane) - 1u));
+                        if (pos < MAX_P) stage[pos] = pack3(cur, x, y);
                         src |= 1ull << x;
                         W.u.b.nxt[x] = (unsigned char)y;
                     }
@@ -1427,13 +1421,10 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
             }
             __syncwarp();
         }
-        if (bad || kept + n_new >= MAX_T) {
+        if (bad || kept + n_new >= MAX_T || n_new > MAX_P) {
             reclip = true;
             break;
         }
-        float4 nV[9];
-        float4 nP[9];
-        for (int q = 0; q < my_new_cnt; q++) vertex_h32<D>(hp, my_new[q], nV[q], nP[q]);
         uint32_t kt[3];
         float4 kd[3];
         float4 kb[3];
@@ -1460,10 +1451,14 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
                 W.V32[kp[j]] = kd[j];
                 W.P32[kp[j]] = kb[j];
             }
-        for (int q = 0; q < my_new_cnt; q++) {
-            W.tri[kept + my_new_pos[q]] = my_new[q];
-            W.V32[kept + my_new_pos[q]] = nV[q];
-            W.P32[kept + my_new_pos[q]] = nP[q];
+        // new vertices after the kept ones, one lane each
+        for (int q = lane; q < n_new; q += 32) {
+            const uint32_t tv = stage[q];
+            float4 V, Pb;
+            vertex_h32<D>(hp, tv, V, Pb);
+            W.tri[kept + q] = tv;
+            W.V32[kept + q] = V;
+            W.P32[kept + q] = Pb;
         }
         if (lane == 0) W.vid[cur] = (int)z;
         nb_v++;
