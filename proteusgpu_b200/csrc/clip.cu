@@ -1271,14 +1271,28 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
     int k_stop = 0, k_last = 0;
     float v_dist = max_vd2f(W, nb_t, lane);
 
+    // neighbours are fetched 32 at a time, one per lane, and broadcast plane by plane
+    uint32_t zc = NO_NEIGHBOR;
+    double cx = 0.0, cy = 0.0, cz = 0.0;
     for (int k = 0; k < K; k++) {
-        const uint32_t z = kl[k];
+        if ((k & 31) == 0) {
+            const int kk = k + lane;
+            zc = kk < K ? kl[kk] : NO_NEIGHBOR;
+            if (zc != NO_NEIGHBOR) {
+                const PT Bc = ext[zc];
+                cx = Bc.x;
+                cy = Bc.y;
+                cz = pz(Bc);
+            }
+        }
+        const uint32_t z = __shfl_sync(FULL, zc, k & 31);
         if (z == NO_NEIGHBOR) break;
         k_stop = k + 1;
-        const PT B = ext[z];
-        const double bx = B.x - sx, by = B.y - sy, bz = pz(B) - sz;  // local frame, exact in FP64
+        const double Bx = __shfl_sync(FULL, cx, k & 31), By = __shfl_sync(FULL, cy, k & 31),
+                     Bz = __shfl_sync(FULL, cz, k & 31);
+        const double bx = Bx - sx, by = By - sy, bz = Bz - sz;  // local frame, exact in FP64
         const float fx = (float)bx, fy = (float)by, fz = (float)bz;
-        const double d2B = seed_d2(B.x, B.y, pz(B), sx, sy, sz);
+        const double d2B = seed_d2(Bx, By, Bz, sx, sy, sz);
         if (nb_v >= MAX_P) {
             reclip = true;
             break;
