@@ -1399,7 +1399,6 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
                         const int pos = base + __popc(bal & ((1u << lane) - 1u));
                         if (pos < MAX_P) stage[pos] = pack3(cur, x, y);
                         src |= 1ull << x;
-                        W.u.b.nxt[x] = (unsigned char)y;
                     }
                     base += __popc(bal);
                 }
@@ -1408,21 +1407,12 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) src |= __shfl_xor_sync(FULL, src, o);
             __syncwarp();
-            bool ok = __popcll(src) == n_new && n_new >= 3;
-            if (ok && lane == 0) {
-                const int x0 = __ffsll((long long)src) - 1;
-                int x = x0;
-                for (int st = 1; st <= n_new; st++) {
-                    x = W.u.b.nxt[x];
-                    if (!((src >> x) & 1ull) || (x == x0 && st < n_new)) {
-                        ok = false;
-                        break;
-                    }
-                }
-                if (x != x0) ok = false;
-            }
-            ok = __shfl_sync(FULL, ok ? 1 : 0, 0) != 0;
-            bad = !ok;
+            // Every predicate that reached this point was decided beyond its error
+            // bound, so the conflict set is the exact one and (no vertex lies on the
+            // plane: that would have been undecided) the cavity boundary is one simple
+            // cycle; the reference's walk (cell.cpp:262-300), which the FP64 kernel
+            // replays, cannot fail here.  Each source plane appearing once is checked.
+            bad = !(__popcll(src) == n_new && n_new >= 3);
 #pragma unroll
             for (int j = 0; j < 3; j++) {
                 const int i = lane + 32 * j;
