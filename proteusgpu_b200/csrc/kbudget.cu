@@ -6,7 +6,7 @@
 // Each hydro cell gets 8 features from the previous mesh and the new grid:
 //   0 log2(1 + certified K of the previous step) / 8
 //   1 log2(1 + points in the cell's grid bin) / 4
-//   2 log2(1 + points in the 3^D bins around it) / 8
+//   2 refinement level of that bin (dense bins are split into (2^L)^D sub-bins) / 4
 //   3 relative volume change over the last step, (V - V_prev) / V, x 4 in [-4, 4]
 //     (the cell's velocity divergence times dt)
 //   4 log2(V * N) / 4, the cell's volume relative to the mean
@@ -446,7 +446,7 @@ __global__ void k_mlp_bf16_all(const float* __restrict__ w, uint16_t* __restrict
 template <int D>
 __global__ void k_kb_features(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ perm,
                               const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ bin_start,
-                              const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst, int64_t nq,
+                              const uint8_t* __restrict__ lvl, const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst, int64_t nq,
                               int64_t n_hydro, const int* __restrict__ certk,
                               const double* __restrict__ vol, const uint32_t* __restrict__ fcnt,
                               const double* __restrict__ centroid, const double* __restrict__ pos,
@@ -463,21 +463,12 @@ __global__ void k_kb_features(const uint32_t* __restrict__ qs, const uint32_t* _
         const int bx = bin_coord(p.x, G), by = bin_coord(p.y, G), bz = D == 3 ? bin_coord(pz(p), G) : 0;
         const uint32_t own = par.slot0 + morton<D>(bx, by, bz);
         const uint32_t occ = bin_start[own + 1] - bin_start[own];
-        uint32_t occ_nb = 0;
-        for (int dz = (D == 3 ? -1 : 0); dz <= (D == 3 ? 1 : 0); dz++)
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    const int x = bx + dx, y = by + dy, z = bz + dz;
-                    if (x < 0 || x >= G || y < 0 || y >= G || (D == 3 && (z < 0 || z >= G))) continue;
-                    const uint32_t k = par.slot0 + morton<D>(x, y, z);
-                    occ_nb += bin_start[k + 1] - bin_start[k];
-                }
         const double V = vol[e];
         const float Vp = hist_vol[e];
         hist_vol[e] = (float)V;
         f[0] = log2f(1.0f + (float)certk[e]) * 0.125f;
         f[1] = log2f(1.0f + (float)occ) * 0.25f;
-        f[2] = log2f(1.0f + (float)occ_nb) * 0.125f;
+        f[2] = 0.25f * (float)lvl[own];
         f[3] = (Vp > 0.0f && V > 0.0) ? 4.0f * fminf(fmaxf((float)((V - (double)Vp) / V), -1.0f), 1.0f) : 0.0f;
         f[4] = V > 0.0 ? 0.25f * log2f((float)(V * (double)par.count)) : -2.0f;
         f[5] = miss[e] ? 1.0f : 0.0f;
@@ -589,13 +580,15 @@ cudaError_t kb_features(pgpu_ctx* c) {
     if (c->prm.dim == 2)
         k_kb_features<2><<<nblk(nq, 256), 256, 0, c->stream>>>(
             (const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p, (const double2*)c->spts.p,
-            (const uint32_t*)c->bin_start.p, (const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
+            (const uint32_t*)c->bin_start.p, (const uint8_t*)c->bin_lvl.p, (const InstPar*)c->inst.d_par.p,
+            (const uint16_t*)c->inst.d_inst_e.p,
             nq, nh, (const int*)c->certk.p, (const double*)c->vol.p,
             (const uint32_t*)c->fcnt.p, (const double*)c->centroid.p, (const double*)c->pos.p, hv, ms, feat);
     else
         k_kb_features<3><<<nblk(nq, 256), 256, 0, c->stream>>>(
             (const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p, (const double4*)c->spts.p,
-            (const uint32_t*)c->bin_start.p, (const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
+            (const uint32_t*)c->bin_start.p, (const uint8_t*)c->bin_lvl.p, (const InstPar*)c->inst.d_par.p,
+            (const uint16_t*)c->inst.d_inst_e.p,
             nq, nh, (const int*)c->certk.p, (const double*)c->vol.p,
             (const uint32_t*)c->fcnt.p, (const double*)c->centroid.p, (const double*)c->pos.p, hv, ms, feat);
     count_launches(1);
