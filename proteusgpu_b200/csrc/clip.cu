@@ -54,6 +54,7 @@ struct WarpCell {
         struct {                     // k_clip32 while clipping
             float4 V32[MAX_T];       // homogeneous vertex coordinates (rx, ry, rz, rw)
             float4 P32[MAX_T];       // permanents of the same minors (their rounding bounds)
+            float D32[MAX_T];        // squared distance of the vertex to the seed
         };
     };
     union {
@@ -1182,7 +1183,7 @@ __device__ __forceinline__ float max_vd2f(const WarpCell& W, int n, int lane) {
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         const int i = lane + 32 * j;
-        if (i < n) m = nan_maxf(m, vd2_of(W.V32[i]));
+        if (i < n) m = nan_maxf(m, W.D32[i]);
     }
     return warp_maxf(m);
 }
@@ -1264,7 +1265,10 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
         W.tri[lane] = tv;
     }
     __syncwarp();
-    if (lane < ntri0) vertex_h32<D>(hp, W.tri[lane], W.V32[lane], W.P32[lane]);
+    if (lane < ntri0) {
+        vertex_h32<D>(hp, W.tri[lane], W.V32[lane], W.P32[lane]);
+        W.D32[lane] = vd2_of(W.V32[lane]);
+    }
     __syncwarp();
     int nb_v = 2 * D, nb_t = ntri0;
     bool reclip = false, certified = false;
@@ -1432,6 +1436,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
         uint32_t kt[3];
         float4 kd[3];
         float4 kb[3];
+        float kr[3];
         int kp[3];
         int before = 0;
 #pragma unroll
@@ -1444,6 +1449,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
             kt[j] = keep ? W.tri[i] : 0u;
             kd[j] = keep ? W.V32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
             kb[j] = keep ? W.P32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            kr[j] = keep ? W.D32[i] : 0.0f;
             kp[j] = keep ? before + __popc(kmj & ((1u << lane) - 1u)) : -1;
             before += __popc(kmj);
         }
@@ -1454,6 +1460,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
                 W.tri[kp[j]] = kt[j];
                 W.V32[kp[j]] = kd[j];
                 W.P32[kp[j]] = kb[j];
+                W.D32[kp[j]] = kr[j];
             }
         // new vertices after the kept ones, one lane each
         for (int q = lane; q < n_new; q += 32) {
@@ -1463,6 +1470,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
             W.tri[kept + q] = tv;
             W.V32[kept + q] = V;
             W.P32[kept + q] = Pb;
+            W.D32[kept + q] = vd2_of(V);
         }
         if (lane == 0) W.vid[cur] = (int)z;
         nb_v++;
