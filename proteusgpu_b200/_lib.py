@@ -27,6 +27,7 @@ EXPORTED = [
     "pgpu_launch_count", "pgpu_fp64_peak", "pgpu_riemann_hll", "pgpu_dt_cfl_static",
     "pgpu_kbudget_enable", "pgpu_kbudget_classes", "pgpu_kbudget_stats", "pgpu_kbudget_weights",
     "pgpu_mlp_forward", "pgpu_mlp_grad", "pgpu_fp32_peak", "pgpu_batch_init", "pgpu_batch_dt", "pgpu_autotune",
+    "pgpu_set_tuning",
 ]
 
 
@@ -56,7 +57,8 @@ BOUNDARY = {"periodic": 0, "reflective": 1}
 
 class Tuning(C.Structure):
     _fields_ = [("ppb", C.c_double), ("knn_warps", C.c_int32), ("clip_warps", C.c_int32),
-                ("ms_default", C.c_float), ("ms_tuned", C.c_float), ("from_cache", C.c_int32)]
+                ("clip_thread", C.c_int32), ("ms_default", C.c_float), ("ms_tuned", C.c_float),
+                ("from_cache", C.c_int32)]
 KB_NPARAM = 1542  # W1[32][8], b1[32], W2[32][32], b2[32], W3[6][32], b3[6]
 
 _LIB = None
@@ -109,6 +111,7 @@ def load(path: str = LIB_PATH):
     L.pgpu_batch_init.argtypes = [vp, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp]
     L.pgpu_batch_dt.argtypes = [vp, vp]
     L.pgpu_autotune.argtypes = [vp, C.POINTER(Tuning)]
+    L.pgpu_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
     L.pgpu_riemann_hll.argtypes = [C.c_int, dbl, vp, vp, vp, vp]
     L.pgpu_dt_cfl_static.argtypes = [C.c_int, dbl, dbl, vp, vp, vp, vp, i64, vp, vp]
     L.pgpu_kbudget_enable.argtypes = [vp, C.c_int, C.c_int, dbl, C.c_uint64]

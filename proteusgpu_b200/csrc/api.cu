@@ -856,12 +856,19 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
             if (t < bt) bt = t, best.knn_warps = kw;
         }
         c->tune.knn_warps = best.knn_warps;
-        // 3. clipping block size
+        // 3. clipping: a warp per cell with 2 or 4 cells per block, or (2D) a thread per cell
         bt = 1e30f;
         for (int cw : {2, 4}) {
             c->tune.clip_warps = cw;
             if ((r = timed_build(c, 0x8, &t))) return r;
             if (t < bt) bt = t, best.clip_warps = cw;
+        }
+        c->tune.clip_warps = best.clip_warps;
+        if (c->prm.dim == 2) {
+            c->tune.clip_thread = true;
+            if ((r = timed_build(c, 0x8, &t))) return r;
+            if (t < bt) bt = t, best.clip_thread = true;
+            c->tune.clip_thread = false;
         }
         c->tune = best;
         if ((r = timed_build(c, 0xF, &t))) return r;
@@ -874,7 +881,21 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
     res.ppb = c->tune.ppb;
     res.knn_warps = c->tune.knn_warps;
     res.clip_warps = c->tune.clip_warps;
+    res.clip_thread = c->tune.clip_thread ? 1 : 0;
     if (out) *out = res;
+    return PGPU_OK;
+}
+
+int pgpu_set_tuning(pgpu_ctx* c, const pgpu_tuning* t) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!t || !(t->ppb >= 0.5 && t->ppb <= 64.0) || (t->knn_warps != 2 && t->knn_warps != 4 && t->knn_warps != 8) ||
+        (t->clip_warps != 2 && t->clip_warps != 4))
+        return fail(c, PGPU_EINVAL, "pgpu_set_tuning: bad launch shapes");
+    c->tune.ppb = t->ppb;
+    c->tune.knn_warps = t->knn_warps;
+    c->tune.clip_warps = t->clip_warps;
+    c->tune.clip_thread = t->clip_thread != 0;
     return PGPU_OK;
 }
 

@@ -1533,6 +1533,268 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
     extract_and_store<D>(W, P, w, lane, nb_v, nb_t, e, certk, sx, sy, sz, true);
 }
 
+// ============================================================================
+// Thread-per-cell 2D clipping.  A 2D cell has ~6 vertices, so the warp-per-cell
+// kernel leaves most lanes idle; here each thread clips one cell with the same
+// arithmetic in the same order (vertex list, predicates, new-vertex orientation,
+// stable compaction, certificate, angle-ordered area, plane-ordered faces), so
+// the result is the warp kernel's bit for bit.  Cells needing more than
+// T2P planes or T2T vertices are marked ST_RECLIP and re-run by the warp kernel.
+constexpr int T2P = 24;
+constexpr int T2T = 24;
+constexpr int T2_THREADS = 128;
+
+__global__ void __launch_bounds__(T2_THREADS) k_clip2t(ClipParams P) {
+    const int64_t t = (int64_t)blockIdx.x * T2_THREADS + threadIdx.x;
+    if (t >= P.nq) return;
+    const int64_t tq = P.slots ? (int64_t)P.slots[t] : t;
+    const uint32_t s = P.qs[tq];
+    const uint32_t e = P.perm[s];
+    const double2* spts = (const double2*)P.spts;
+    const double2* ext = (const double2*)P.ext;
+    const double2 sp = spts[s];
+    const double sx = sp.x, sy = sp.y, sz = 0.0;
+    const int K = P.kq ? (int)P.kq[tq] : P.K;
+    const uint32_t* kl = P.knn + (size_t)tq * P.K;
+
+    double4 hp[T2P];
+    int vid[T2P];
+    uint32_t tri[T2T];
+    double vd2[T2T];
+    const double beps = 1e-14;
+    const double xmin = -beps, xmax = 1.0 + beps;
+    hp[0] = make_double4(1.0, 0.0, 0.0, -xmin);
+    hp[1] = make_double4(-1.0, 0.0, 0.0, xmax);
+    hp[2] = make_double4(0.0, 1.0, 0.0, -xmin);
+    hp[3] = make_double4(0.0, -1.0, 0.0, xmax);
+    for (int i = 0; i < 4; i++) vid[i] = -1;
+    tri[0] = pack3(2, 0, 0);
+    tri[1] = pack3(1, 2, 0);
+    tri[2] = pack3(3, 1, 0);
+    tri[3] = pack3(0, 3, 0);
+    double v_dist = 0.0;
+    for (int i = 0; i < 4; i++) {
+        double x, y, z;
+        vertex_pos<2>(hp, tri[i], x, y, z);
+        vd2[i] = seed_d2(x, y, z, sx, sy, sz);
+        v_dist = nan_max(v_dist, vd2[i]);
+    }
+    int nb_v = 4, nb_t = 4;
+    int status = ST_SUCCESS, certk = 0;
+    double fail_vdist = 0.0;
+    bool too_big = false;
+    for (int k = 0; k < K; k++) {
+        const uint32_t z = kl[k];
+        if (z == NO_NEIGHBOR) break;
+        const double2 B = ext[z];
+        const double bx = B.x, by = B.y, bz = 0.0;
+        const double d2B = seed_d2(bx, by, bz, sx, sy, sz);
+        if (nb_v >= MAX_P) {
+            status = ST_VERTEX_OVERFLOW;
+            fail_vdist = v_dist;
+            break;
+        }
+        if (nb_v >= T2P) {
+            too_big = true;
+            break;
+        }
+        const double dx = sx - bx, dy = sy - by, dz = sz - bz;
+        const double ax = sx + bx, ay = sy + by, az = sz + bz;
+        const double dot = ax * dx + ay * dy + az * dz;
+        const double4 eq = make_double4(dx, dy, dz, -dot / 2.0);
+        const int cur = nb_v;
+        hp[cur] = eq;
+        uint32_t cm = 0;  // vertices in conflict (nb_t <= T2T < 32)
+        bool near = false;
+        for (int i = 0; i < nb_t; i++)
+            if (in_conflict<2>(hp, tri[i], eq, &near, P.robust)) cm |= 1u << i;
+        const int nb_r = __popc(cm);
+        if (near) {
+            status = ST_NEEDS_EXACT_PREDICATES;
+            double m = 0.0;
+            for (int i = 0; i < nb_t; i++)
+                if (!((cm >> i) & 1u)) m = nan_max(m, vd2[i]);
+            fail_vdist = m;
+            break;
+        }
+        if (nb_r == 0) {
+            if (d2B > 4 * v_dist) {
+                certk = k + 1;
+                break;
+            }
+            continue;
+        }
+        unsigned long long xm = 0ull;
+        for (int i = 0; i < nb_t; i++)
+            if ((cm >> i) & 1u) xm ^= (1ull << tri_a(tri[i])) ^ (1ull << tri_b(tri[i]));
+        const int kept = nb_t - nb_r;
+        if (__popcll(xm) < 2) {
+            status = ST_INCONSISTENT_BOUNDARY;
+            double m = 0.0;
+            for (int i = 0; i < nb_t; i++)
+                if (!((cm >> i) & 1u)) m = nan_max(m, vd2[i]);
+            fail_vdist = m;
+            break;
+        }
+        const int b0 = __ffsll((long long)xm) - 1;
+        const unsigned long long x2 = xm & (xm - 1);
+        const int b1 = __ffsll((long long)x2) - 1;
+        uint32_t nt[2];
+        double nd[2];
+        double newmax = 0.0;
+        for (int q = 0; q < 2; q++) {
+            const int j = q == 0 ? b0 : b1;
+            const double rw = det2(hp[cur].x, hp[cur].y, hp[j].x, hp[j].y);  // new_vertex orientation
+            nt[q] = rw > 0 ? pack3(j, cur, 0) : pack3(cur, j, 0);
+            double x, y, zz;
+            vertex_pos<2>(hp, nt[q], x, y, zz);
+            nd[q] = seed_d2(x, y, zz, sx, sy, sz);
+            newmax = nan_max(newmax, nd[q]);
+        }
+        if (kept + 2 >= MAX_T) {
+            status = ST_TRIANGLE_OVERFLOW;
+            double m = 0.0;
+            for (int i = 0; i < nb_t; i++)
+                if (!((cm >> i) & 1u)) m = nan_max(m, vd2[i]);
+            fail_vdist = nan_max(m, newmax);
+            break;
+        }
+        if (kept + 2 > T2T) {
+            too_big = true;
+            break;
+        }
+        int w = 0;
+        for (int i = 0; i < nb_t; i++)
+            if (!((cm >> i) & 1u)) {
+                tri[w] = tri[i];
+                vd2[w] = vd2[i];
+                w++;
+            }
+        tri[kept] = nt[0];
+        vd2[kept] = nd[0];
+        tri[kept + 1] = nt[1];
+        vd2[kept + 1] = nd[1];
+        vid[cur] = (int)z;
+        nb_v++;
+        nb_t = kept + 2;
+        double m = 0.0;
+        for (int i = 0; i < nb_t; i++) m = nan_max(m, vd2[i]);
+        v_dist = m;
+        if (d2B > 4 * v_dist) {
+            certk = k + 1;
+            break;
+        }
+    }
+    if (too_big) {
+        P.status[e] = ST_RECLIP;
+        atomicAdd(P.reclip, 1u);
+        return;
+    }
+    {
+        const double vdf = status == ST_SUCCESS ? v_dist : fail_vdist;
+        const uint32_t zK = kl[K - 1];
+        if (zK == NO_NEIGHBOR) {
+            status = ST_SECURITY_RADIUS_NOT_REACHED;
+        } else {
+            const double2 BK = ext[zK];
+            if (!(seed_d2(BK.x, BK.y, 0.0, sx, sy, sz) > 4 * vdf)) status = ST_SECURITY_RADIUS_NOT_REACHED;
+        }
+    }
+    if (status != ST_SUCCESS) {
+        if (status == ST_SECURITY_RADIUS_NOT_REACHED && (int64_t)e < P.n_hydro) atomicAdd(P.uncertified, 1u);
+        P.vol[e] = 0.0;
+        P.fptr[e] = 0;
+        P.fcnt[e] = 0;
+        P.status[e] = status;
+        P.certk[e] = 0;
+        P.centroid[3 * (size_t)e] = P.centroid[3 * (size_t)e + 1] = P.centroid[3 * (size_t)e + 2] = 0.0;
+        return;
+    }
+    // ---- extraction (cell.cpp:416-669), the warp kernel's 2D branch in one thread
+    double vx[T2T], vy[T2T];
+    for (int i = 0; i < nb_t; i++) {
+        double z;
+        vertex_pos<2>(hp, tri[i], vx[i], vy[i], z);
+    }
+    double cx = 0, cy = 0;
+    for (int i = 0; i < nb_t; i++) cx += vx[i], cy += vy[i];
+    cx /= nb_t;
+    cy /= nb_t;
+    double ang[T2T];
+    for (int i = 0; i < nb_t; i++) ang[i] = atan2(vy[i] - cy, vx[i] - cx);
+    unsigned char order[T2T];
+    for (int i = 0; i < nb_t; i++) {
+        int rank = 0;
+        for (int q = 0; q < nb_t; q++) rank += (ang[q] < ang[i] || (ang[q] == ang[i] && q < i)) ? 1 : 0;
+        order[rank] = (unsigned char)i;
+    }
+    double a = 0, mx = 0, my = 0, sa = 0;
+    for (int i = 0; i < nb_t; i++) {
+        const int j = (i + 1) % nb_t;
+        const int pi = order[i], qi = order[j];
+        a += vx[pi] * vy[qi];
+        a -= vx[qi] * vy[pi];
+        const double cr = (vx[pi] - cx) * (vy[qi] - cy) - (vx[qi] - cx) * (vy[pi] - cy);
+        mx += (vx[pi] + vx[qi] - 2 * cx) * cr;
+        my += (vy[pi] + vy[qi] - 2 * cy) * cr;
+        sa += cr;
+    }
+    const double cell_vol = fabs(a) / 2.0;
+    const double cen0 = cx + mx / (3.0 * sa), cen1 = cy + my / (3.0 * sa);
+    // faces: planes in order, the first two vertices on each give its edge
+    double area[T2P];
+    unsigned valid = 0;
+    int nf = 0;
+    for (int p = 0; p < nb_v; p++) {
+        int cnt = 0, v0 = -1, v1 = -1;
+        for (int i = 0; i < nb_t; i++)
+            if ((int)tri_a(tri[i]) == p || (int)tri_b(tri[i]) == p) {
+                if (cnt == 0) v0 = i; else if (cnt == 1) v1 = i;
+                cnt++;
+            }
+        if (cnt >= 2) {
+            const double ddx = vx[v1] - vx[v0], ddy = vy[v1] - vy[v0];
+            area[p] = sqrt(ddx * ddx + ddy * ddy);
+            valid |= 1u << p;
+            nf++;
+        }
+    }
+    const double uscale = P.ip[P.inst[e]].scale_out;
+    const double vscale = uscale * uscale, ascale = uscale;
+    const unsigned long long base = atomicAdd(P.face_counter, (unsigned long long)nf);
+    const bool fits = base + (unsigned long long)nf <= P.face_cap;
+    if (!fits) {
+        atomicOr(P.overflow, 1u);
+    } else {
+        int idx = 0;
+        for (int p = 0; p < nb_v; p++) {
+            if (!((valid >> p) & 1u)) continue;
+            const size_t f = base + idx++;
+            const double4 pe = hp[p];
+            const double nlen = sqrt(pe.x * pe.x + pe.y * pe.y + pe.z * pe.z);  // compute_face_normal
+            const int nbr = vid[p];
+            P.f_nb[f] = nbr;
+            uint32_t own = BOX_FACE;
+            if (nbr >= 0) {
+                if ((int64_t)nbr < P.n_hydro)
+                    own = pack_owner((uint32_t)nbr, 0);
+                else
+                    own = pack_owner(P.ghost_src[nbr - P.n_hydro], P.ghost_code[nbr - P.n_hydro]);
+            }
+            P.f_own[f] = own;
+            P.f_geo[f] = make_double4(pe.x / nlen, pe.y / nlen, pe.z / nlen, ascale * area[p]);
+        }
+    }
+    P.vol[e] = vscale * cell_vol;
+    P.fptr[e] = fits ? (uint32_t)base : 0u;
+    P.fcnt[e] = fits ? (uint32_t)nf : 0u;
+    P.status[e] = ST_SUCCESS;
+    P.certk[e] = certk;
+    P.centroid[3 * (size_t)e] = (cen0 - 0.5) * uscale + 0.5;
+    P.centroid[3 * (size_t)e + 1] = (cen1 - 0.5) * uscale + 0.5;
+    P.centroid[3 * (size_t)e + 2] = 0.0;
+}
+
 }  // namespace
 
 namespace {
@@ -1592,7 +1854,7 @@ cudaError_t select_cells(pgpu_ctx* c, int code, bool hydro_only, bool as_slots, 
 cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const uint32_t* knn, bool reset,
                       unsigned long long* fc, unsigned* overflow, unsigned* uncert, bool fp32 = false,
                       unsigned* reclip = nullptr, const uint32_t* slots = nullptr, const uint16_t* kq = nullptr,
-                      bool pruned = false) {
+                      bool pruned = false, bool thread2d = false) {
     const int D = c->prm.dim;
     cudaError_t e = cudaSuccess;
     DevScalars* sc = (DevScalars*)c->scalars.p;
@@ -1635,7 +1897,9 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
         const unsigned blocks = (unsigned)((nq + CLIP_WARPS - 1) / CLIP_WARPS);
         const int CW = c->tune.clip_warps;  // cells (warps) per block: autotuned, 2 or 4
         const unsigned blocks_cw = (unsigned)((nq + CW - 1) / CW);
-        if (pruned) {
+        if (thread2d && D == 2 && !slots) {
+            k_clip2t<<<(unsigned)((nq + T2_THREADS - 1) / T2_THREADS), T2_THREADS, 0, c->stream>>>(P);
+        } else if (pruned) {
             const SubGrid g = {(const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
                                (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
                                (const uint32_t*)c->sub_start.p};
@@ -1708,12 +1972,13 @@ cudaError_t launch_clip(pgpu_ctx* c) {
         unsigned of = 0, unc = 0, rc = 0;
         const bool fp32 = c->prm.precision == PGPU_CLIP_FP32;
         const uint16_t* kq = c->use_kq ? (const uint16_t*)c->kq.p : nullptr;
+        // 2D: a thread per cell when the autotuner chose it (cells beyond its capacity come back as RECLIP)
         if ((e = clip_pass(c, (const uint32_t*)c->qs.p, c->n_query, c->knn_stride, (const uint32_t*)c->knn.p, true, &fc,
-                           &of, &unc, fp32, &rc, nullptr, kq)))
+                           &of, &unc, fp32, &rc, nullptr, kq, false, c->tune.clip_thread && D == 2)))
             return e;
         c->n_reclip = rc;
         if (!of && rc > 0) {
-            // cells the FP32 clip could not decide: the FP64 kernel, faces appended
+            // cells the FP32 clip could not decide (or too big for a thread): the FP64 warp kernel, faces appended
             uint32_t* fq = ensure<uint32_t>(c->fb_qs, c->n_query + 1, &e);
             if (e) return e;
             uint32_t nr = 0;

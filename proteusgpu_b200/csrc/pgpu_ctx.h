@@ -93,6 +93,7 @@ struct Tuning {
     double ppb = 2.0;    // mean points per coarse grid bin
     int knn_warps = 4;   // queries (warps) per KNN block: 2, 4 or 8
     int clip_warps = 4;  // cells (warps) per clipping block: 2 or 4
+    bool clip_thread = false;  // 2D: one thread per cell instead of one warp
 };
 
 struct KBudget {

@@ -35,3 +35,41 @@ def test_autotune_is_cached_per_workload_class():
     assert again["from_cache"] == 1
     assert (again["ppb"], again["knn_warps"], again["clip_warps"]) == (first["ppb"], first["knn_warps"],
                                                                         first["clip_warps"])
+
+
+def _mesh2d(pts, k, shapes, **kw):
+    with Context(dim=2, k=k, gamma=1.4, **kw) as ctx:
+        if shapes:
+            ctx.set_tuning(**shapes)
+        return ctx.compute_periodic_mesh(pts)
+
+
+@pytest.mark.parametrize("case", ["sod", "uniform_k16", "kh"])
+def test_thread_per_cell_2d_equals_warp_per_cell(case):
+    """The 2D thread-per-cell clip gives the warp kernel's mesh bit for bit, including
+    failing cells (uniform points at K = 16) and cells handed back for being too big."""
+    if case == "sod":
+        pts, k = ics.sod_2d().pos, 16
+    elif case == "uniform_k16":
+        pts, k = ics.uniform_points(20000, 2, 31), 16
+    else:
+        pts, k = ics.kh_2d(n_side=150, seed=3).pos, 32
+    a = _mesh2d(pts, k, None)
+    b = _mesh2d(pts, k, dict(clip_thread=True))
+    for f in ("status", "cert_k", "face_counts", "neighbor", "normal", "area", "volumes", "centroid", "seeds"):
+        assert np.array_equal(getattr(a, f), getattr(b, f)), f
+
+
+def test_thread_per_cell_2d_moving_mesh_and_batch():
+    B = ics.batch_2d(5, 21, 1000, 9000)
+    outs = []
+    for thread in (False, True):
+        with Context(dim=2, k=32, flux="physical", predicates="robust") as ctx:
+            ctx.set_tuning(clip_thread=thread)
+            ctx.batch_init(B.counts, B.buff, B.gamma, B.boundary, B.concat("pos"), B.concat("rho"),
+                           B.concat("vel"), B.concat("energy"), B.concat("deposit"))
+            for _ in range(3):
+                ctx.sim_step(0.3)
+            outs.append(ctx.sim_get())
+    for u, v in zip(*outs):
+        assert np.array_equal(u, v)
