@@ -354,7 +354,7 @@ def run_ours(args, rank, world, local_rank):
         forms[f] = {"value": rate(r), "ms_per_step": r["ms"] / args.steps,
                     "stages_ms": dict(zip(STAGES, r["stage"])), "reclip_cells": r["stats"]["reclip_cells"],
                     "speedup_vs_plain": rate(r) / rate(base),
-                    "tuning": {k: r["tuning"][k] for k in ("ppb", "knn_warps", "clip_warps", "clip_thread",
+                    "tuning": {k: r["tuning"][k] for k in ("ppb", "knn_warps", "clip_warps", "clip_thread", "knn_thread",
                                                            "ms_default", "ms_tuned")}}
         if r["kbudget"]:
             kb = r["kbudget"]

@@ -238,7 +238,8 @@ int pgpu_batch_dt(pgpu_ctx *ctx, double *dt_per_instance);
 /* -------------------------------------------------------- autotuner ---
  * Extension.  Times mesh builds of the current simulation state (nothing
  * advances) and picks the coarse grid's mean points per bin (1.5, 2, 3, 4), the
- * KNN block size (2, 4, 8 queries) and the clipping block size (2, 4 cells; in 2D
+ * KNN block size (2, 4, 8 queries; or one thread per query for the queries whose
+ * K is at most 32 or 64) and the clipping block size (2, 4 cells; in 2D
  * also one thread per cell instead of one warp), one
  * after the other; the choice is cached for the process by (dim, log2 n, batch,
  * precision, learned K, k) and reused without timing.  Results do not depend on
@@ -247,12 +248,13 @@ typedef struct {
     double ppb;
     int32_t knn_warps, clip_warps;
     int32_t clip_thread;         /* 2D: one thread per cell chosen over one warp per cell */
+    int32_t knn_thread;          /* 0, 32 or 64: queries with K <= this are searched one per thread */
     float ms_default, ms_tuned;  /* ghosts + sort + KNN + clip of one build, before and after */
     int32_t from_cache;
 } pgpu_tuning;
 int pgpu_autotune(pgpu_ctx *ctx, pgpu_tuning *out);
 /* Sets the launch shapes directly (ppb in [0.5, 64], knn_warps 2/4/8, clip_warps 2/4,
- * clip_thread 0/1; the timing fields are ignored). */
+ * clip_thread 0/1, knn_thread 0/32/64; the timing fields are ignored). */
 int pgpu_set_tuning(pgpu_ctx *ctx, const pgpu_tuning *t);
 
 /* ------------------------------------------- learned neighbour budget ---

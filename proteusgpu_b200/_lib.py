@@ -57,7 +57,7 @@ BOUNDARY = {"periodic": 0, "reflective": 1}
 
 class Tuning(C.Structure):
     _fields_ = [("ppb", C.c_double), ("knn_warps", C.c_int32), ("clip_warps", C.c_int32),
-                ("clip_thread", C.c_int32), ("ms_default", C.c_float), ("ms_tuned", C.c_float),
+                ("clip_thread", C.c_int32), ("knn_thread", C.c_int32), ("ms_default", C.c_float), ("ms_tuned", C.c_float),
                 ("from_cache", C.c_int32)]
 KB_NPARAM = 1542  # W1[32][8], b1[32], W2[32][32], b2[32], W3[6][32], b3[6]
 

@@ -221,9 +221,11 @@ class Context:
         check(self._h, self._L.pgpu_autotune(self._h, C.byref(t)), "pgpu_autotune")
         return {f: getattr(t, f) for f, _ in t._fields_}
 
-    def set_tuning(self, ppb: float = 2.0, knn_warps: int = 4, clip_warps: int = 4, clip_thread: bool = False):
+    def set_tuning(self, ppb: float = 2.0, knn_warps: int = 4, clip_warps: int = 4, clip_thread: bool = False,
+                   knn_thread: int = 0):
         """Launch shapes set directly (what pgpu_autotune would pick)."""
-        t = _lib.Tuning(ppb=ppb, knn_warps=knn_warps, clip_warps=clip_warps, clip_thread=int(clip_thread))
+        t = _lib.Tuning(ppb=ppb, knn_warps=knn_warps, clip_warps=clip_warps, clip_thread=int(clip_thread),
+                        knn_thread=int(knn_thread))
         check(self._h, self._L.pgpu_set_tuning(self._h, C.byref(t)), "pgpu_set_tuning")
 
     def batch_dt(self) -> np.ndarray:

@@ -806,14 +806,20 @@ static TuneKey tune_key(const pgpu_ctx* c) {
 
 // One mesh build of the current simulation state with stage timing; returns the
 // summed stage times selected by mask (bit i: stage i of ghosts, sort, knn, clip).
+// The faster of two builds: the first one of a new shape also pays for loading
+// its kernels and growing buffers.
 static int timed_build(pgpu_ctx* c, unsigned mask, float* ms) {
-    int r = build_mesh(c, c->n_hydro, false, false);
-    if (r) return r;
-    collect_times(c);
-    float t = 0.0f;
-    for (int i = 0; i < 4; i++)
-        if (mask & (1u << i)) t += c->stage_ms[i];
-    *ms = t;
+    float best = 1e30f;
+    for (int rep = 0; rep < 2; rep++) {
+        int r = build_mesh(c, c->n_hydro, false, false);
+        if (r) return r;
+        collect_times(c);
+        float t = 0.0f;
+        for (int i = 0; i < 4; i++)
+            if (mask & (1u << i)) t += c->stage_ms[i];
+        best = std::min(best, t);
+    }
+    *ms = best;
     return PGPU_OK;
 }
 
@@ -848,14 +854,21 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
             if (t < bt) bt = t, best.ppb = ppb;
         }
         c->tune.ppb = best.ppb;
-        // 2. KNN block size
+        // 2. KNN block size, then one thread per query for the small K
         bt = 1e30f;
+        c->tune.knn_thread = 0;
         for (int kw : {2, 4, 8}) {
             c->tune.knn_warps = kw;
             if ((r = timed_build(c, 0x4, &t))) return r;
-            if (t < bt) bt = t, best.knn_warps = kw;
+            if (t < bt) bt = t, best.knn_warps = kw, best.knn_thread = 0;
         }
         c->tune.knn_warps = best.knn_warps;
+        for (int kt : {32, 64}) {
+            c->tune.knn_thread = kt;
+            if ((r = timed_build(c, 0x4, &t))) return r;
+            if (t < bt) bt = t, best.knn_thread = kt;
+        }
+        c->tune.knn_thread = best.knn_thread;
         // 3. clipping: a warp per cell with 2 or 4 cells per block, or (2D) a thread per cell
         bt = 1e30f;
         for (int cw : {2, 4}) {
@@ -882,6 +895,7 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
     res.knn_warps = c->tune.knn_warps;
     res.clip_warps = c->tune.clip_warps;
     res.clip_thread = c->tune.clip_thread ? 1 : 0;
+    res.knn_thread = c->tune.knn_thread;
     if (out) *out = res;
     return PGPU_OK;
 }
@@ -890,12 +904,14 @@ int pgpu_set_tuning(pgpu_ctx* c, const pgpu_tuning* t) {
     int r = check_ctx(c);
     if (r) return r;
     if (!t || !(t->ppb >= 0.5 && t->ppb <= 64.0) || (t->knn_warps != 2 && t->knn_warps != 4 && t->knn_warps != 8) ||
-        (t->clip_warps != 2 && t->clip_warps != 4))
+        (t->clip_warps != 2 && t->clip_warps != 4) ||
+        (t->knn_thread != 0 && t->knn_thread != 32 && t->knn_thread != 64))
         return fail(c, PGPU_EINVAL, "pgpu_set_tuning: bad launch shapes");
     c->tune.ppb = t->ppb;
     c->tune.knn_warps = t->knn_warps;
     c->tune.clip_warps = t->clip_warps;
     c->tune.clip_thread = t->clip_thread != 0;
+    c->tune.knn_thread = t->knn_thread;
     return PGPU_OK;
 }
 

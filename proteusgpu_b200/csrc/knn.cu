@@ -260,7 +260,7 @@ __global__ void __launch_bounds__(KW * 32)
     k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
           const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
           int K, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
-          unsigned long long* __restrict__ cand_counter) {
+          unsigned long long* __restrict__ cand_counter, int skip_upto) {
     __shared__ WarpKnn S_all[KW];
     using PT = typename PointOf<D>::type;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -268,6 +268,7 @@ __global__ void __launch_bounds__(KW * 32)
     if (t >= nq) return;  // warp-uniform
     WarpKnn& S = S_all[w];
     if (kq) K = kq[t];
+    if (K <= skip_upto) return;  // done by k_knn_t
     const int nrows = (K + 31) >> 5;
     for (int r = 0; r < nrows; r++) {
         S.row_d[r * 32 + lane] = CUDART_INF;
@@ -363,6 +364,138 @@ __global__ void __launch_bounds__(KW * 32)
     if (cand_counter && lane == 0) atomicAdd(cand_counter, ncand);
 }
 
+// Thread-per-query variant for small K (<= KT): the same bins in the same order,
+// pruned against the running K-th key, the K best kept sorted in the thread's own
+// list by insertion.  Pruning only drops boxes that cannot hold a key below the
+// final K-th, so the list equals the warp kernel's.  Queries with a larger K return
+// at once here and are done by k_knn, which skips the ones done here.
+// The lists live in shared memory, entry i of thread t at [i * KNN_T_THREADS + t]
+// (conflict-free; per-thread local arrays of this size spill out of L1).
+constexpr int KNN_T_THREADS = 64;
+
+// Dynamic shared memory: kcap * KNN_T_THREADS doubles, then as many u32, with
+// kcap = min(Kall, KT) (at most 48 KB).
+template <int D>
+__global__ void __launch_bounds__(KNN_T_THREADS)
+    k_knn_t(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
+            const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
+            int Kall, int KT, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
+            unsigned long long* __restrict__ cand_counter) {
+    using PT = typename PointOf<D>::type;
+    extern __shared__ __align__(16) unsigned char knn_t_smem[];
+    const int kcap = min(Kall, KT);
+    double* kd = (double*)knn_t_smem + threadIdx.x;
+    uint32_t* ki = (uint32_t*)(knn_t_smem + (size_t)kcap * KNN_T_THREADS * sizeof(double)) + threadIdx.x;
+    constexpr int S = KNN_T_THREADS;
+    const int64_t t = (int64_t)blockIdx.x * KNN_T_THREADS + threadIdx.x;
+    unsigned long long ncand = 0;
+    if (t < nq) {
+        const int K = kq ? (int)kq[t] : Kall;
+        if (K <= kcap) {  // the rest: k_knn
+            int cnt = 0;
+            double thr_d = CUDART_INF;  // the K-th key once K are held, else (inf, none)
+            uint32_t thr_i = NO_NEIGHBOR;
+            const uint32_t s = qs[t];
+            const PT p = spts[s];
+            const uint32_t qid = perm[s];
+            if (isfinite(p.x) && isfinite(p.y) && isfinite(pz(p))) {
+                const double pc[3] = {p.x, p.y, pz(p)};
+                const InstPar& ipq = grid.ip[grid.inst[qid]];
+                const int G0 = ipq.G;
+                const uint32_t slot0 = ipq.slot0;
+                const int Lq = grid.lvl[slot0 + morton<D>(bin_coord(p.x, G0), bin_coord(p.y, G0),
+                                                          D == 3 ? bin_coord(pz(p), G0) : 0)];
+                const int G = G0 << Lq;
+                const int bc[3] = {sub_coord(p.x, G0, Lq), sub_coord(p.y, G0, Lq),
+                                   D == 3 ? sub_coord(pz(p), G0, Lq) : 0};
+                const double h = 1.0 / (double)G;
+                auto full = [&]() { return cnt >= K; };  // thr_* then hold the K-th key
+                auto scan_range = [&](uint32_t bstart, uint32_t bcnt) {
+                    ncand += bcnt;
+                    for (uint32_t q = bstart; q < bstart + bcnt; q++) {
+                        const uint32_t eid = perm[q];
+                        if (eid == qid) continue;
+                        const PT c = spts[q];
+                        const double ddx = p.x - c.x, ddy = p.y - c.y;
+                        double d2;
+                        if (D == 2) {
+                            d2 = ddx * ddx + ddy * ddy;
+                        } else {
+                            const double ddz = pz(p) - pz(c);
+                            d2 = ddx * ddx + ddy * ddy + ddz * ddz;
+                        }
+                        // the warp kernel's test: against (inf, none) until K are held (drops NaN)
+                        if (!key_less(d2, eid, thr_d, thr_i)) continue;
+                        int i = cnt < K ? cnt : K - 1;
+                        while (i > 0) {
+                            const double od = kd[(i - 1) * S];
+                            const uint32_t oi = ki[(i - 1) * S];
+                            if (!key_less(d2, eid, od, oi)) break;
+                            kd[i * S] = od;
+                            ki[i * S] = oi;
+                            i--;
+                        }
+                        kd[i * S] = d2;
+                        ki[i * S] = eid;
+                        if (cnt < K) cnt++;
+                        if (cnt == K) {
+                            thr_d = kd[(K - 1) * S];
+                            thr_i = ki[(K - 1) * S];
+                        }
+                    }
+                };
+                // 1. offsets in order of their lower bound
+                for (int ci = 0; ci < table_n; ci++) {
+                    const int2 ent = table[ci];
+                    if (full() && (double)ent.y * h * h * (1.0 - 1e-12) > thr_d) break;
+                    const int dx = (int)(signed char)(ent.x & 255), dy = (int)(signed char)((ent.x >> 8) & 255),
+                              dz = (int)(signed char)((ent.x >> 16) & 255);
+                    const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
+                    if (!(x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G)))) continue;
+                    if (full() && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) continue;
+                    uint32_t bstart, bcnt;
+                    if (box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) scan_range(bstart, bcnt);
+                }
+                // 2. beyond the table: Chebyshev rings
+                for (int r = table_r + 1;; r++) {
+                    double lb = CUDART_INF;
+                    bool all = true;
+                    for (int a = 0; a < D; a++) {
+                        const int lo = bc[a] - (r - 1), hi = bc[a] + (r - 1);
+                        if (lo > 0) {
+                            all = false;
+                            lb = fmin(lb, pc[a] - (double)lo * h);
+                        }
+                        if (hi < G - 1) {
+                            all = false;
+                            lb = fmin(lb, (double)(hi + 1) * h - pc[a]);
+                        }
+                    }
+                    if (all || r > G + 1) break;
+                    if (full() && lb > 0.0 && thr_d < lb * lb * (1.0 - 1e-12)) break;
+                    const int w1 = 2 * r + 1;
+                    const int ncube = D == 2 ? w1 * w1 : w1 * w1 * w1;
+                    for (int ci = 0; ci < ncube; ci++) {
+                        const int dx = ci % w1 - r, rest = ci / w1;
+                        const int dy = rest % w1 - r, dz = D == 3 ? rest / w1 - r : 0;
+                        if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
+                        const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
+                        if (!(x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G)))) continue;
+                        if (full() && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) continue;
+                        uint32_t bstart, bcnt;
+                        if (box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) scan_range(bstart, bcnt);
+                    }
+                }
+            }
+            for (int i = 0; i < K; i++) out[t * stride + i] = i < cnt ? ki[i * S] : NO_NEIGHBOR;
+        }
+    }
+    if (cand_counter) {
+        for (int o = 16; o > 0; o >>= 1) ncand += __shfl_xor_sync(FULL, ncand, o);
+        if ((threadIdx.x & 31) == 0 && ncand) atomicAdd(cand_counter, ncand);
+    }
+}
+
 }  // namespace
 
 // Offset table: every (dx, dy, dz) with |d|_inf <= R, sorted by the lower bound
@@ -409,22 +542,42 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
     if (c->knn_table_n == 0 && (e = build_knn_table(c))) return e;
     DevScalars* sc = (DevScalars*)c->scalars.p;
     const int KW = c->tune.knn_warps;  // warps (queries) per block: autotuned, 2, 4 or 8
+    const int KT = c->tune.knn_thread;  // queries with K <= KT: one thread each (0 = none)
+    const bool all_small = KT > 0 && K <= KT;  // K bounds every per-query kq
     const unsigned blocks = (unsigned)((nq + KW - 1) / KW);
     const uint32_t* perm = (const uint32_t*)c->perm.p;
     const SubGrid grid = {(const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p,
                           (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
                           (const uint32_t*)c->sub_start.p};
     const int2* tab = (const int2*)c->knn_table.p;
+    int launches = 0;
+    if (KT > 0) {
+        const unsigned tblocks = (unsigned)((nq + KNN_T_THREADS - 1) / KNN_T_THREADS);
+        const size_t smem = (size_t)std::min(K, KT) * KNN_T_THREADS * (sizeof(double) + sizeof(uint32_t));
+#define PGPU_KNN_T(DD, PT)                                                                                    \
+    k_knn_t<DD><<<tblocks, KNN_T_THREADS, smem, c->stream>>>((const PT*)c->spts.p, perm, grid, tab,            \
+                                                              c->knn_table_n, c->knn_table_r, qs, nq, K, KT, kq, \
+                                                              stride, out, &sc->knn_cand)
+        if (c->prm.dim == 2) PGPU_KNN_T(2, double2); else PGPU_KNN_T(3, double4);
+#undef PGPU_KNN_T
+        launches++;
+        if (all_small) {
+            count_launches(launches);
+            return cudaGetLastError();
+        }
+    }
+    const int skip = KT > 0 ? std::min(K, KT) : 0;  // the queries k_knn_t did
 #define PGPU_KNN(DD, PT, WW)                                                                                 \
     k_knn<DD, WW><<<blocks, WW * 32, 0, c->stream>>>((const PT*)c->spts.p, perm, grid, tab, c->knn_table_n,     \
-                                                      c->knn_table_r, qs, nq, K, kq, stride, out, &sc->knn_cand)
+                                                      c->knn_table_r, qs, nq, K, kq, stride, out, &sc->knn_cand, \
+                                                      skip)
     if (c->prm.dim == 2) {
         if (KW == 2) PGPU_KNN(2, double2, 2); else if (KW == 8) PGPU_KNN(2, double2, 8); else PGPU_KNN(2, double2, 4);
     } else {
         if (KW == 2) PGPU_KNN(3, double4, 2); else if (KW == 8) PGPU_KNN(3, double4, 8); else PGPU_KNN(3, double4, 4);
     }
 #undef PGPU_KNN
-    count_launches(1);
+    count_launches(launches + 1);
     return cudaGetLastError();
 }
 

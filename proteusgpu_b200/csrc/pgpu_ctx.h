@@ -94,6 +94,7 @@ struct Tuning {
     int knn_warps = 4;   // queries (warps) per KNN block: 2, 4 or 8
     int clip_warps = 4;  // cells (warps) per clipping block: 2 or 4
     bool clip_thread = false;  // 2D: one thread per cell instead of one warp
+    int knn_thread = 0;        // queries with K <= 32 or 64 searched one per thread (0 = none)
 };
 
 struct KBudget {

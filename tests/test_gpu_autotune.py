@@ -22,6 +22,7 @@ def test_autotuned_shapes_give_identical_steps(precision):
     _, ref, mref = _run(ic, False, precision)
     t, got, mgot = _run(ic, True, precision)
     assert t["ppb"] in (1.5, 2.0, 3.0, 4.0) and t["knn_warps"] in (2, 4, 8) and t["clip_warps"] in (2, 4)
+    assert t["knn_thread"] in (0, 32, 64)
     assert t["ms_tuned"] > 0 and t["ms_default"] > 0
     for a, b in zip(ref, got):
         assert np.array_equal(a, b)
@@ -65,7 +66,7 @@ def test_thread_per_cell_2d_moving_mesh_and_batch():
     outs = []
     for thread in (False, True):
         with Context(dim=2, k=32, flux="physical", predicates="robust") as ctx:
-            ctx.set_tuning(clip_thread=thread)
+            ctx.set_tuning(clip_thread=thread, knn_thread=32 if thread else 0)
             ctx.batch_init(B.counts, B.buff, B.gamma, B.boundary, B.concat("pos"), B.concat("rho"),
                            B.concat("vel"), B.concat("energy"), B.concat("deposit"))
             for _ in range(3):

@@ -146,3 +146,19 @@ def test_every_proposal_rejected_still_gives_the_plain_mesh():
     starved = _sim(ic, 190, 0.1, 4, True, quantile=1e-6)
     _same(starved, plain)
     assert starved[5][-1]["misses"] > 0
+
+
+def test_learned_k_with_thread_per_query_knn():
+    """Per-query K from 32 to 128 split between the thread kernel (K <= 64) and
+    the warp kernel (the rest) in one search: the steps still equal the plain ones."""
+    ic = ics.sedov_3d(n=20000, seed=14)
+    plain = _sim(ic, 190, 0.1, 4, False)
+    with Context(dim=3, k=190, buff=0.1, flux="physical", gamma=ic.gamma, precision="fp32") as ctx:
+        ctx.set_tuning(knn_thread=64)
+        ctx.kbudget_enable(train_steps=2, iters_per_step=48, quantile=0.99, seed=3)
+        ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+        for _ in range(4):
+            ctx.sim_step(0.3)
+        mesh = ctx.download_mesh()
+        got = ctx.sim_get() + (mesh,)
+    _same(got, plain)

@@ -90,3 +90,38 @@ def test_knn_many_duplicates_in_one_bin():
     with Context(dim=3, k=32) as ctx:
         g = ctx.knn(pts)
     assert np.array_equal(g, om.knn(pts, 32))
+
+
+def _knn_thread(pts, k, kt):
+    with Context(dim=pts.shape[1], k=k) as ctx:
+        ctx.set_tuning(knn_thread=kt)
+        return ctx.knn(pts)
+
+
+@pytest.mark.parametrize("case,k,kt", [("uniform2", 16, 32), ("uniform2", 32, 32), ("uniform2", 48, 64),
+                                       ("uniform3", 64, 64), ("uniform3", 100, 64), ("blob3", 64, 64),
+                                       ("blob2", 32, 32), ("lattice2", 24, 32), ("dups3", 20, 32),
+                                       ("few3", 16, 32)])
+def test_knn_thread_per_query(case, k, kt):
+    """One thread per query (the small-K kernel) gives the warp kernel's lists: the
+    same exact K nearest with ties by index, over refined bins, grid-line points,
+    duplicates and fewer points than K."""
+    rng = np.random.default_rng(sum(map(ord, case)) + k)
+    if case == "uniform2":
+        pts = ics.uniform_points(6000, 2, 50 + k)
+    elif case == "uniform3":
+        pts = ics.uniform_points(9000, 3, 50 + k)
+    elif case == "blob3":
+        pts = _dense_blob(30000, 8000, 3, 0.002, 14)
+    elif case == "blob2":
+        pts = _dense_blob(30000, 8000, 2, 0.001, 13)
+    elif case == "lattice2":
+        g1 = np.arange(40) / 2048 + 0.25
+        lat = np.stack(np.meshgrid(g1, g1, indexing="ij"), -1).reshape(-1, 2)
+        pts = np.ascontiguousarray(np.concatenate([lat, rng.random((3000, 2))]))
+    elif case == "dups3":
+        base = rng.random((500, 3))
+        pts = np.ascontiguousarray(np.concatenate([base, base[:100]]))
+    else:
+        pts = ics.uniform_points(10, 3, 3)
+    assert np.array_equal(_knn_thread(pts, k, kt), om.knn(pts, k))
