@@ -353,6 +353,9 @@ def run_ours(args, rank, world, local_rank):
     for f, r in res.items():
         forms[f] = {"value": rate(r), "ms_per_step": r["ms"] / args.steps,
                     "stages_ms": dict(zip(STAGES, r["stage"])), "reclip_cells": r["stats"]["reclip_cells"],
+                    "clip_split_ms": dict(zip(("main_clip", "fallback", "grid_walk"),
+                                              r["stats"]["clip_split_ms"])),
+                    "walked_cells": r["stats"]["pruned_cells"],
                     "speedup_vs_plain": rate(r) / rate(base),
                     "tuning": {k: r["tuning"][k] for k in ("ppb", "knn_warps", "clip_warps", "clip_thread", "knn_thread",
                                                            "ms_default", "ms_tuned")}}

@@ -214,6 +214,9 @@ typedef struct {
     int64_t pruned_cells;       /* moving-mesh steps: hydro cells whose certificate needed more than the
                                    neighbour budget(s), clipped by walking the grid instead (extension) */
     int64_t walk_points, walk_boxes; /* that walk's work: points clipped, grid boxes visited */
+    float clip_split_ms[3];     /* with timing on: the last build's clip stage as main clip (with the
+                                   FP64 re-clip), fallback KNN + clip, grid walk */
+    int32_t pad_;
 } pgpu_stats;
 
 /* Statistics of the last step (synchronises the stream). */

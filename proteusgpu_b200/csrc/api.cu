@@ -119,6 +119,7 @@ int build_mesh(pgpu_ctx* c, int64_t n, bool no_ghosts, bool all_cells) {
     CK(pgpu::launch_knn(c));
     mark(c, 3);
     CK(pgpu::launch_clip(c));
+    mark(c, 6);
     if (c->use_kq) {
         // proposals the certificate rejected: KNN and clipping again at the plain budget
         kb.cells = c->n_query;
@@ -132,12 +133,14 @@ int build_mesh(pgpu_ctx* c, int64_t n, bool no_ghosts, bool all_cells) {
         // cells whose certificate did not close within k: KNN and clipping again with the fallback budget
         CK(pgpu::launch_fallback(c, c->prm.k_fallback));
     }
+    mark(c, 7);
     c->n_pruned = 0;
     if (!all_cells) {
         // cells whose security sphere reaches past every budget (beside dense clumps), or that
         // failed otherwise: grid walk in the seed's local frame
         CK(pgpu::launch_pruned(c));
     }
+    mark(c, 8);
     if (kb_on && !kb.trained) {
         // a plain-method step: its certified K train the proposal
         CK(pgpu::kb_train_step(c));
@@ -161,6 +164,12 @@ void collect_times(pgpu_ctx* c) {
     for (int i = 0; i < 5; i++) {
         c->stage_ms[i] = 0.0f;
         if ((c->ev_mask >> i & 3u) == 3u) cudaEventElapsedTime(&c->stage_ms[i], c->ev[i], c->ev[i + 1]);
+    }
+    const int from[3] = {3, 6, 7};
+    for (int i = 0; i < 3; i++) {
+        c->clip_ms[i] = 0.0f;
+        if ((c->ev_mask >> from[i] & 1u) && (c->ev_mask >> (6 + i) & 1u))
+            cudaEventElapsedTime(&c->clip_ms[i], c->ev[from[i]], c->ev[6 + i]);
     }
 }
 
@@ -206,7 +215,7 @@ int pgpu_create(const pgpu_params* p, pgpu_ctx** out) {
     }
     cudaError_t e = pgpu::ensure_bytes(c->scalars, sizeof(DevScalars));
     if (e == cudaSuccess) e = cudaMemsetAsync(c->scalars.p, 0, sizeof(DevScalars), c->stream);
-    for (int i = 0; i < 6 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
+    for (int i = 0; i < 9 && e == cudaSuccess; i++) e = cudaEventCreate(&c->ev[i]);
     if (e != cudaSuccess) {
         pgpu_destroy(c);
         return PGPU_ECUDA;
@@ -229,7 +238,7 @@ void pgpu_destroy(pgpu_ctx* c) {
                       &c->kb.feat, &c->kb.hist_vol, &c->kb.miss, &c->kb.ksum, &c->kb.labels, &c->kb.tmp_out,
                       &c->bin_lvl, &c->sub_off, &c->sub_cnt, &c->sub_start};
     for (DevBuf* b : bufs) free_buf(*b);
-    for (int i = 0; i < 6; i++)
+    for (int i = 0; i < 9; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
@@ -688,6 +697,7 @@ int pgpu_sim_stats(pgpu_ctx* c, pgpu_stats* out) {
     out->pruned_cells = c->n_pruned;
     out->walk_points = (int64_t)h.walk_points;
     out->walk_boxes = (int64_t)h.walk_boxes;
+    for (int i = 0; i < 3; i++) out->clip_split_ms[i] = c->clip_ms[i];
     return PGPU_OK;
 }
 

@@ -439,6 +439,84 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
     }
 }
 
+// Cavity boundary of a 3D cut: the removed vertices are the triangles flagged in
+// cm (nb_r of nb_t); a boundary edge is an edge of a removed triangle whose twin
+// triangle is kept.  Each gives a new vertex (cur, x, y), staged in the order of
+// the removed vertices and then of their three edges.  The removed triangles are
+// first listed in order; with at most 32 of their edges, an edge is interior when
+// its undirected key occurs twice (once per adjacent triangle, __match_any_sync),
+// else the directed edges are marked in the per-plane rows of emask.  Returns the
+// number of new vertices; src gets the OR of their first planes and, with
+// WANT_NXT, nxt[x] = y (for the FP64 kernel's cycle check).
+template <bool WANT_NXT>
+__device__ __forceinline__ int cavity_boundary3(WarpCell& W, int lane, const uint32_t (&cm)[3], int nb_t, int nb_r,
+                                                uint32_t cur, unsigned long long& src) {
+    uint32_t* rl = reinterpret_cast<uint32_t*>(W.u.b.stage_d2);  // removed triangles (scratch: MAX_T u32)
+    uint32_t* stage = W.u.b.stage;
+    unsigned long long* em = W.u.b.emask;
+    int before = 0;
+#pragma unroll
+    for (int j = 0; j < 3; j++) {
+        const int i = lane + 32 * j;
+        if (i < nb_t && ((cm[j] >> lane) & 1u)) rl[before + __popc(cm[j] & ((1u << lane) - 1u))] = W.tri[i];
+        before += __popc(cm[j]);
+    }
+    __syncwarp();
+    const int ne = 3 * nb_r;
+    const bool by_match = ne <= 32;
+    if (!by_match) {
+        for (int q = lane; q < ne; q += 32) {
+            const int r = q / 3, ed = q - 3 * r;
+            const uint32_t tv = rl[r];
+            const uint32_t x = (tv >> (8 * ed)) & 255u, y = (tv >> (8 * (ed == 2 ? 0 : ed + 1))) & 255u;
+            atomicOr(&em[x], 1ull << y);
+        }
+        __syncwarp();
+    }
+    int base = 0;
+    uint32_t slo = 0u, shi = 0u;
+    for (int c0 = 0; c0 < ne; c0 += 32) {
+        const int q = c0 + lane;
+        const bool valid = q < ne;
+        uint32_t x = 0u, y = 0u;
+        if (valid) {
+            const int r = q / 3, ed = q - 3 * r;
+            const uint32_t tv = rl[r];
+            x = (tv >> (8 * ed)) & 255u;
+            y = (tv >> (8 * (ed == 2 ? 0 : ed + 1))) & 255u;
+        }
+        bool isb;
+        if (by_match) {
+            // every lane takes part in the match (lanes without an edge carry a unique key)
+            const uint32_t key = valid ? ((min(x, y) << 8) | max(x, y)) : (0x10000u | (uint32_t)lane);
+            const unsigned same = __match_any_sync(FULL, key);
+            isb = valid && __popc(same) == 1;
+        } else {
+            isb = valid && !((em[y] >> x) & 1ull);
+        }
+        const unsigned bal = __ballot_sync(FULL, isb);
+        if (isb) {
+            const int pos = base + __popc(bal & ((1u << lane) - 1u));
+            if (pos < MAX_P) stage[pos] = pack3(cur, x, y);
+            if (x < 32u) slo |= 1u << x; else shi |= 1u << (x - 32u);
+            if (WANT_NXT) W.u.b.nxt[x] = (unsigned char)y;
+        }
+        base += __popc(bal);
+    }
+    slo = __reduce_or_sync(FULL, slo);
+    shi = __reduce_or_sync(FULL, shi);
+    src = ((unsigned long long)shi << 32) | slo;
+    if (!by_match) {
+        __syncwarp();
+        for (int q = lane; q < ne; q += 32) {
+            const int r = q / 3, ed = q - 3 * r;
+            em[(rl[r] >> (8 * ed)) & 255u] = 0ull;
+        }
+    }
+    __syncwarp();
+    return base;
+}
+
 // One step of ConvexCell::clip_by_plane (cell.cpp:120-205) in FP64: the
 // bisector of the seed and ext point z = (bx, by, bz).  CLIP_FAIL sets status
 // (and the vertex distance the final certificate uses); CLIP_NONE leaves the
@@ -541,46 +619,9 @@ __device__ __forceinline__ int clip_by(WarpCell& W, int lane, uint32_t z, double
             }
         }
     } else {
-        unsigned long long* em = W.u.b.emask;
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            int i = lane + 32 * j;
-            if (i < nb_t && ((cm[j] >> lane) & 1u)) {
-                uint32_t tv = W.tri[i];
-                uint32_t a = tri_a(tv), b = tri_b(tv), c = tri_c(tv);
-                atomicOr(&em[a], 1ull << b);
-                atomicOr(&em[b], 1ull << c);
-                atomicOr(&em[c], 1ull << a);
-            }
-        }
-        __syncwarp();
         unsigned long long src = 0ull;
-        int base = 0;
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            int i = lane + 32 * j;
-            bool rem = i < nb_t && ((cm[j] >> lane) & 1u);
-            uint32_t tv = rem ? W.tri[i] : 0u;
-            uint32_t v3[3] = {tri_a(tv), tri_b(tv), tri_c(tv)};
-#pragma unroll
-            for (int ed = 0; ed < 3; ed++) {
-                uint32_t x = v3[ed], y = v3[(ed + 1) % 3];
-                bool isb = rem && !((em[y] >> x) & 1ull);
-                unsigned bal = __ballot_sync(FULL, isb);
-                if (isb) {
-                    const int pos = base + __popc(bal & ((1u << lane) - 1u));
-                    if (pos < MAX_P) stage[pos] = pack3(cur, x, y);
-                    src |= 1ull << x;
-                    W.u.b.nxt[x] = (unsigned char)y;
-                }
-                base += __popc(bal);
-            }
-        }
-        n_new = base;
-        // OR-reduce the source planes; a simple cycle visits each source once
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) src |= __shfl_xor_sync(FULL, src, o);
-        __syncwarp();
+        n_new = cavity_boundary3<true>(W, lane, cm, nb_t, nb_r, (uint32_t)cur, src);
+        // a simple cycle visits each source plane once
         bool ok = __popcll(src) == n_new && n_new >= 3;
         if (ok && lane == 0) {
             int x0 = __ffsll((long long)src) - 1, x = x0;
@@ -595,18 +636,6 @@ __device__ __forceinline__ int clip_by(WarpCell& W, int lane, uint32_t z, double
         }
         ok = __shfl_sync(FULL, ok ? 1 : 0, 0) != 0;
         bad = !ok;
-        // clear the edge rows of removed vertices
-#pragma unroll
-        for (int j = 0; j < 3; j++) {
-            int i = lane + 32 * j;
-            if (i < nb_t && ((cm[j] >> lane) & 1u)) {
-                uint32_t tv = W.tri[i];
-                em[tri_a(tv)] = 0ull;
-                em[tri_b(tv)] = 0ull;
-                em[tri_c(tv)] = 0ull;
-            }
-        }
-        __syncwarp();
     }
     if (bad) {
         status = ST_INCONSISTENT_BOUNDARY;
@@ -1178,14 +1207,17 @@ __device__ __forceinline__ float warp_maxf(float v) {
     return v;
 }
 
+// The squared distances are >= +0 or NaN, so their bit patterns order as unsigned
+// integers (any NaN above every number): one integer max-reduction gives the
+// maximum, NaN when any is NaN.
 __device__ __forceinline__ float max_vd2f(const WarpCell& W, int n, int lane) {
-    float m = 0.0f;
+    uint32_t m = 0u;
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         const int i = lane + 32 * j;
-        if (i < n) m = nan_maxf(m, W.D32[i]);
+        if (i < n) m = max(m, __float_as_uint(W.D32[i]));
     }
-    return warp_maxf(m);
+    return __uint_as_float(__reduce_max_sync(FULL, m));
 }
 
 // The reference's FP64 plane p of the cell (box planes, or the bisector with
@@ -1275,33 +1307,34 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
     int k_stop = 0, k_last = 0;
     float v_dist = max_vd2f(W, nb_t, lane);
 
-    // neighbours are fetched 32 at a time, one per lane, and broadcast plane by plane
+    // neighbours are fetched 32 at a time, one per lane; each lane forms its
+    // neighbour's local-frame plane and distance, broadcast plane by plane
     uint32_t zc = NO_NEIGHBOR;
-    double cx = 0.0, cy = 0.0, cz = 0.0;
+    float cfx = 0.f, cfy = 0.f, cfz = 0.f, cfw = 0.f, cd2 = 0.f;
     for (int k = 0; k < K; k++) {
         if ((k & 31) == 0) {
             const int kk = k + lane;
             zc = kk < K ? kl[kk] : NO_NEIGHBOR;
             if (zc != NO_NEIGHBOR) {
                 const PT Bc = ext[zc];
-                cx = Bc.x;
-                cy = Bc.y;
-                cz = pz(Bc);
+                const double bx = Bc.x - sx, by = Bc.y - sy, bz = pz(Bc) - sz;  // local frame, exact in FP64
+                cfx = (float)bx;
+                cfy = (float)by;
+                cfz = (float)bz;
+                cfw = 0.5f * fmaf(cfx, cfx, fmaf(cfy, cfy, cfz * cfz));
+                cd2 = (float)seed_d2(Bc.x, Bc.y, pz(Bc), sx, sy, sz);
             }
         }
         const uint32_t z = __shfl_sync(FULL, zc, k & 31);
         if (z == NO_NEIGHBOR) break;
         k_stop = k + 1;
-        const double Bx = __shfl_sync(FULL, cx, k & 31), By = __shfl_sync(FULL, cy, k & 31),
-                     Bz = __shfl_sync(FULL, cz, k & 31);
-        const double bx = Bx - sx, by = By - sy, bz = Bz - sz;  // local frame, exact in FP64
-        const float fx = (float)bx, fy = (float)by, fz = (float)bz;
-        const double d2B = seed_d2(Bx, By, Bz, sx, sy, sz);
+        const float d2Bf = __shfl_sync(FULL, cd2, k & 31);
         if (nb_v >= MAX_P) {
             reclip = true;
             break;
         }
-        const float4 eq = make_float4(-fx, -fy, -fz, 0.5f * fmaf(fx, fx, fmaf(fy, fy, fz * fz)));
+        const float4 eq = make_float4(-__shfl_sync(FULL, cfx, k & 31), -__shfl_sync(FULL, cfy, k & 31),
+                                      -__shfl_sync(FULL, cfz, k & 31), __shfl_sync(FULL, cfw, k & 31));
         const int cur = nb_v;
         if (lane == 0) hp[cur] = eq;
         __syncwarp();
@@ -1326,7 +1359,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
         const int nb_r = __popc(cm[0]) + __popc(cm[1]) + __popc(cm[2]);
         const uint32_t km[3] = {~cm[0], ~cm[1], ~cm[2]};
         if (nb_r == 0) {
-            if ((float)d2B > 4.004f * v_dist) {
+            if (d2Bf > 4.004f * v_dist) {
                 certified = true;
                 break;
             }
@@ -1373,61 +1406,14 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
                 if (__any_sync(FULL, und)) bad = true;
             }
         } else {
-            unsigned long long* em = W.u.b.emask;
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                const int i = lane + 32 * j;
-                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
-                    const uint32_t tv = W.tri[i];
-                    const uint32_t a = tri_a(tv), b = tri_b(tv), c = tri_c(tv);
-                    atomicOr(&em[a], 1ull << b);
-                    atomicOr(&em[b], 1ull << c);
-                    atomicOr(&em[c], 1ull << a);
-                }
-            }
-            __syncwarp();
             unsigned long long src = 0ull;
-            int base = 0;
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                const int i = lane + 32 * j;
-                const bool rem = i < nb_t && ((cm[j] >> lane) & 1u);
-                const uint32_t tv = rem ? W.tri[i] : 0u;
-                const uint32_t v3[3] = {tri_a(tv), tri_b(tv), tri_c(tv)};
-#pragma unroll
-                for (int ed = 0; ed < 3; ed++) {
-                    const uint32_t x = v3[ed], y = v3[(ed + 1) % 3];
-                    const bool isb = rem && !((em[y] >> x) & 1ull);
-                    const unsigned bal = __ballot_sync(FULL, isb);
-                    if (isb) {
-                        const int pos = base + __popc(bal & ((1u << lane) - 1u));
-                        if (pos < MAX_P) stage[pos] = pack3(cur, x, y);
-                        src |= 1ull << x;
-                    }
-                    base += __popc(bal);
-                }
-            }
-            n_new = base;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) src |= __shfl_xor_sync(FULL, src, o);
-            __syncwarp();
+            n_new = cavity_boundary3<false>(W, lane, cm, nb_t, nb_r, (uint32_t)cur, src);
             // Every predicate that reached this point was decided beyond its error
             // bound, so the conflict set is the exact one and (no vertex lies on the
             // plane: that would have been undecided) the cavity boundary is one simple
             // cycle; the reference's walk (cell.cpp:262-300), which the FP64 kernel
             // replays, cannot fail here.  Each source plane appearing once is checked.
             bad = !(__popcll(src) == n_new && n_new >= 3);
-#pragma unroll
-            for (int j = 0; j < 3; j++) {
-                const int i = lane + 32 * j;
-                if (i < nb_t && ((cm[j] >> lane) & 1u)) {
-                    const uint32_t tv = W.tri[i];
-                    em[tri_a(tv)] = 0ull;
-                    em[tri_b(tv)] = 0ull;
-                    em[tri_c(tv)] = 0ull;
-                }
-            }
-            __syncwarp();
         }
         if (bad || kept + n_new >= MAX_T || n_new > MAX_P) {
             reclip = true;
@@ -1477,7 +1463,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
         nb_t = kept + n_new;
         __syncwarp();
         v_dist = max_vd2f(W, nb_t, lane);
-        if ((float)d2B > 4.004f * v_dist) {
+        if (d2Bf > 4.004f * v_dist) {
             certified = true;
             break;
         }

@@ -120,9 +120,10 @@ struct pgpu_ctx {
     cudaStream_t stream = nullptr;
     std::string err;
     bool timing = false;
-    cudaEvent_t ev[6] = {};
+    cudaEvent_t ev[9] = {};    // 0-5: stage boundaries; 6-8: after the main clip, the fallback, the walk
     unsigned ev_mask = 0;      // events recorded since the last build began
     float stage_ms[5] = {};
+    float clip_ms[3] = {};     // the clip stage split: main clip (+ re-clip), fallback, grid walk
 
     // sizes of the current mesh
     int64_t n_hydro = 0, n_ext = 0, num_faces = 0, n_query = 0;
