@@ -76,6 +76,8 @@ def parse():
     ap.add_argument("--skip-e2e", action="store_true", help="omit the end-to-end leg")
     ap.add_argument("--skip-forms", action="store_true",
                     help="time only the headline form and the plain baseline (not fp32_clip, learned_fp64)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="time only the headline form (profiling runs; no speed-up against the plain form)")
     return ap.parse_args()
 
 
@@ -227,9 +229,9 @@ FORMS = {
 }
 HEADLINE, BASELINE_FORM = "learned_fp32", "plain_fp64"
 
-# DRAM bytes per cell of one k_clip32 launch, from the ncu capture summarised in
-# profiles/k_clip32_clustered3d_1m.md (read + write / cells), used for `traffic`.
-CLIP32_DRAM_BYTES_PER_CELL = (713.581312e6 + 822.387968e6) / 1_048_576
+# DRAM bytes per cell of one k_clip32 launch (read + write / cells), from an ncu capture
+# of the clustered 1,048,576-cell case on learned-K lists, used for `traffic`.
+CLIP32_DRAM_BYTES_PER_CELL = (665.013248e6 + 770.234112e6) / 1_048_576
 
 
 def _barrier(dist):
@@ -333,7 +335,7 @@ def run_ours(args, rank, world, local_rank):
                                 device_id=torch.device("cuda", local_rank))
     ic = make_ic(cfg)
     n = ic.n
-    names = [BASELINE_FORM, HEADLINE] if args.skip_forms else list(FORMS)
+    names = [HEADLINE] if args.headline_only else [BASELINE_FORM, HEADLINE] if args.skip_forms else list(FORMS)
     res = {}
     for f in names:
         res[f] = time_form(args, cfg, ic, local_rank, dist, f, want_e2e=(f == HEADLINE and not args.skip_e2e),
@@ -347,7 +349,7 @@ def run_ours(args, rank, world, local_rank):
     def rate(r):
         return n * args.steps * world / (r["ms"] / 1e3)
 
-    head, base = res[HEADLINE], res[BASELINE_FORM]
+    head, base = res[HEADLINE], res.get(BASELINE_FORM)
     value = rate(head)
     forms = {}
     for f, r in res.items():
@@ -356,7 +358,7 @@ def run_ours(args, rank, world, local_rank):
                     "clip_split_ms": dict(zip(("main_clip", "fallback", "grid_walk"),
                                               r["stats"]["clip_split_ms"])),
                     "walked_cells": r["stats"]["pruned_cells"],
-                    "speedup_vs_plain": rate(r) / rate(base),
+                    "speedup_vs_plain": rate(r) / rate(base) if base else None,
                     "tuning": {k: r["tuning"][k] for k in ("ppb", "knn_warps", "clip_warps", "clip_thread", "knn_thread",
                                                            "ms_default", "ms_tuned")}}
         if r["kbudget"]:
@@ -384,12 +386,16 @@ def run_ours(args, rank, world, local_rank):
     n_query = stats["n_hydro"]
     if dom == "clip":
         peak = fp32.value
-        ach = n_query * W["clip_flop_per_cell"] / (stage[3] * 1e-3) / 1e12
+        # the main clip pass (k_clip32 and the FP64 re-clip of its undecided cells), timed
+        # by CUDA events on the context's stream; the fallback and the grid walk excluded
+        main_ms = stats["clip_split_ms"][0] or stage[3]
+        ach = n_query * W["clip_flop_per_cell"] / (main_ms * 1e-3) / 1e12
         roof = {"kernel": "k_clip32 (+ FP64 re-clip of undecided cells)", "bound": "fp32", "achieved": ach,
                 "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
                 "traffic": CLIP32_DRAM_BYTES_PER_CELL * n_query if D == 3 else None,
                 "traffic_note": "DRAM bytes per launch: ncu capture of the clustered 1,048,576-cell case "
-                                "(K = 190 lists) scaled by cells",
+                                "(learned-K lists) scaled by cells",
+                "timed": "main clip pass (CUDA events): k_clip32 + FP64 re-clip",
                 "peak_source": "FP32 FMA rate measured in this run (pgpu_fp32_peak)",
                 "work": f"{W['clip_flop_per_cell']:.0f} algorithmic flop per cell x {n_query} cells"}
     elif dom == "knn":
@@ -436,7 +442,7 @@ def run_ours(args, rank, world, local_rank):
                    "l2": "inputs larger than L2: per-step KNN lists alone are "
                          f"{stats['n_hydro'] * cfg['k'] * 4 / 2 ** 20:.0f} MiB at the plain K",
                    "parallelism": f"replicas x{world}"},
-        "speedup_vs_plain_gpu": value / rate(base),
+        "speedup_vs_plain_gpu": value / rate(base) if base else None,
         "roofline": roof, "roofline_hydro": roof_hydro,
         "stages_ms": dict(zip(STAGES, stage)),
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"], "forms": forms,
