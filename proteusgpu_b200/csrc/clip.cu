@@ -193,6 +193,8 @@ struct ClipParams {
     unsigned long long* walk_stats;  // grid walk: points clipped, boxes visited
     unsigned int* overflow;
     unsigned long long face_cap;
+    int walk_prefix;  // grid walk: list neighbours clipped before the walk (same in every form)
+    int walk_certk;   // grid walk: certified K reported for walked cells
 };
 
 // Cell outputs of a cell that was not extracted (the reference leaves volume 0
@@ -827,18 +829,19 @@ __device__ __forceinline__ double pt_box_d2(double x, double y, double z, const 
 
 template <int D>
 __global__ void __launch_bounds__(CLIP_WARPS * 32)
-    k_clip_pruned(ClipParams P, SubGrid g, const int2* __restrict__ table, int table_n, int table_r,
-                  const uint32_t* __restrict__ cells, int64_t ncells) {
+    k_clip_pruned(ClipParams P, SubGrid g, const int2* __restrict__ table, int table_n, int table_r) {
     using PT = typename PointOf<D>::type;
     __shared__ WarpCell cells_sm[CLIP_WARPS];
     __shared__ int4 stack_sm[CLIP_WARPS][PRUNE_STACK];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t t = (int64_t)blockIdx.x * CLIP_WARPS + w;
-    if (t >= ncells) return;  // warp-uniform
+    if (t >= P.nq) return;  // warp-uniform
     WarpCell& W = cells_sm[w];
     int4* stk = stack_sm[w];
     const PT* spts = (const PT*)P.spts;
-    const uint32_t s = cells[t];
+    const PT* ext = (const PT*)P.ext;
+    const int64_t tq = P.slots[t];  // the cell's query slot: its sorted position and its neighbour list
+    const uint32_t s = P.qs[tq];
     const uint32_t e = P.perm[s];
     const PT sp = spts[s];
     // absolute seed; the cell is clipped in the frame centred on it (planes (-b, |b|^2 / 2)
@@ -904,6 +907,38 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
         }
     };
     refresh();
+    // 1. The first walk_prefix neighbours of the cell's own list, in list order (the
+    // list-based clip's order) and in the local frame; the walk then adds only the points
+    // beyond them (keys above the last one's), so the cell stays near its final shape
+    // instead of collecting transient vertices box by box.  The prefix is the same in
+    // every form (plain K, learned K), so the walk is too.
+    double key_d2 = -1.0;  // (distance, id) of the last listed neighbour clipped
+    uint32_t key_id = 0u;
+    bool alive = true, done = false;
+    {
+        const int Kc = P.kq ? (int)P.kq[tq] : P.K;
+        const int L = min(Kc, P.walk_prefix);
+        const uint32_t* kl = P.knn + (size_t)tq * P.K;
+        for (int k = 0; k < L; k++) {
+            const uint32_t z = kl[k];
+            if (z == NO_NEIGHBOR) break;
+            const PT B = ext[z];
+            const double bx = B.x - sx, by = B.y - sy, bz = pz(B) - sz;
+            const double d2 = seed_d2(bx, by, bz, 0.0, 0.0, 0.0);  // the KNN's key, exactly
+            key_d2 = d2;
+            key_id = z;
+            if (d2 > 4 * v_dist) {  // certified: every point not clipped yet is farther
+                done = true;
+                break;
+            }
+            if (clip_by<D, true>(W, lane, z, bx, by, bz, 0.0, 0.0, 0.0, P.robust, nb_v, nb_t, status, v_dist,
+                                 fail_vdist) == CLIP_FAIL) {
+                alive = false;
+                break;
+            }
+        }
+        if (alive && !done) refresh();
+    }
     // true when no point of the box can cut the cell (with a relative margin for rounding)
     auto prunable = [&](const double (&lo)[3], double side) -> bool {
         const double ll[3] = {lo[0] - sx, lo[1] - sy, lo[2] - sz};  // the box in the local frame
@@ -980,9 +1015,12 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
                 if (q == s) continue;
                 const PT B = spts[q];
                 const double bx = B.x - sx, by = B.y - sy, bz = pz(B) - sz;
-                if (seed_d2(bx, by, bz, 0.0, 0.0, 0.0) > 4 * v_dist) continue;
+                const double d2 = seed_d2(bx, by, bz, 0.0, 0.0, 0.0);
+                if (d2 > 4 * v_dist) continue;
+                const uint32_t id = P.perm[q];
+                if (d2 < key_d2 || (d2 == key_d2 && id <= key_id)) continue;  // clipped from the list
                 if (++points > WALK_MAX_POINTS) return false;
-                const int r = clip_by<D, true>(W, lane, P.perm[q], bx, by, bz, 0.0, 0.0, 0.0, P.robust, nb_v, nb_t,
+                const int r = clip_by<D, true>(W, lane, id, bx, by, bz, 0.0, 0.0, 0.0, P.robust, nb_v, nb_t,
                                                status, v_dist, fail_vdist);
                 if (r == CLIP_FAIL) return false;
                 if (r == CLIP_CUT) refresh();
@@ -993,8 +1031,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
     // coarse bins around the seed's: the offset table (ascending lower bound), then rings
     const int bc[3] = {bin_coord(sx, G), bin_coord(sy, G), D == 3 ? bin_coord(sz, G) : 0};
     const double pc[3] = {sx, sy, sz};
-    bool alive = true;
-    for (int ci = 0; ci < table_n && alive; ci++) {
+    for (int ci = 0; ci < table_n && alive && !done; ci++) {
         const int2 ent = table[ci];
         if ((double)ent.y * h0 * h0 * (1.0 - 1e-12) > 4 * v_dist) break;
         const int x = bc[0] + (int)(signed char)(ent.x & 255), y = bc[1] + (int)(signed char)((ent.x >> 8) & 255),
@@ -1008,7 +1045,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
     // a vertex without a position (three planes through one line, w = 0) makes v_dist
     // NaN and no radius bounds the walk: such a cell stays uncertified, as in k_clip
     if (v_dist != v_dist) alive = false;
-    for (int r = table_r + 1; alive; r++) {
+    for (int r = table_r + 1; alive && !done; r++) {
         double lb = CUDART_INF;
         bool all = true;
 #pragma unroll
@@ -1056,7 +1093,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
         return;
     }
     // every point within the security radius was clipped or excluded: certified
-    extract_and_store<D>(W, P, w, lane, nb_v, nb_t, e, P.K + 1, 0.0, 0.0, 0.0, false, sx, sy, sz);
+    extract_and_store<D>(W, P, w, lane, nb_v, nb_t, e, P.walk_certk, 0.0, 0.0, 0.0, false, sx, sy, sz);
 }
 
 // ============================================================================
@@ -1879,6 +1916,9 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     P.walk_stats = &sc->walk_points;
     P.overflow = &sc->overflow;
     P.face_cap = c->face_cap;
+    // the shortest list any form builds: the smallest learned class (capped at k)
+    P.walk_prefix = std::min(c->prm.k, D == 3 ? 32 : 12);
+    P.walk_certk = c->prm.k + 1;
     if (nq > 0) {
         const unsigned blocks = (unsigned)((nq + CLIP_WARPS - 1) / CLIP_WARPS);
         const int CW = c->tune.clip_warps;  // cells (warps) per block: autotuned, 2 or 4
@@ -1892,10 +1932,10 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
             const int2* tab = (const int2*)c->knn_table.p;
             if (D == 2)
                 k_clip_pruned<2><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P, g, tab, c->knn_table_n,
-                                                                            c->knn_table_r, qs, nq);
+                                                                            c->knn_table_r);
             else
                 k_clip_pruned<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P, g, tab, c->knn_table_n,
-                                                                            c->knn_table_r, qs, nq);
+                                                                            c->knn_table_r);
         } else if (fp32) {
             if (D == 2) {
                 if (CW == 2) k_clip32<2, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
@@ -2017,11 +2057,14 @@ cudaError_t launch_pruned(pgpu_ctx* c) {
     c->n_pruned = 0;
     DevScalars* sc = (DevScalars*)c->scalars.p;
     if ((e = cudaMemsetAsync(&sc->walk_points, 0, 2 * sizeof(unsigned long long), c->stream))) return e;
-    if ((e = select_cells(c, -1, true, false, fq, &nf))) return e;
+    if ((e = select_cells(c, -1, true, true, fq, &nf))) return e;
     if (nf == 0) return cudaSuccess;
     unsigned long long fc = 0;
     unsigned of = 0, unc = 0;
-    if ((e = clip_pass(c, fq, nf, c->prm.k, nullptr, false, &fc, &of, &unc, false, nullptr, nullptr, nullptr, true)))
+    // work items are query slots: the walk starts from each cell's own neighbour list
+    const uint16_t* kq = c->use_kq ? (const uint16_t*)c->kq.p : nullptr;
+    if ((e = clip_pass(c, (const uint32_t*)c->qs.p, nf, c->knn_stride, (const uint32_t*)c->knn.p, false, &fc, &of,
+                       &unc, false, nullptr, fq, kq, true)))
         return e;
     if (of) return cudaErrorMemoryAllocation;
     c->num_faces = (int64_t)fc;

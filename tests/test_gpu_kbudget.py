@@ -162,3 +162,17 @@ def test_learned_k_with_thread_per_query_knn():
         mesh = ctx.download_mesh()
         got = ctx.sim_get() + (mesh,)
     _same(got, plain)
+
+
+def test_clustered_walk_forms_identical_without_failures():
+    """Clustered points: cells beside the clumps need the grid walk.  The walk starts
+    from the same list prefix in every form, so learned-K + FP32 steps still equal the
+    plain FP64 steps bit for bit, and no cell fails (none collects more than the
+    reference's 96 vertices on the way)."""
+    ic = ics.clustered_3d(n=150000, seed=5)
+    plain = _sim(ic, 190, 0.1, 4, False)
+    fast = _sim(ic, 190, 0.1, 4, True, precision="fp32")
+    _same(fast, plain)
+    for st in (plain[6], fast[6]):
+        assert st["pruned_cells"] > 0
+        assert st["failed_cells"] == 0
