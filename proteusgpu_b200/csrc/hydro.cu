@@ -201,9 +201,14 @@ __global__ void k_flux_update(const double4* __restrict__ w4, const double* __re
                               const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst,
                               const unsigned long long* __restrict__ dt_inst, double fixed_dt,
                               double* __restrict__ mass, double* __restrict__ mom, double* __restrict__ en,
-                              double* __restrict__ pos, DevScalars* __restrict__ sc) {
-    int64_t i = (int64_t)blockIdx.x * HT + threadIdx.x;
-    if (i >= n) return;
+                              double* __restrict__ pos, DevScalars* __restrict__ sc,
+                              const uint32_t* __restrict__ order, const uint32_t* __restrict__ perm) {
+    const int64_t t = (int64_t)blockIdx.x * HT + threadIdx.x;
+    if (t >= n) return;
+    // cells in the mesh's spatial order when given (the query list: sorted positions of
+    // the hydro cells): neighbouring threads then read neighbouring faces and share
+    // neighbour states in cache.  Every cell's arithmetic is the same either way.
+    const int64_t i = order ? (int64_t)perm[order[t]] : t;
     const int b = inst[i];
     const double gamma = ip[b].gamma;
     // MIRROR 0 / 1: every instance periodic / walled; 2: per instance
@@ -434,6 +439,8 @@ cudaError_t launch_flux_update(pgpu_ctx* c, double fixed_dt) {
     if (n <= 0) return cudaSuccess;
     DevScalars* sc = (DevScalars*)c->scalars.p;
     const bool phys = c->prm.flux_mode == PGPU_FLUX_PHYSICAL;
+    // the current mesh's query list covers exactly the hydro cells, in spatial order
+    const uint32_t* order = c->have_mesh && !c->all_cells && c->n_query == n ? (const uint32_t*)c->qs.p : nullptr;
     // walls: 0 all periodic, 1 all reflective, 2 mixed across the instances of a batch
     int mir = c->inst.par[0].mirror;
     for (const auto& q : c->inst.par)
@@ -443,7 +450,8 @@ cudaError_t launch_flux_update(pgpu_ctx* c, double fixed_dt) {
         (const double4*)c->w4.p, (const double*)c->we.p, (const uint32_t*)c->fptr.p, (const uint32_t*)c->fcnt.p, \
         (const uint32_t*)c->f_own.p, (const double4*)c->f_geo.p, n, (const InstPar*)c->inst.d_par.p,              \
         (const uint16_t*)c->inst.d_inst_h.p, (const unsigned long long*)c->inst.d_dt.p, fixed_dt,                 \
-        (double*)c->mass.p, (double*)c->mom.p, (double*)c->en.p, (double*)c->pos.p, sc)
+        (double*)c->mass.p, (double*)c->mom.p, (double*)c->en.p, (double*)c->pos.p, sc, order,             \
+        (const uint32_t*)c->perm.p)
 #define PGPU_FLUX_M(DD, PH) \
     do {                    \
         if (mir == 0)       \
