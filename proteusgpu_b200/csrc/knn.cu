@@ -38,6 +38,9 @@ constexpr int MAX_ROWS = MAX_K / 32;
 constexpr unsigned FULL = 0xffffffffu;
 constexpr int TABLE_R3 = 8;   // offsets with |d|_inf <= 8 in 3D (17^3 entries)
 constexpr int TABLE_R2 = 24;  // and |d|_inf <= 24 in 2D (49^2 entries)
+#ifndef KNN_FLUSH_MIN
+#define KNN_FLUSH_MIN 24  // queued survivors that trigger a merge at a table-chunk boundary
+#endif
 
 __device__ __forceinline__ bool key_less(double ad, uint32_t ai, double bd, uint32_t bi) {
     return ad < bd || (ad == bd && ai < bi);
@@ -317,9 +320,11 @@ __global__ void __launch_bounds__(KW * 32)
             if (ok && !box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
         }
         scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, lane, nrows, K, qn, thr_d, thr_i, ncand);
-        // the bound is tested at chunk boundaries: merge what is queued
-        flush_queue(S, lane, nrows, K, qn, thr_d, thr_i);
+        // the bound is tested at chunk boundaries: merge what is queued once it is worth a
+        // merge (a staler bound only prunes less; the rows fill up first)
+        if (qn >= KNN_FLUSH_MIN || thr_i == NO_NEIGHBOR) flush_queue(S, lane, nrows, K, qn, thr_d, thr_i);
     }
+    flush_queue(S, lane, nrows, K, qn, thr_d, thr_i);
 
     // 2. beyond the table: Chebyshev rings table_r + 1, table_r + 2, ... (sparse regions)
     for (int r = table_r + 1; !done; r++) {
