@@ -9,12 +9,12 @@
 // oriented.  Per clipping plane:
 //   1. every lane tests its vertices against the plane with the reference's
 //      determinant predicate and error bound (cell.cpp:175-221);
-//   2. the cavity boundary is the set of directed edges of removed vertices
-//      whose reverse edge belongs to no removed vertex (3D: a 64x64 edge bit
-//      matrix in shared memory; 2D: the two lines used once), checked to be a
-//      single cycle; one new vertex (plane, x, y) per boundary edge x -> y,
-//      which is the vertex the reference's boundary walk (cell.cpp:224-364)
-//      creates for that edge;
+//   2. the cavity boundary is the set of edges of removed vertices whose twin
+//      belongs to a kept vertex (3D: one key match over the removed vertices'
+//      edges, or a 64x64 edge bit matrix for large cavities; 2D: the two lines
+//      used once), checked to be a single cycle; one new vertex (plane, x, y)
+//      per boundary edge x -> y, which is the vertex the reference's boundary
+//      walk (cell.cpp:224-364) creates for that edge;
 //   3. kept vertices are compacted in order and new ones appended, each with
 //      its squared distance to the seed cached for the certificate
 //      (cell.cpp:369-384), whose maximum is a warp reduction.
@@ -796,8 +796,9 @@ __global__ void __launch_bounds__(CW * 32) k_clip(ClipParams P) {
 // Security-radius clipping without a neighbour budget (extension).  Cells whose
 // certificate does not close within the K nearest neighbours -- large cells
 // beside dense clumps, whose security sphere holds thousands of clump points --
-// are clipped by walking the grid instead of a list: coarse bins in order of
-// their distance lower bound, dense bins descended sub-bin by sub-bin.  A box
+// are clipped from the head of their own list and then by walking the grid:
+// coarse bins in order of their distance lower bound, dense bins descended
+// sub-bin by sub-bin, points already clipped from the list skipped.  A box
 // is skipped when it lies beyond the security radius (2 sqrt(v_dist)) or when
 // no point in it can cut the cell: a point q cuts the convex cell iff some
 // vertex v is nearer to q than to the seed, so a box whose distance to every
@@ -806,9 +807,9 @@ __global__ void __launch_bounds__(CW * 32) k_clip(ClipParams P) {
 // or excluded, which is the certificate.  The walk also takes the cells that
 // failed for other reasons (predicates the absolute-frame determinants cannot
 // decide, plane or vertex overflow): it clips in the seed's local frame and
-// reuses plane slots, which removes most of those causes.  Points of a sub-bin are clipped in
-// their sorted order (by extended id within the sub-bin), so the result is
-// deterministic.
+// reuses plane slots, which removes most of those causes.  Points of a
+// sub-bin are clipped in their sorted order (by extended id within the
+// sub-bin), so the result is deterministic.
 constexpr int PRUNE_STACK = 64;
 constexpr int WALK_MAX_BOXES = 1 << 17;   // boxes popped per cell
 constexpr int WALK_MAX_POINTS = 1 << 15;  // points clipped per cell
