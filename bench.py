@@ -243,7 +243,7 @@ def _max_over_ranks(dist, ms):
     if not dist:
         return ms
     import torch
-    t = torch.tensor([ms], device="cuda")
+    t = torch.tensor([ms], device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
