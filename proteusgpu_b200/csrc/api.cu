@@ -236,7 +236,9 @@ void pgpu_destroy(pgpu_ctx* c) {
                       &c->en,    &c->w4,      &c->we,       &c->red_tmp, &c->dl_ptr,   &c->dl_a,       &c->dl_b,
                       &c->dl_c,  &c->kq,      &c->kb.w,     &c->kb.wbf,  &c->kb.adam_m, &c->kb.adam_v, &c->kb.part,
                       &c->kb.feat, &c->kb.hist_vol, &c->kb.miss, &c->kb.ksum, &c->kb.labels, &c->kb.tmp_out,
-                      &c->bin_lvl, &c->sub_off, &c->sub_cnt, &c->sub_start};
+                      &c->bin_lvl, &c->sub_off, &c->sub_cnt, &c->sub_start, &c->sort_big, &c->sort_keys,
+                      &c->sort_pts, &c->inst.d_par, &c->inst.d_inst_h, &c->inst.d_inst_e, &c->inst.d_dt,
+                      &c->inst.d_gather};
     for (DevBuf* b : bufs) free_buf(*b);
     for (int i = 0; i < 9; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);

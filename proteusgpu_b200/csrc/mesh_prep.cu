@@ -162,14 +162,23 @@ __global__ void k_sub_count(const typename PointOf<D>::type* __restrict__ ext, i
 
 // Points of each sub-bin in ascending extended id (the scatter's atomics leave
 // them in arbitrary order), so that every walk over a sub-bin is deterministic.
+// Sub-bins of more points than this are sorted by a block each (k_sub_sort_big);
+// the smaller ones, nearly all, by one thread.
+constexpr uint32_t SUBSORT_THREAD_MAX = 64;
+constexpr uint32_t SUBSORT_SMEM_KEYS = 8192;  // larger ones sort their keys in global scratch
+
 template <int D>
 __global__ void k_sub_sort(const uint32_t* __restrict__ sub_start, int64_t T,
                            typename PointOf<D>::type* __restrict__ spts, uint32_t* __restrict__ perm,
-                           uint32_t* __restrict__ inv) {
+                           uint32_t* __restrict__ inv, uint32_t* __restrict__ big, unsigned int* __restrict__ n_big) {
     const int64_t slot = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (slot >= T) return;
     const uint32_t a = sub_start[slot], b = sub_start[slot + 1];
     if (b - a < 2) return;
+    if (b - a > SUBSORT_THREAD_MAX) {  // gas piled beyond the deepest refinement level
+        big[atomicAdd(n_big, 1u)] = (uint32_t)slot;
+        return;
+    }
     for (uint32_t i = a + 1; i < b; i++) {
         const uint32_t id = perm[i];
         const typename PointOf<D>::type pt = spts[i];
@@ -183,6 +192,70 @@ __global__ void k_sub_sort(const uint32_t* __restrict__ sub_start, int64_t T,
         spts[j] = pt;
     }
     for (uint32_t i = a; i < b; i++) inv[perm[i]] = i;
+}
+
+// Ascending sort of n keys by one block: the bitonic network in the form whose
+// compare-exchanges all put the smaller key first (a mirrored stage, then
+// half-cleaners, per merge size), on n rounded up to a power of two with the
+// missing keys taken as +inf -- they never move, so they need no storage.
+__device__ void block_sort_u64(unsigned long long* k, uint32_t n) {
+    uint32_t P = 1;
+    while (P < n) P <<= 1;
+    for (uint32_t size = 2; size <= P; size <<= 1) {
+        for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+            const uint32_t half = size / 2, blk = t / half, off = t % half;
+            const uint32_t lo = blk * size + off, hi = blk * size + size - 1 - off;
+            if (hi < n && k[hi] < k[lo]) {
+                const unsigned long long x = k[lo];
+                k[lo] = k[hi];
+                k[hi] = x;
+            }
+        }
+        __syncthreads();
+        for (uint32_t j = size / 4; j > 0; j >>= 1) {
+            for (uint32_t t = threadIdx.x; t < P / 2; t += blockDim.x) {
+                const uint32_t lo = (t / j) * 2 * j + t % j, hi = lo + j;
+                if (hi < n && k[hi] < k[lo]) {
+                    const unsigned long long x = k[lo];
+                    k[lo] = k[hi];
+                    k[hi] = x;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+// The large sub-bins listed by k_sub_sort, a block each: keys (id, position in the
+// sub-bin) sorted in shared memory (or, beyond SUBSORT_SMEM_KEYS, in the scratch at
+// the sub-bin's own range), then ids and points put in that order through a copy.
+template <int D>
+__global__ void __launch_bounds__(256)
+    k_sub_sort_big(const uint32_t* __restrict__ sub_start, const uint32_t* __restrict__ big,
+                   const unsigned int* __restrict__ n_big, typename PointOf<D>::type* __restrict__ spts,
+                   uint32_t* __restrict__ perm, uint32_t* __restrict__ inv, unsigned long long* __restrict__ keys,
+                   typename PointOf<D>::type* __restrict__ tmp) {
+    extern __shared__ unsigned long long sk[];
+    const unsigned nb = *n_big;
+    for (unsigned i = blockIdx.x; i < nb; i += gridDim.x) {
+        const uint32_t slot = big[i];
+        const uint32_t a = sub_start[slot], m = sub_start[slot + 1] - a;
+        unsigned long long* k = m <= SUBSORT_SMEM_KEYS ? sk : keys + a;
+        for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
+            k[j] = ((unsigned long long)perm[a + j] << 32) | j;
+            tmp[a + j] = spts[a + j];
+        }
+        __syncthreads();
+        block_sort_u64(k, m);
+        for (uint32_t j = threadIdx.x; j < m; j += blockDim.x) {
+            const unsigned long long key = k[j];
+            const uint32_t id = (uint32_t)(key >> 32);
+            perm[a + j] = id;
+            spts[a + j] = tmp[a + (uint32_t)(key & 0xffffffffull)];
+            inv[id] = a + j;
+        }
+        __syncthreads();
+    }
 }
 
 // Point range of each coarse bin from the sub-bin starts.
@@ -457,11 +530,40 @@ cudaError_t launch_grid_sort(pgpu_ctx* c) {
         else
             k_bin_scatter<3><<<nblk(n, 256), 256, 0, c->stream>>>((const double4*)c->ext.p, n, key, sstart, scnt,
                                                                   (double4*)c->spts.p, perm, inv);
+        DevScalars* sc = (DevScalars*)c->scalars.p;
+        uint32_t* big = ensure<uint32_t>(c->sort_big, (size_t)T + 1, &e);
+        if (e) return e;
+        if ((e = cudaMemsetAsync(&sc->sort_big, 0, sizeof(unsigned int), c->stream))) return e;
         if (D == 2)
-            k_sub_sort<2><<<nblk(T, 256), 256, 0, c->stream>>>(sstart, T, (double2*)c->spts.p, perm, inv);
+            k_sub_sort<2><<<nblk(T, 256), 256, 0, c->stream>>>(sstart, T, (double2*)c->spts.p, perm, inv, big,
+                                                               &sc->sort_big);
         else
-            k_sub_sort<3><<<nblk(T, 256), 256, 0, c->stream>>>(sstart, T, (double4*)c->spts.p, perm, inv);
+            k_sub_sort<3><<<nblk(T, 256), 256, 0, c->stream>>>(sstart, T, (double4*)c->spts.p, perm, inv, big,
+                                                               &sc->sort_big);
         count_launches(2);
+        unsigned int nbig = 0;
+        if ((e = cudaMemcpyAsync(&nbig, &sc->sort_big, sizeof(nbig), cudaMemcpyDeviceToHost, c->stream))) return e;
+        if ((e = cudaStreamSynchronize(c->stream))) return e;
+        if (nbig > 0) {
+            const size_t psz = D == 2 ? sizeof(double2) : sizeof(double4);
+            unsigned long long* keys = ensure<unsigned long long>(c->sort_keys, (size_t)n + 1, &e);
+            void* tmp = ensure<unsigned char>(c->sort_pts, ((size_t)n + 1) * psz, &e);
+            if (e) return e;
+            const unsigned grid = nbig < 296u ? nbig : 296u;
+            const size_t smem = SUBSORT_SMEM_KEYS * sizeof(unsigned long long);
+            if (D == 2) {
+                if ((e = cudaFuncSetAttribute(k_sub_sort_big<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+                    return e;
+                k_sub_sort_big<2><<<grid, 256, smem, c->stream>>>(sstart, big, &sc->sort_big, (double2*)c->spts.p,
+                                                                  perm, inv, keys, (double2*)tmp);
+            } else {
+                if ((e = cudaFuncSetAttribute(k_sub_sort_big<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+                    return e;
+                k_sub_sort_big<3><<<grid, 256, smem, c->stream>>>(sstart, big, &sc->sort_big, (double4*)c->spts.p,
+                                                                  perm, inv, keys, (double4*)tmp);
+            }
+            count_launches(1);
+        }
     }
     return cudaGetLastError();
 }

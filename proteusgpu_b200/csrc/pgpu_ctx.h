@@ -58,6 +58,7 @@ struct DevScalars {
     double sums[5];                 // mass, mom x/y/z, energy
     unsigned long long walk_points; // grid walk: points clipped (statistics; after the
     unsigned long long walk_boxes;  //   per-step counters, which are cleared up to dt)
+    unsigned int sort_big;          // grid sort: sub-bins too large for one thread
 };
 
 // Learned neighbour budget: a per-cell MLP (8 features -> 32 -> 32 -> 6 classes,
@@ -143,6 +144,7 @@ struct pgpu_ctx {
     pgpu::DevBuf bin_lvl;      // u8 per coarse bin: refinement level L ((2^L)^D sub-bins)
     pgpu::DevBuf sub_off;      // u32 per coarse bin: first sub-bin slot (M + 1 entries)
     pgpu::DevBuf sub_cnt, sub_start;  // per sub-bin slot: counts, first sorted point (T + 1)
+    pgpu::DevBuf sort_big, sort_keys, sort_pts;  // large sub-bins: their slots, key and point scratch
     int64_t sub_slots = 0;     // T
     pgpu::DevBuf spts, perm, inv;  // sorted points, sorted->ext id, ext id->sorted
     pgpu::DevBuf qflag, qoff, qs;  // query list (sorted positions of the cells to compute)

@@ -125,3 +125,23 @@ def test_knn_thread_per_query(case, k, kt):
     else:
         pts = ics.uniform_points(10, 3, 3)
     assert np.array_equal(_knn_thread(pts, k, kt), om.knn(pts, k))
+
+
+def test_knn_sub_bin_beyond_the_deepest_level():
+    """Thousands of points inside one deepest-level sub-bin (a pile-up far denser than
+    the refinement can split): such sub-bins are sorted by a block, and the lists and
+    the sorted order (ids ascending inside the sub-bin) stay the same as for small ones."""
+    rng = np.random.default_rng(31)
+    pile = 0.4321 + 1e-9 * rng.random((9000, 3))       # > 8192: keys sorted in global scratch
+    pile2 = 0.7123 + 1e-9 * rng.random((3000, 3))      # <= 8192: keys sorted in shared memory
+    pts = np.ascontiguousarray(np.concatenate([rng.random((20000, 3)), pile, pile2]))
+    with Context(dim=3, k=24) as ctx:
+        g = ctx.knn(pts)
+        sp, perm, _ = ctx.knn_sorted()
+        g2 = ctx.knn(pts)
+    assert np.array_equal(g, om.knn(pts, 24)) and np.array_equal(g, g2)
+    for lo, hi in ((20000, 29000), (29000, 32000)):
+        at = np.nonzero((perm >= lo) & (perm < hi))[0]
+        assert np.array_equal(at, np.arange(at[0], at[0] + len(at)))  # contiguous: one sub-bin
+        assert np.array_equal(perm[at], np.arange(lo, hi))            # ids ascending inside it
+    assert np.array_equal(sp, pts[perm])
