@@ -239,6 +239,25 @@ def _barrier(dist):
         dist.barrier()
 
 
+def compare_states(ref, got):
+    """Cells whose state (position, mass, momentum, energy) differs from the reference
+    form's after the same steps from the same initial condition, and each field's
+    relative L1 difference.  Identical states after a run mean every step's mesh was
+    identical too: any face or area difference changes the fluxes."""
+    names = ("position", "mass", "momentum", "energy")
+    n = len(ref[1])
+    differ = np.zeros(n, bool)
+    l1 = {}
+    for nm, a, b in zip(names, ref, got):
+        a = np.asarray(a, np.float64).reshape(n, -1)
+        b = np.asarray(b, np.float64).reshape(n, -1)
+        neq = (a != b) & ~(np.isnan(a) & np.isnan(b))
+        differ |= neq.any(axis=1)
+        den = float(np.nansum(np.abs(a)))
+        l1[nm] = float(np.nansum(np.abs(a - b))) / den if den > 0 else 0.0
+    return {"cells_differing": int(differ.sum()), "l1_rel": l1}
+
+
 def _max_over_ranks(dist, ms):
     if not dist:
         return ms
@@ -248,7 +267,7 @@ def _max_over_ranks(dist, ms):
     return float(t.item())
 
 
-def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks=False):
+def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks=False, want_state=False):
     """Runs one form from the initial condition: W warm-up steps (the learned forms
     train their proposal on them), one step with per-stage CUDA events, then K timed
     steps bracketed by a barrier and synchronize (max over ranks)."""
@@ -300,6 +319,8 @@ def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks
     kb_after = ctx.kbudget_stats() if spec["kbudget"] else None
     out = {"ms": ms, "stage": stage, "stats": stats, "launches": launches, "clocks": clk.summary(),
            "kbudget": kb_after or kb, "tuning": tuning}
+    if want_state:  # the state after the timed steps, for the comparison between forms
+        out["state"] = ctx.sim_get()
     if want_e2e:
         # end to end: the same step through the C ABI with the state in pinned host
         # memory, copied to the device before and back after every step
@@ -337,9 +358,16 @@ def run_ours(args, rank, world, local_rank):
     n = ic.n
     names = [HEADLINE] if args.headline_only else [BASELINE_FORM, HEADLINE] if args.skip_forms else list(FORMS)
     res = {}
+    ref_state = None  # the plain form runs first; every other form is compared with it
     for f in names:
         res[f] = time_form(args, cfg, ic, local_rank, dist, f, want_e2e=(f == HEADLINE and not args.skip_e2e),
-                           want_clocks=(f == HEADLINE))
+                           want_clocks=(f == HEADLINE), want_state=BASELINE_FORM in names)
+        st = res[f].pop("state", None)
+        if f == BASELINE_FORM:
+            ref_state = st
+        elif ref_state is not None and st is not None:
+            res[f]["vs_plain"] = compare_states(ref_state, st)
+        del st
     _barrier(dist)
     if dist:
         dist.destroy_process_group()
@@ -361,6 +389,8 @@ def run_ours(args, rank, world, local_rank):
                     "speedup_vs_plain": rate(r) / rate(base) if base else None,
                     "tuning": {k: r["tuning"][k] for k in ("ppb", "knn_warps", "clip_warps", "clip_thread", "knn_thread",
                                                            "ms_default", "ms_tuned")}}
+        if "vs_plain" in r:
+            forms[f]["vs_plain"] = r["vs_plain"]
         if r["kbudget"]:
             kb = r["kbudget"]
             forms[f]["learned_k"] = {"mean_k": kb["mean_k"], "plain_k": cfg["k"], "cells": kb["cells"],
@@ -443,6 +473,9 @@ def run_ours(args, rank, world, local_rank):
                          f"{stats['n_hydro'] * cfg['k'] * 4 / 2 ** 20:.0f} MiB at the plain K",
                    "parallelism": f"replicas x{world}"},
         "speedup_vs_plain_gpu": value / rate(base) if base else None,
+        # the headline's state after the timed steps against the plain FP64 form's (same IC,
+        # same steps): 0 cells differing and 0 L1 error = the same meshes and fluxes every step
+        "matched_l1": ({"vs": BASELINE_FORM, **head["vs_plain"]} if "vs_plain" in head else None),
         "roofline": roof, "roofline_hydro": roof_hydro,
         "stages_ms": dict(zip(STAGES, stage)),
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"], "forms": forms,

@@ -245,8 +245,13 @@ int pgpu_batch_dt(pgpu_ctx *ctx, double *dt_per_instance);
  * K is at most 32 or 64) and the clipping block size (2, 4 cells; in 2D
  * also one thread per cell instead of one warp), one
  * after the other; the choice is cached for the process by (dim, log2 n, batch,
- * precision, learned K, k) and reused without timing.  Results do not depend on
- * the launch shapes. */
+ * precision, learned K, k) and reused without timing.  The block sizes and the
+ * thread-or-warp choices change no result.  The grid bin size changes nothing
+ * either except in cells certified by the grid walk (beside dense clumps), whose
+ * clipping order follows the grid: their areas and volumes move at rounding
+ * level.  So the bin size is chosen once per (dim, log2 n, batch, k) and shared
+ * by every form (plain or learned K, FP64 or FP32), which therefore build the
+ * same meshes bit for bit. */
 typedef struct {
     double ppb;
     int32_t knn_warps, clip_warps;

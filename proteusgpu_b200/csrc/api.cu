@@ -806,14 +806,24 @@ int pgpu_mlp_grad(pgpu_ctx* c, const float* feat, const int32_t* labels, int64_t
 }
 
 // ------------------------------------------------------------------ autotuner
-// Launch shapes per workload class, shared by the contexts of this process.
+// Launch shapes per workload class, shared by the contexts of this process.  The
+// grid bin size is shared by every form of a workload (plain or learned K, FP64 or
+// FP32 clipping): the grid walk clips the points beyond a cell's list in the grid's
+// box order, so forms on one grid give the same meshes bit for bit.
 using TuneKey = std::tuple<int, int, int, int, int, int>;  // dim, log2 n, batch, precision, learned K, k
+using GridKey = std::tuple<int, int, int, int>;            // dim, log2 n, batch, k
 static std::mutex g_tune_mu;
 static std::map<TuneKey, pgpu::Tuning> g_tune_cache;
+static std::map<GridKey, double> g_ppb_cache;
 
 static TuneKey tune_key(const pgpu_ctx* c) {
     const int lg = c->n_hydro > 0 ? (int)std::lround(std::log2((double)c->n_hydro)) : 0;
     return TuneKey(c->prm.dim, lg, c->inst.n > 1, c->prm.precision, c->kb.enabled && c->kb.trained, c->prm.k);
+}
+
+static GridKey grid_key(const pgpu_ctx* c) {
+    const int lg = c->n_hydro > 0 ? (int)std::lround(std::log2((double)c->n_hydro)) : 0;
+    return GridKey(c->prm.dim, lg, c->inst.n > 1, c->prm.k);
 }
 
 // One mesh build of the current simulation state with stage timing; returns the
@@ -840,7 +850,9 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
     if (r) return r;
     if (!c->have_sim) return fail(c, PGPU_ESTATE, "pgpu_autotune: needs a simulation (pgpu_sim_init or pgpu_batch_init)");
     const TuneKey key = tune_key(c);
+    const GridKey gkey = grid_key(c);
     pgpu_tuning res{};
+    double shared_ppb = 0.0;  // the workload's grid bin size, if another form has chosen it
     {
         std::lock_guard<std::mutex> lock(g_tune_mu);
         auto it = g_tune_cache.find(key);
@@ -848,6 +860,8 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
             c->tune = it->second;
             res.from_cache = 1;
         }
+        auto ig = g_ppb_cache.find(gkey);
+        if (ig != g_ppb_cache.end()) shared_ppb = ig->second;
     }
     if (!res.from_cache) {
         const bool timing = c->timing;
@@ -858,12 +872,16 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
         float t = 0.0f;
         if ((r = timed_build(c, 0xF, &t))) return r;
         res.ms_default = t;
-        // 1. grid bin size: sort + KNN + clip
+        // 1. grid bin size: sort + KNN + clip (unless another form of this workload chose it)
         float bt = 1e30f;
-        for (double ppb : {1.5, 2.0, 3.0, 4.0}) {
-            c->tune.ppb = ppb;
-            if ((r = timed_build(c, 0xE, &t))) return r;
-            if (t < bt) bt = t, best.ppb = ppb;
+        if (shared_ppb > 0.0) {
+            best.ppb = shared_ppb;
+        } else {
+            for (double ppb : {1.5, 2.0, 3.0, 4.0}) {
+                c->tune.ppb = ppb;
+                if ((r = timed_build(c, 0xE, &t))) return r;
+                if (t < bt) bt = t, best.ppb = ppb;
+            }
         }
         c->tune.ppb = best.ppb;
         // 2. KNN block size, then one thread per query for the small K
@@ -902,6 +920,7 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
         c->kb.enabled = kb_enabled;
         std::lock_guard<std::mutex> lock(g_tune_mu);
         g_tune_cache[key] = best;
+        g_ppb_cache.emplace(gkey, best.ppb);
     }
     res.ppb = c->tune.ppb;
     res.knn_warps = c->tune.knn_warps;

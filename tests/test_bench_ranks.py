@@ -48,3 +48,22 @@ def test_two_ranks_take_the_slowest_time_and_rank0_alone_reports():
         assert p.exitcode == 0
     assert [r[1] for r in res] == [11.0, 11.0]  # max over ranks, on every rank
     assert res[1][2] is None  # rank 1: no reference work, nothing to print
+
+
+def test_compare_states_counts_cells_and_l1():
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import bench
+    rng = np.random.default_rng(1)
+    ref = (rng.random((50, 3)), rng.random(50) + 1, rng.random((50, 3)), rng.random(50) + 1)
+    same = tuple(a.copy() for a in ref)
+    r = bench.compare_states(ref, same)
+    assert r["cells_differing"] == 0 and all(v == 0.0 for v in r["l1_rel"].values())
+    got = tuple(a.copy() for a in ref)
+    got[1][7] *= 1 + 1e-12          # one mass
+    got[2][9, 2] = np.nextafter(got[2][9, 2], 2.0)  # one momentum component, one ulp
+    got[0][7, 0] = np.nan           # the same cell as the mass change
+    ref[0][3, 1] = got[0][3, 1] = np.nan  # NaN in both: equal
+    r = bench.compare_states(ref, got)
+    assert r["cells_differing"] == 2
+    assert r["l1_rel"]["mass"] > 0 and r["l1_rel"]["energy"] == 0.0
