@@ -1133,44 +1133,6 @@ __device__ __forceinline__ float per3f(float a11, float a12, float a13, float a2
            fabsf(a31) * per2f(a12, a13, a22, a23);
 }
 
-// det4 of the reference's expansion and its permanent, single precision.
-__device__ __forceinline__ void det4f(float a11, float a12, float a13, float a14, float a21, float a22, float a23,
-                                      float a24, float a31, float a32, float a33, float a34, float a41, float a42,
-                                      float a43, float a44, float& det, float& per) {
-    const float m12 = fmaf(a21, a12, -(a11 * a22)), p12 = fabsf(a21 * a12) + fabsf(a11 * a22);
-    const float m13 = fmaf(a31, a12, -(a11 * a32)), p13 = fabsf(a31 * a12) + fabsf(a11 * a32);
-    const float m14 = fmaf(a41, a12, -(a11 * a42)), p14 = fabsf(a41 * a12) + fabsf(a11 * a42);
-    const float m23 = fmaf(a31, a22, -(a21 * a32)), p23 = fabsf(a31 * a22) + fabsf(a21 * a32);
-    const float m24 = fmaf(a41, a22, -(a21 * a42)), p24 = fabsf(a41 * a22) + fabsf(a21 * a42);
-    const float m34 = fmaf(a41, a32, -(a31 * a42)), p34 = fabsf(a41 * a32) + fabsf(a31 * a42);
-    const float m123 = fmaf(m12, a33, fmaf(m23, a13, -(m13 * a23)));
-    const float m124 = fmaf(m12, a43, fmaf(m24, a13, -(m14 * a23)));
-    const float m134 = fmaf(m13, a43, fmaf(m34, a13, -(m14 * a33)));
-    const float m234 = fmaf(m23, a43, fmaf(m34, a23, -(m24 * a33)));
-    const float q123 = p23 * fabsf(a13) + p13 * fabsf(a23) + p12 * fabsf(a33);
-    const float q124 = p24 * fabsf(a13) + p14 * fabsf(a23) + p12 * fabsf(a43);
-    const float q134 = p34 * fabsf(a13) + p14 * fabsf(a33) + p13 * fabsf(a43);
-    const float q234 = p34 * fabsf(a23) + p24 * fabsf(a33) + p23 * fabsf(a43);
-    det = fmaf(-m123, a44, fmaf(m124, a34, fmaf(m234, a14, -(m134 * a24))));
-    per = q234 * fabsf(a14) + q134 * fabsf(a24) + q124 * fabsf(a34) + q123 * fabsf(a44);
-}
-
-// 0 = not in conflict, 1 = in conflict, 2 = undecided in FP32
-template <int D>
-__device__ __forceinline__ int conflict_f(const float4* hp, uint32_t t, const float4& e) {
-    const float4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)];
-    float det, per;
-    if (D == 2) {
-        det = det3f(p1.x, p2.x, e.x, p1.y, p2.y, e.y, p1.w, p2.w, e.w);
-        per = per3f(p1.x, p2.x, e.x, p1.y, p2.y, e.y, p1.w, p2.w, e.w);
-    } else {
-        const float4 p3 = hp[tri_c(t)];
-        det4f(p1.x, p2.x, p3.x, e.x, p1.y, p2.y, p3.y, e.y, p1.z, p2.z, p3.z, e.z, p1.w, p2.w, p3.w, e.w, det, per);
-    }
-    if (!(fabsf(det) > F32_BOUND * per)) return 2;
-    return det > 0.0f ? 1 : 0;
-}
-
 // Homogeneous coordinates of a vertex in the local frame -- the cofactors of the
 // plane-vertex determinant: det4(p1, p2, p3, e) = e . V (and det3 in 2D) -- and
 // the permanents of the same minors, which bound their rounding errors.  The
@@ -1215,34 +1177,6 @@ __device__ __forceinline__ int conflict_h32(const float4& V, const float4& P, co
     const float per = fmaf(fabsf(e.w), P.w, fmaf(fabsf(e.z), P.z, fmaf(fabsf(e.y), P.y, fabsf(e.x) * P.x)));
     if (!(fabsf(t) > F32_BOUND * per)) return 2;
     return t > 0.0f ? 1 : 0;
-}
-
-// Squared distance of a vertex to the seed (the origin of the local frame).
-template <int D>
-__device__ __forceinline__ float vertex_d2f(const float4* hp, uint32_t t) {
-    const float4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)];
-    if (D == 2) {
-        const float rx = -det2f(p1.w, p1.y, p2.w, p2.y);
-        const float ry = -det2f(p1.x, p1.w, p2.x, p2.w);
-        const float rw = det2f(p1.x, p1.y, p2.x, p2.y);
-        const float x = rx / rw, y = ry / rw;
-        return fmaf(x, x, y * y);
-    }
-    const float4 p3 = hp[tri_c(t)];
-    const float rx = -det3f(p1.w, p1.y, p1.z, p2.w, p2.y, p2.z, p3.w, p3.y, p3.z);
-    const float ry = -det3f(p1.x, p1.w, p1.z, p2.x, p2.w, p2.z, p3.x, p3.w, p3.z);
-    const float rz = -det3f(p1.x, p1.y, p1.w, p2.x, p2.y, p2.w, p3.x, p3.y, p3.w);
-    const float rw = det3f(p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z);
-    const float x = rx / rw, y = ry / rw, z = rz / rw;
-    return fmaf(x, x, fmaf(y, y, z * z));
-}
-
-__device__ __forceinline__ float nan_maxf(float a, float b) { return (a != a || b != b) ? (a + b) : fmaxf(a, b); }
-
-__device__ __forceinline__ float warp_maxf(float v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = nan_maxf(v, __shfl_xor_sync(FULL, v, o));
-    return v;
 }
 
 // The squared distances are >= +0 or NaN, so their bit patterns order as unsigned
