@@ -51,7 +51,7 @@ CONFIGS = {
                           n_inst=256),
 }
 
-# Algorithmic work per unit ("Roofline"): counted with the oracle's
+# Algorithmic work per unit, counted with the oracle's
 # instrumented restatement of the reference's search and clipping on the same
 # distributions (3D uniform K=190; 2D jittered lattice K=16).
 #   KNN: candidates per query x flops per squared distance (3D: 8, 2D: 5)
@@ -227,7 +227,7 @@ FORMS = {
     "learned_fp64": dict(precision="fp64", kbudget=True),
     "learned_fp32": dict(precision="fp32", kbudget=True),
 }
-HEADLINE, BASELINE_FORM = "learned_fp32", "plain_fp64"
+HEADLINE, PLAIN_FORM = "learned_fp32", "plain_fp64"
 
 # DRAM bytes per cell of one k_clip32 launch (read + write / cells), from an ncu capture
 # of the clustered 1,048,576-cell case on learned-K lists, used for `traffic`.
@@ -356,14 +356,14 @@ def run_ours(args, rank, world, local_rank):
                                 device_id=torch.device("cuda", local_rank))
     ic = make_ic(cfg)
     n = ic.n
-    names = [HEADLINE] if args.headline_only else [BASELINE_FORM, HEADLINE] if args.skip_forms else list(FORMS)
+    names = [HEADLINE] if args.headline_only else [PLAIN_FORM, HEADLINE] if args.skip_forms else list(FORMS)
     res = {}
     ref_state = None  # the plain form runs first; every other form is compared with it
     for f in names:
         res[f] = time_form(args, cfg, ic, local_rank, dist, f, want_e2e=(f == HEADLINE and not args.skip_e2e),
-                           want_clocks=(f == HEADLINE), want_state=BASELINE_FORM in names)
+                           want_clocks=(f == HEADLINE), want_state=PLAIN_FORM in names)
         st = res[f].pop("state", None)
-        if f == BASELINE_FORM:
+        if f == PLAIN_FORM:
             ref_state = st
         elif ref_state is not None and st is not None:
             res[f]["vs_plain"] = compare_states(ref_state, st)
@@ -377,7 +377,7 @@ def run_ours(args, rank, world, local_rank):
     def rate(r):
         return n * args.steps * world / (r["ms"] / 1e3)
 
-    head, base = res[HEADLINE], res.get(BASELINE_FORM)
+    head, base = res[HEADLINE], res.get(PLAIN_FORM)
     value = rate(head)
     forms = {}
     for f, r in res.items():
@@ -475,7 +475,7 @@ def run_ours(args, rank, world, local_rank):
         "speedup_vs_plain_gpu": value / rate(base) if base else None,
         # the headline's state after the timed steps against the plain FP64 form's (same IC,
         # same steps): 0 cells differing and 0 L1 error = the same meshes and fluxes every step
-        "matched_l1": ({"vs": BASELINE_FORM, **head["vs_plain"]} if "vs_plain" in head else None),
+        "matched_l1": ({"vs": PLAIN_FORM, **head["vs_plain"]} if "vs_plain" in head else None),
         "roofline": roof, "roofline_hydro": roof_hydro,
         "stages_ms": dict(zip(STAGES, stage)),
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"], "forms": forms,

@@ -1098,7 +1098,7 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
 }
 
 // ============================================================================
-// FP32 local-frame clipping (BASELINE's precision form).  The cell is clipped
+// FP32 local-frame clipping (the precision form).  The cell is clipped
 // in single precision in a frame centred on its seed: a neighbour b = B - seed
 // gives the plane (-b, |b|^2 / 2), the box planes get w + n.seed.  Every
 // plane-vertex determinant is accepted only when it exceeds a bound on its

@@ -16,7 +16,7 @@
 // An MLP 8 -> 32 -> 32 -> 6 (GELU) classifies the cell's certified K into the
 // classes {12,16,20,24,32,48} (2D) or {32,40,48,64,96,128} (3D); the proposal
 // is the smallest class whose cumulative probability reaches the quantile.
-// Every proposal is judged by the certificate: a cell that does not certify
+// Every proposal is checked by the certificate: a cell that does not certify
 // within its K is computed again at the plain budget, so the mesh is the plain
 // method's mesh bit for bit.
 //
