@@ -78,6 +78,8 @@ def parse():
                     help="time only the headline form and the plain baseline (not fp32_clip, learned_fp64)")
     ap.add_argument("--headline-only", action="store_true",
                     help="time only the headline form (profiling runs; no speed-up against the plain form)")
+    ap.add_argument("--skip-oracle", action="store_true",
+                    help="omit the oracle checks (sampled cells at full size, density error of a full oracle run)")
     return ap.parse_args()
 
 
@@ -267,10 +269,20 @@ def _max_over_ranks(dist, ms):
     return float(t.item())
 
 
-def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks=False, want_state=False):
+def _oracle_check_module():
+    """oracle/check.py: the checker of the full-size meshes (used after the timed region only)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import check
+    return check
+
+
+def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks=False, want_state=False,
+              want_check=False):
     """Runs one form from the initial condition: W warm-up steps (the learned forms
     train their proposal on them), one step with per-stage CUDA events, then K timed
-    steps bracketed by a barrier and synchronize (max over ranks)."""
+    steps bracketed by a barrier and synchronize (max over ranks).  want_check: the
+    oracle checks the first mesh and, after the timed steps, the mesh of one more step
+    on samples of their cells (nothing of it is timed)."""
     import torch
     from proteusgpu_b200 import Context, _lib
     L = _lib.load()
@@ -288,6 +300,13 @@ def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks
                        ic.concat("vel"), ic.concat("energy"), ic.concat("deposit"))
     else:
         ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+    checks = {}
+    if want_check:
+        t0 = time.perf_counter()
+        checks["first_mesh"] = _oracle_check_module().sampled_cells(
+            ctx, n_random=20000, n_walked=2000, pos_before=ic.pos, buff=cfg["buff"], boundary=cfg["boundary"],
+            seed=11)
+        checks["first_mesh"]["seconds"] = time.perf_counter() - t0
     for _ in range(max(args.warmup, 0)):
         ctx.sim_step(cfg["cfl"], want_dt=False)
     # launch shapes for this workload, timed on mesh builds of the current state (nothing advances)
@@ -338,7 +357,58 @@ def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks
         e_ms = _max_over_ranks(dist, (time.perf_counter() - t0) * 1e3)
         nbytes = int(sum(a.nbytes for a in hn))
         out["e2e"] = {"ms": e_ms, "steps": ke, "bytes": nbytes}
+    if want_check:
+        # one more step, its mesh checked against the oracle from the positions it started at
+        t0 = time.perf_counter()
+        x_before = ctx.sim_get()[0]
+        ctx.sim_step(cfg["cfl"], want_dt=False)
+        checks["after_timed_steps"] = _oracle_check_module().sampled_cells(
+            ctx, n_random=20000, n_walked=2000, pos_before=x_before, buff=cfg["buff"], boundary=cfg["boundary"],
+            seed=12)
+        checks["after_timed_steps"]["seconds"] = time.perf_counter() - t0
+        out["checks"] = checks
+    if spec["kbudget"]:
+        out["weights"] = ctx.kbudget_weights()
     ctx.close()
+    return out
+
+
+def density_check(cfg, form, weights, steps=3, n_max=1_048_576):
+    """The density error of a whole run against the oracle's: the workload's distribution
+    at min(n, n_max) points (ghost layer spanning the same number of mean cells), `steps`
+    moving-mesh steps of the given form (learned forms use the proposal trained on the full
+    workload) and of the plain FP64 form on the GPU, and the oracle's own run."""
+    from proteusgpu_b200 import Context
+    check = _oracle_check_module()
+    n = min(cfg["n"], n_max)
+    sub = dict(cfg, n=n, buff=min(cfg["buff"] * (cfg["n"] / n) ** (1 / cfg["dim"]), 0.15))
+    ic = make_ic(sub)
+    t0 = time.perf_counter()
+
+    def gpu(spec, w):
+        with Context(dim=sub["dim"], k=sub["k"], buff=sub["buff"], boundary=sub["boundary"], flux="physical",
+                     gamma=ic.gamma, precision=spec["precision"]) as ctx:
+            if spec["kbudget"] and w is not None:
+                ctx.kbudget_enable(train_steps=0, iters_per_step=1, quantile=0.98, seed=1)
+                ctx.kbudget_weights(set_to=w)
+            ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+            dts = [ctx.sim_step(sub["cfl"]) for _ in range(steps)]
+            vol = ctx.download_volumes()[: ic.n]
+            x, m, p, e = ctx.sim_get()
+            kb = ctx.kbudget_stats() if spec["kbudget"] else None
+        return (dts, x, m, p, e, vol), kb
+
+    head, kb = gpu(FORMS[form], weights)
+    plain, _ = gpu(FORMS[PLAIN_FORM], None)
+    t_gpu = time.perf_counter() - t0
+    ora = check.oracle_moving_run(ic, sub["k"], sub["buff"], sub["boundary"], steps, cfl=sub["cfl"])
+    out = {"workload": f"{sub.get('ic', 'uniform')} 3D Sedov, {n} points (seed {sub['seed']}), buff "
+                       f"{sub['buff']:.4f}, {steps} moving-mesh steps from the initial condition",
+           "oracle": "om_build_mesh (hydro cells, K then growing budgets) + om_step_moving, FP64",
+           form: check.state_errors(head, ora), PLAIN_FORM: check.state_errors(plain, ora),
+           "seconds_gpu": t_gpu, "seconds_oracle": time.perf_counter() - t0 - t_gpu}
+    if kb:
+        out[form]["learned_k"] = {"mean_k": kb["mean_k"], "misses": kb["misses"], "cells": kb["cells"]}
     return out
 
 
@@ -359,15 +429,22 @@ def run_ours(args, rank, world, local_rank):
     names = [HEADLINE] if args.headline_only else [PLAIN_FORM, HEADLINE] if args.skip_forms else list(FORMS)
     res = {}
     ref_state = None  # the plain form runs first; every other form is compared with it
+    want_check = not args.skip_oracle and rank == 0 and not cfg.get("batch") and cfg["dim"] == 3
     for f in names:
         res[f] = time_form(args, cfg, ic, local_rank, dist, f, want_e2e=(f == HEADLINE and not args.skip_e2e),
-                           want_clocks=(f == HEADLINE), want_state=PLAIN_FORM in names)
+                           want_clocks=(f == HEADLINE), want_state=PLAIN_FORM in names,
+                           want_check=want_check and f == HEADLINE)
         st = res[f].pop("state", None)
         if f == PLAIN_FORM:
             ref_state = st
         elif ref_state is not None and st is not None:
             res[f]["vs_plain"] = compare_states(ref_state, st)
         del st
+    oracle_check = None
+    if want_check:
+        oracle_check = dict(res[HEADLINE].pop("checks"))
+        oracle_check["form"] = HEADLINE
+        oracle_check["density_run"] = density_check(cfg, HEADLINE, res[HEADLINE].get("weights"))
     _barrier(dist)
     if dist:
         dist.destroy_process_group()
@@ -473,9 +550,13 @@ def run_ours(args, rank, world, local_rank):
                          f"{stats['n_hydro'] * cfg['k'] * 4 / 2 ** 20:.0f} MiB at the plain K",
                    "parallelism": f"replicas x{world}"},
         "speedup_vs_plain_gpu": value / rate(base) if base else None,
-        # the headline's state after the timed steps against the plain FP64 form's (same IC,
+        # the headline's state after the timed steps against the plain FP64 GPU form's (same IC,
         # same steps): 0 cells differing and 0 L1 error = the same meshes and fluxes every step
-        "matched_l1": ({"vs": PLAIN_FORM, **head["vs_plain"]} if "vs_plain" in head else None),
+        "matched_l1": ({"vs": f"{PLAIN_FORM} (the plain GPU form, not the oracle)", **head["vs_plain"]}
+                       if "vs_plain" in head else None),
+        # the oracle's checks: sampled cells of the full-size meshes, and the density error of a
+        # whole run against the oracle's own run (oracle/check.py; outside the timed region)
+        "oracle_check": oracle_check,
         "roofline": roof, "roofline_hydro": roof_hydro,
         "stages_ms": dict(zip(STAGES, stage)),
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"], "forms": forms,

@@ -114,18 +114,47 @@ int pgpu_knn_sorted(pgpu_ctx *ctx, double *sorted_pts, uint32_t *perm, int *n_gr
  * device; sizes are returned. */
 int pgpu_periodic_mesh(pgpu_ctx *ctx, const double *pts, int64_t n, int64_t *n_seeds, int64_t *num_faces);
 
-/* voronoi::compute_mesh (src/voronoi/voronoi.cpp:103-151) on n points already
+/* voronoi::compute_mesh (src/voronoi/voronoi.cpp:17-64) on n points already
  * in the unit box: no ghosts, no scaling; n_hydro = n. */
 int pgpu_compute_mesh(pgpu_ctx *ctx, const double *pts, int64_t n, int64_t *num_faces);
 
 /* Copies the current mesh to host arrays in the reference's VMesh layout,
  * cells in input order with faces contiguous per cell
- * (src/voronoi/voronoi.cpp:298-419 unpermute_vmesh).  Any pointer may be NULL.
+ * (src/voronoi/voronoi.cpp:212-333 unpermute_vmesh).  Any pointer may be NULL.
  * status and cert_k are per cell; cert_k is the 1-based neighbour index at which
  * the certificate closed (0 if it did not); centroid is an extension. */
 int pgpu_download_mesh(pgpu_ctx *ctx, double *seeds, double *volumes, uint64_t *face_counts,
                        uint64_t *face_ptr, int32_t *neighbor, double *normal, double *area,
                        uint64_t *ghost_ids, int32_t *status, int32_t *cert_k, double *centroid);
+
+/* ------------------------------------------------------ mesh checkers ---
+ * Diagnostics with no reference counterpart: read parts of the current mesh
+ * back without downloading all of it, so that a checker can recompute sampled
+ * cells of a full-size mesh on the host.  They allocate and free staging
+ * memory and synchronise the stream.
+ *
+ * pgpu_download_points: the extended point set the mesh was built on, hydro
+ * points then ghosts (extended ids), in the unit box (n_seeds x dim doubles),
+ * exactly the coordinates the KNN and the clipping used. */
+int pgpu_download_points(pgpu_ctx *ctx, double *ext_unit);
+
+/* The query slots of the hydro cells that the last mesh build certified by the
+ * grid walk (cells whose security sphere reaches past every neighbour budget):
+ * *count receives their number; out (capacity cap) may be NULL. */
+int pgpu_walked_slots(pgpu_ctx *ctx, uint32_t *out, int64_t cap, int64_t *count);
+
+/* n sampled query slots (0 <= slot < number of cells the last build computed;
+ * slot order is the mesh's internal spatial order): per slot its extended id,
+ * the neighbour row the main clipping pass used (lists: n x k extended ids;
+ * list_len = the budget it had, k or the cell's learned budget, the rest of
+ * the row UINT32_MAX), status, cert_k,
+ * volume and centroid (physical units, as pgpu_download_mesh), and the
+ * cell's faces in stored order: face_ptr (n + 1 entries, always filled),
+ * neighbor / normal (x 3) / area (physical units) of capacity face_cap, or all
+ * three NULL to get face_ptr only.  PGPU_ECAPACITY if face_ptr[n] > face_cap. */
+int pgpu_sample_cells(pgpu_ctx *ctx, const uint32_t *slots, int64_t n, uint32_t *ext_id, uint16_t *list_len,
+                      uint32_t *lists, int32_t *status, int32_t *cert_k, double *volumes, double *centroid,
+                      uint64_t *face_ptr, int32_t *neighbor, double *normal, double *area, int64_t face_cap);
 
 /* Mesh sizes: cells (hydro + ghost), hydro cells, faces. */
 int pgpu_mesh_sizes(pgpu_ctx *ctx, int64_t *n_seeds, int64_t *n_hydro, int64_t *num_faces);
@@ -163,8 +192,12 @@ int pgpu_hydro_step(pgpu_ctx *ctx, double dt);
  * any device work.  Nothing in the scratch has to start at zero.  The first
  * call on each device looks up the scratch's address (cudaGetSymbolAddress)
  * with that device current; make that first call before capturing work on a
- * stream.  Calls that overlap on one device (other threads, other streams)
- * share the scratch and race: order them.
+ * stream.  The address is kept per device ordinal for the life of the process
+ * and belongs to that device's primary context (the runtime's): a caller that
+ * drives the device through a context of its own, or that resets the device
+ * after the first call, must not use this entry point.  Calls that overlap on
+ * one device (other threads, other streams) share the scratch and race: order
+ * them.
  *   Runs on the current device, on `stream` (a cudaStream_t; NULL = the legacy
  * default stream), and waits for it before writing *dt on the host. */
 #define PGPU_DT_STATIC_MAX_CELLS 16777216

@@ -74,6 +74,14 @@ def lib():
         L.om_set_predicate_mode.argtypes = [C.c_int]
         L.om_set_fallback_k.argtypes = [C.c_int]
         L.om_set_boundary_mode.argtypes = [C.c_int]
+        L.om_set_expand_k.argtypes = [C.c_int]
+        L.om_grid_new.argtypes = [C.c_int, _dp, C.c_long]
+        L.om_grid_new.restype = C.c_void_p
+        L.om_grid_free.argtypes = [C.c_void_p]
+        L.om_grid_knn.argtypes = [C.c_void_p, _lp, C.c_long, C.c_int, _up]
+        L.om_cells_list.argtypes = [C.c_int, _dp, C.c_long, _lp, C.c_long, _up, C.c_int, C.POINTER(_Mesh)]
+        L.om_cells_certified.argtypes = [C.c_void_p, _dp, C.c_long, _lp, C.c_long, C.c_int, C.c_int,
+                                         C.POINTER(_Mesh), _ip]
         _LIB = L
     return _LIB
 
@@ -159,19 +167,72 @@ def cells(ext_unit: np.ndarray, n_hydro: int, knn_lists: np.ndarray, n_compute: 
     return _wrap(m)
 
 
+class Grid:
+    """The KNN grid of one extended unit-box point set (om_grid_new): exact K
+    nearest neighbours of listed queries, each row identical to the one
+    :func:`knn` gives that point."""
+
+    def __init__(self, ext_unit: np.ndarray):
+        self.ext = np.ascontiguousarray(ext_unit, np.float64)
+        self.dim = self.ext.shape[1]
+        self._g = lib().om_grid_new(self.dim, self.ext.ravel(), len(self.ext))
+
+    def knn(self, queries, k: int) -> np.ndarray:
+        q = np.ascontiguousarray(queries, np.int64)
+        out = np.zeros(max(len(q), 1) * k, np.uint32)
+        lib().om_grid_knn(self._g, q, len(q), k, out)
+        return out[: len(q) * k].reshape(len(q), k)
+
+    def close(self):
+        if getattr(self, "_g", None):
+            lib().om_grid_free(self._g)
+            self._g = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def cells_list(ext_unit: np.ndarray, ids, knn_rows: np.ndarray) -> Mesh:
+    """Listed cells clipped with their neighbour rows (om_cells_list): cell t of the
+    result is ids[t]; unit-box units; face neighbours are extended ids."""
+    ext = np.ascontiguousarray(ext_unit, np.float64)
+    ids = np.ascontiguousarray(ids, np.int64)
+    kl = np.ascontiguousarray(knn_rows, np.uint32)
+    m = _Mesh()
+    lib().om_cells_list(ext.shape[1], ext.ravel(), len(ext), ids, len(ids), kl.ravel(), kl.shape[1], C.byref(m))
+    return _wrap(m)
+
+
+def cells_certified(grid: Grid, ids, k0: int = 190, k_max: int = 1 << 16):
+    """Listed cells clipped by the reference's algorithm with a budget large enough to
+    certify each (om_cells_certified): K0 neighbours, then 4x budgets up to k_max for
+    the cells whose certificate did not close.  Returns (mesh, budget of the final
+    attempt per cell)."""
+    ids = np.ascontiguousarray(ids, np.int64)
+    m = _Mesh()
+    ku = np.zeros(max(len(ids), 1), np.int32)
+    lib().om_cells_certified(grid._g, grid.ext.ravel(), len(grid.ext), ids, len(ids), k0, k_max, C.byref(m), ku)
+    return _wrap(m), ku[: len(ids)]
+
+
 def build_mesh(pts: np.ndarray, k: int, buff: float = 0.04, boundary: int = PERIODIC,
-               hydro_only: bool = False, robust: bool = False, k_fallback: int = 0) -> Mesh:
-    """The whole mesh build.  robust / k_fallback: the moving-mesh extensions (om.h)."""
+               hydro_only: bool = False, robust: bool = False, k_fallback: int = 0, expand_k: int = 0) -> Mesh:
+    """The whole mesh build.  robust / k_fallback / expand_k: the moving-mesh extensions (om.h)."""
     pts = np.ascontiguousarray(pts, np.float64)
     m = _Mesh()
     L = lib()
     L.om_set_predicate_mode(1 if robust else 0)
     L.om_set_fallback_k(k_fallback)
+    L.om_set_expand_k(expand_k)
     try:
         L.om_build_mesh(pts.shape[1], boundary, buff, k, pts.ravel(), len(pts), int(hydro_only), C.byref(m))
     finally:
         L.om_set_predicate_mode(0)
         L.om_set_fallback_k(0)
+        L.om_set_expand_k(0)
     return _wrap(m)
 
 

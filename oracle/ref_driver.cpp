@@ -10,7 +10,7 @@
 //
 // Nothing here re-implements reference behaviour: every entry point forwards to
 // the reference's own functions.  The one exception is ref_compute_mesh, which
-// repeats the call sequence of voronoi::compute_mesh (voronoi.cpp:103-151) so
+// repeats the call sequence of voronoi::compute_mesh (voronoi.cpp:17-64) so
 // that the per-cell Status vector it builds can be returned to the caller.
 //
 // The product never links this: only tests, smoke() and bench.py's CPU arms do.
@@ -113,7 +113,7 @@ REF_API void* ref_periodic_mesh(const double* pts, long n) {
     return voronoi::compute_periodic_mesh((POINT_TYPE*)pts, (hsize_t)n);
 }
 
-// The call sequence of voronoi::compute_mesh (voronoi.cpp:103-151) on n points
+// The call sequence of voronoi::compute_mesh (voronoi.cpp:17-64) on n points
 // already in [0,1]^D, additionally returning each cell's Status in input
 // order.  NULL when the grid would be below 16^D.
 REF_API void* ref_compute_mesh(const double* pts, long n, int* status_out) {

@@ -78,8 +78,8 @@ def load(dim: int, k: int):
     path = lib_path(dim, k)
     if path not in _LIBS:
         if not os.path.exists(path):
-            raise FileNotFoundError(f"library {path} missing (run `make -C oracle ref` or "
-                                    "`make -C proteusgpu_b200/dropin`)")
+            raise FileNotFoundError(f"library {path} missing (run `make -C oracle ref REF=<reference tree>` or "
+                                    "`make -C proteusgpu_b200/dropin REF=<reference tree>`)")
         _LIBS[path] = _bind(C.CDLL(path, mode=os.RTLD_LOCAL))
     return _LIBS[path]
 

@@ -9,7 +9,7 @@
  *   - exact K nearest neighbours               (src/knn/knn.cpp:16-347)
  *   - Ray et al. half-space clipping + security-radius certificate
  *                                              (src/voronoi/cell.cpp:42-411,
- *                                               src/voronoi/voronoi.cpp:201-241)
+ *                                               src/voronoi/voronoi.cpp:115-155)
  *   - cell -> mesh extraction                  (src/voronoi/cell.cpp:416-669)
  *   - CFL time step and HLL flux update        (src/hydro/finite_volume_solver.cpp:43-186,
  *                                               src/hydro/riemann.cpp:7-124)
@@ -101,6 +101,17 @@ void om_get_counters(long *out4);
  * knn.cpp:16-315.  Returns 0. */
 int om_knn(int dim, const double *pts, long n, int K, uint32_t *out);
 
+/* Exact K nearest neighbours of listed queries (checker extension): the grid
+ * of om_knn built once for a point set (which must outlive it), and per query
+ * the same ring order and stopping rule, hence the same row as om_knn gives
+ * that point; the best K are selected from a candidate buffer, so large K
+ * (thousands) stays cheap.  out is nq x K. */
+typedef struct om_grid om_grid;
+om_grid *om_grid_new(int dim, const double *pts, long n);
+void om_grid_free(om_grid *g);
+int om_grid_dim(const om_grid *g);
+int om_grid_knn(const om_grid *g, const long *queries, long nq, int K, uint32_t *out);
+
 /* ---- cells ------------------------------------------------------------- */
 
 /* Clips and extracts cells [0, n_cells) of the extended unit-box point set
@@ -117,6 +128,17 @@ int om_build_mesh(int dim, int boundary, double buff, int K, const double *pts, 
 
 void om_mesh_free(om_mesh *mesh);
 
+/* Checker extensions.  om_cells_list clips the listed cells ids[0, nq) with
+ * their neighbour rows knn (nq x K) as om_cells does; the result's cell t is
+ * ids[t] (n_seeds = nq, unit-box units, extended ids as face neighbours).
+ * om_cells_certified clips them with K0 neighbours and again with 4x budgets,
+ * up to k_max, while their certificate does not close: the reference's
+ * algorithm with a _K_ large enough for each cell.  k_used may be NULL. */
+int om_cells_list(int dim, const double *ext, long n_ext, const long *ids, long nq, const uint32_t *knn, int K,
+                  om_mesh *mesh);
+int om_cells_certified(const om_grid *g, const double *ext, long n_ext, const long *ids, long nq, int K0,
+                       int k_max, om_mesh *mesh, int *k_used);
+
 /* Test hook: 0 = the reference's boundary walk (default), 1 = the set-based
  * cavity boundary that the CUDA kernel uses. */
 void om_set_boundary_mode(int mode);
@@ -129,6 +151,11 @@ void om_set_boundary_mode(int mode);
  *   certificate did not close within K with the larger budget. */
 void om_set_predicate_mode(int mode);
 void om_set_fallback_k(int k);
+/* Extension (default 0 = off): in hydro-only builds, hydro cells whose
+ * certificate did not close within K are clipped again by om_cells_certified
+ * with budgets from 4K up to k_max (the cells the CUDA path certifies by its
+ * grid walk). */
+void om_set_expand_k(int k_max);
 
 /* ---- hydro ------------------------------------------------------------- */
 

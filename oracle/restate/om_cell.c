@@ -3,7 +3,7 @@
  * Voronoi cells by half-space clipping + extraction (test-infrastructure oracle).
  *
  * Restates the reference's ConvexCell (src/voronoi/cell.cpp:42-411), the cell
- * loop of cpu_compute_cell (src/voronoi/voronoi.cpp:201-241) and
+ * loop of cpu_compute_cell (src/voronoi/voronoi.cpp:115-155) and
  * extract_cell_to_vmesh (src/voronoi/cell.cpp:416-669), which follow Ray,
  * Sokolov, Lefebvre, Levy, "Meshless Voronoi on the GPU", ACM TOG 37(6), 2018.
  * A cell is kept in dual form: planes (a, b, c, d) with a.x + d >= 0 inside,
@@ -541,15 +541,16 @@ static void extract(const cell_t *c, cell_out_t *o) {
     }
 }
 
-/* ---- cell loop (voronoi.cpp:201-241) ---- */
-static void one_cell(int dim, const double *ext, long i, const uint32_t *knn, int K, cell_out_t *o, int *status,
+/* ---- cell loop (voronoi.cpp:115-155) ---- */
+/* row: the cell's K neighbour ids (knn + K * i in a full list) */
+static void one_cell(int dim, const double *ext, long i, const uint32_t *row, int K, cell_out_t *o, int *status,
                      int *cert_k) {
     cell_t c;
     cell_init(&c, dim, ext, i);
     c.n_pred = c.n_newv = 0;
     *cert_k = 0;
     for (int v = 0; v < K; v++) {
-        uint32_t z = knn[(long)K * i + v];
+        uint32_t z = row[v];
         if (z == UINT32_MAX) break;
         clip(&c, z);
         double nb[4];
@@ -560,7 +561,7 @@ static void one_cell(int dim, const double *ext, long i, const uint32_t *knn, in
         }
         if (c.status != OM_SUCCESS) break;
     }
-    uint32_t last = knn[(long)K * i + K - 1];
+    uint32_t last = row[K - 1];
     if (last == UINT32_MAX) {
         c.status = OM_SECURITY_RADIUS_NOT_REACHED;
     } else {
@@ -612,7 +613,7 @@ int om_cells(int dim, const double *ext, long n_ext, long n_hydro, const uint32_
                 o->volume = 0;
                 continue;
             }
-            one_cell(dim, ext, i, knn, K, o, &m->status[i], &m->cert_k[i]);
+            one_cell(dim, ext, i, knn + (long)K * i, K, o, &m->status[i], &m->cert_k[i]);
             /* extract_cell_to_vmesh writes the seed only for extracted cells
                (cell.cpp:418-420); the others keep calloc's zeros */
             if (m->status[i] == OM_SUCCESS) {
@@ -662,8 +663,145 @@ void om_mesh_free(om_mesh *m) {
     memset(m, 0, sizeof(*m));
 }
 
+/* ---- listed cells (checker extension) ----
+ * Cells ids[0, nq) of the extended point set clipped with their rows of `knn`
+ * (nq x K, in list order) exactly as om_cells clips them; the result is a mesh
+ * whose cell t is ids[t] (unit-box units, face neighbours are extended ids). */
+int om_cells_list(int dim, const double *ext, long n_ext, const long *ids, long nq, const uint32_t *knn, int K,
+                  om_mesh *m) {
+    (void)n_ext;
+    memset(m, 0, sizeof(*m));
+    m->dim = dim;
+    m->n_seeds = nq;
+    m->n_hydro = nq;
+    m->seeds = (double *)calloc(nq * 3 + 3, sizeof(double));
+    m->volumes = (double *)calloc(nq + 1, sizeof(double));
+    m->face_counts = (long *)calloc(nq + 1, sizeof(long));
+    m->face_ptr = (long *)calloc(nq + 1, sizeof(long));
+    m->status = (int *)calloc(nq + 1, sizeof(int));
+    m->cert_k = (int *)calloc(nq + 1, sizeof(int));
+    m->centroid = (double *)calloc(nq * 3 + 3, sizeof(double));
+    cell_out_t *outs = (cell_out_t *)malloc((nq > 0 ? nq : 1) * sizeof(cell_out_t));
+#pragma omp parallel for schedule(dynamic, 4)
+    for (long t = 0; t < nq; t++) {
+        one_cell(dim, ext, ids[t], knn + (long)K * t, K, &outs[t], &m->status[t], &m->cert_k[t]);
+        if (m->status[t] == OM_SUCCESS)
+            for (int k = 0; k < dim; k++) m->seeds[3 * t + k] = ext[dim * ids[t] + k];
+    }
+    long F = 0;
+    for (long t = 0; t < nq; t++) F += outs[t].nf;
+    m->neighbor = (int *)malloc((F + 1) * sizeof(int));
+    m->normal = (double *)malloc((F + 1) * 3 * sizeof(double));
+    m->area = (double *)malloc((F + 1) * sizeof(double));
+    F = 0;
+    for (long t = 0; t < nq; t++) {
+        const cell_out_t *o = &outs[t];
+        m->face_ptr[t] = F;
+        m->face_counts[t] = o->nf;
+        m->volumes[t] = o->volume;
+        if (m->status[t] == OM_SUCCESS)
+            for (int k = 0; k < 3; k++) m->centroid[3 * t + k] = o->centroid[k];
+        for (int f = 0; f < o->nf; f++, F++) {
+            m->neighbor[F] = o->neighbor[f];
+            for (int k = 0; k < 3; k++) m->normal[3 * F + k] = o->normal[f][k];
+            m->area[F] = o->area[f];
+        }
+    }
+    m->num_faces = F;
+    free(outs);
+    return 0;
+}
+
+/* m <- per cell i: b's cell sel[i] where sel[i] >= 0, else m's own */
+static void merge_cells(om_mesh *m, const om_mesh *b, const long *sel) {
+    long F = 0;
+    for (long i = 0; i < m->n_seeds; i++) F += sel[i] >= 0 ? b->face_counts[sel[i]] : m->face_counts[i];
+    int *nb = (int *)malloc((F + 1) * sizeof(int));
+    double *nr = (double *)malloc((F + 1) * 3 * sizeof(double));
+    double *ar = (double *)malloc((F + 1) * sizeof(double));
+    long *fp = (long *)malloc((m->n_seeds + 1) * sizeof(long));
+    long *fc = (long *)malloc((m->n_seeds + 1) * sizeof(long));
+    long f = 0;
+    for (long i = 0; i < m->n_seeds; i++) {
+        const om_mesh *s = sel[i] >= 0 ? b : m;
+        const long j = sel[i] >= 0 ? sel[i] : i;
+        fp[i] = f;
+        fc[i] = s->face_counts[j];
+        for (long q = 0; q < s->face_counts[j]; q++, f++) {
+            long g = s->face_ptr[j] + q;
+            nb[f] = s->neighbor[g];
+            for (int k = 0; k < 3; k++) nr[3 * f + k] = s->normal[3 * g + k];
+            ar[f] = s->area[g];
+        }
+        if (sel[i] >= 0) {
+            m->volumes[i] = b->volumes[j];
+            m->status[i] = b->status[j];
+            m->cert_k[i] = b->cert_k[j];
+            for (int k = 0; k < 3; k++) m->centroid[3 * i + k] = b->centroid[3 * j + k], m->seeds[3 * i + k] = b->seeds[3 * j + k];
+        }
+    }
+    free(m->neighbor);
+    free(m->normal);
+    free(m->area);
+    free(m->face_ptr);
+    free(m->face_counts);
+    m->neighbor = nb;
+    m->normal = nr;
+    m->area = ar;
+    m->face_ptr = fp;
+    m->face_counts = fc;
+    m->num_faces = F;
+}
+
+/* Listed cells clipped by the reference's algorithm with a budget large enough
+ * to certify them: first K0 neighbours; every cell whose certificate did not
+ * close (SECURITY_RADIUS_NOT_REACHED) is clipped again from scratch with 4x the
+ * budget, up to k_max.  Since the clipping loop stops at the neighbour that
+ * closes the certificate (voronoi.cpp:138), a certified result is the one the
+ * reference gives with any _K_ at or beyond that neighbour.  k_used[t] (may be
+ * NULL) receives the budget of the final attempt. */
+int om_cells_certified(const om_grid *g, const double *ext, long n_ext, const long *ids, long nq, int K0,
+                       int k_max, om_mesh *m, int *k_used) {
+    const int dim = om_grid_dim(g);
+    uint32_t *kl = (uint32_t *)malloc(((size_t)nq * K0 + 1) * sizeof(uint32_t));
+    om_grid_knn(g, ids, nq, K0, kl);
+    om_cells_list(dim, ext, n_ext, ids, nq, kl, K0, m);
+    free(kl);
+    if (k_used)
+        for (long t = 0; t < nq; t++) k_used[t] = K0;
+    int K = K0;
+    long *sel = (long *)malloc((nq + 1) * sizeof(long));
+    long *sub = (long *)malloc((nq + 1) * sizeof(long));
+    long *pos = (long *)malloc((nq + 1) * sizeof(long));
+    while (K < k_max) {
+        long ns = 0;
+        for (long t = 0; t < nq; t++)
+            if (m->status[t] == OM_SECURITY_RADIUS_NOT_REACHED) sub[ns] = ids[t], pos[ns] = t, ns++;
+        if (!ns) break;
+        K = 4 * K < k_max ? 4 * K : k_max;
+        uint32_t *k2 = (uint32_t *)malloc(((size_t)ns * K + 1) * sizeof(uint32_t));
+        om_grid_knn(g, sub, ns, K, k2);
+        om_mesh b;
+        om_cells_list(dim, ext, n_ext, sub, ns, k2, K, &b);
+        free(k2);
+        for (long t = 0; t < nq; t++) sel[t] = -1;
+        for (long s = 0; s < ns; s++) {
+            sel[pos[s]] = s;
+            if (k_used) k_used[pos[s]] = K;
+        }
+        merge_cells(m, &b, sel);
+        om_mesh_free(&b);
+    }
+    free(sel);
+    free(sub);
+    free(pos);
+    return 0;
+}
+
 int om_fallback_k = 0;
 void om_set_fallback_k(int k) { om_fallback_k = k; }
+int om_expand_k_max = 0;
+void om_set_expand_k(int k_max) { om_expand_k_max = k_max; }
 
 /* m <- per cell: b's result where m's hydro cell was SECURITY_RADIUS_NOT_REACHED, else m's */
 static void merge_refit(om_mesh *m, const om_mesh *b, long n_hydro) {
@@ -716,10 +854,43 @@ int om_build_mesh(int dim, int boundary, double buff, int K, const double *pts, 
     long *gsrc = (long *)malloc((size_t)nreg * (n > 0 ? n : 1) * sizeof(long));
     int *gcode = (int *)malloc((size_t)nreg * (n > 0 ? n : 1) * sizeof(int));
     long ntot = om_ghosts(dim, boundary, buff, pts, n, ext, gsrc, gcode);
-    uint32_t *knn = (uint32_t *)malloc((size_t)ntot * K * sizeof(uint32_t));
-    om_knn(dim, ext, ntot, K, knn);
+    uint32_t *knn = (uint32_t *)malloc(((size_t)ntot * K + 1) * sizeof(uint32_t));
+    om_grid *grid = NULL;
+    if (hydro_only) {
+        /* only the hydro cells are clipped: only their rows are searched (the
+           same lists as om_knn's first n rows) */
+        grid = om_grid_new(dim, ext, ntot);
+        long *q = (long *)malloc((n + 1) * sizeof(long));
+        for (long i = 0; i < n; i++) q[i] = i;
+        om_grid_knn(grid, q, n, K, knn);
+        free(q);
+    } else {
+        om_knn(dim, ext, ntot, K, knn);
+    }
     om_cells(dim, ext, ntot, n, knn, K, hydro_only ? n : ntot, m);
     free(knn);
+    if (hydro_only && om_expand_k_max > K) {
+        /* extension: hydro cells whose certificate did not close within K are
+           clipped again with growing budgets up to om_expand_k_max */
+        long nunc = 0;
+        for (long i = 0; i < n; i++) nunc += m->status[i] == OM_SECURITY_RADIUS_NOT_REACHED;
+        if (nunc) {
+            long *ids = (long *)malloc(nunc * sizeof(long));
+            long *sel = (long *)malloc((ntot + 1) * sizeof(long));
+            nunc = 0;
+            for (long i = 0; i < ntot; i++) {
+                sel[i] = -1;
+                if (i < n && m->status[i] == OM_SECURITY_RADIUS_NOT_REACHED) sel[i] = nunc, ids[nunc++] = i;
+            }
+            om_mesh b;
+            om_cells_certified(grid, ext, ntot, ids, nunc, 4 * K, om_expand_k_max, &b, NULL);
+            merge_cells(m, &b, sel);
+            om_mesh_free(&b);
+            free(ids);
+            free(sel);
+        }
+    }
+    om_grid_free(grid);
     if (hydro_only && om_fallback_k > K) {
         /* extension: hydro cells whose certificate did not close within K are
            recomputed with the fallback budget (the other cells keep their K result) */

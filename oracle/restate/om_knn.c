@@ -145,3 +145,129 @@ int om_knn(int dim, const double *pts, long n, int K, uint32_t *out) {
     free(bin);
     return 0;
 }
+
+/* ---- exact K nearest neighbours of listed queries (checker extension) ----
+ * The same grid (N_grid from knn.cpp:22), the same Chebyshev-ring order and the
+ * same stopping rule as om_knn, so a query's list is identical to its om_knn
+ * row; only the listed queries are searched, and the best K are kept by
+ * selection over a candidate buffer instead of insertion, so that budgets of
+ * thousands of neighbours stay cheap.  The grid is built once per point set. */
+struct om_grid {
+    int dim, G;
+    long n;
+    const double *pts;
+    long *start, *order;
+};
+
+om_grid *om_grid_new(int dim, const double *pts, long n) {
+    om_grid *g = (om_grid *)calloc(1, sizeof(om_grid));
+    g->dim = dim;
+    g->n = n;
+    g->pts = pts;
+    g->G = n_grid_for(n, dim);
+    const int G = g->G;
+    const long nb = dim == 2 ? (long)G * G : (long)G * G * G;
+    g->start = (long *)calloc(nb + 1, sizeof(long));
+    g->order = (long *)malloc((n > 0 ? n : 1) * sizeof(long));
+    int *bin = (int *)malloc((n > 0 ? n : 1) * sizeof(int));
+    for (long i = 0; i < n; i++) {
+        const double *p = pts + i * dim;
+        int b = bin_coord(p[0], G) + G * bin_coord(p[1], G);
+        if (dim == 3) b += G * G * bin_coord(p[2], G);
+        bin[i] = b;
+        g->start[b + 1]++;
+    }
+    for (long b = 0; b < nb; b++) g->start[b + 1] += g->start[b];
+    long *fill = (long *)calloc(nb, sizeof(long));
+    for (long i = 0; i < n; i++) g->order[g->start[bin[i]] + fill[bin[i]]++] = i;
+    free(fill);
+    free(bin);
+    return g;
+}
+
+int om_grid_dim(const om_grid *g) { return g->dim; }
+
+void om_grid_free(om_grid *g) {
+    if (!g) return;
+    free(g->start);
+    free(g->order);
+    free(g);
+}
+
+typedef struct {
+    double d;
+    uint32_t i;
+} om_cand;
+
+static int cmp_cand(const void *a, const void *b) {
+    const om_cand *x = (const om_cand *)a, *y = (const om_cand *)b;
+    if (x->d < y->d) return -1;
+    if (x->d > y->d) return 1;
+    return (x->i > y->i) - (x->i < y->i);
+}
+
+int om_grid_knn(const om_grid *g, const long *queries, long nq, int K, uint32_t *out) {
+    const int dim = g->dim, G = g->G;
+    const double *pts = g->pts;
+#pragma omp parallel
+    {
+        long cap = 4096;
+        om_cand *buf = (om_cand *)malloc(cap * sizeof(om_cand));
+#pragma omp for schedule(dynamic, 16)
+        for (long t = 0; t < nq; t++) {
+            const long q = queries[t];
+            const double *p = pts + q * dim;
+            int c[3] = {bin_coord(p[0], G), bin_coord(p[1], G), dim == 3 ? bin_coord(p[2], G) : 0};
+            long cnt = 0;
+            int have = 0;
+            double kth = 0.0;
+            for (int r = 0; r <= G; r++) {
+                if (r >= 1 && have) {
+                    double md = (double)(r - 1) / (double)G;
+                    if (kth < md * md) break;
+                }
+                int zlo = dim == 3 ? -r : 0, zhi = dim == 3 ? r : 0;
+                for (int dz = zlo; dz <= zhi; dz++) {
+                    int z = c[2] + dz;
+                    if (dim == 3 && (z < 0 || z >= G)) continue;
+                    for (int dy = -r; dy <= r; dy++) {
+                        int y = c[1] + dy;
+                        if (y < 0 || y >= G) continue;
+                        for (int dx = -r; dx <= r; dx++) {
+                            int ar = abs(dx);
+                            if (abs(dy) > ar) ar = abs(dy);
+                            if (abs(dz) > ar) ar = abs(dz);
+                            if (ar != r) continue;
+                            int x = c[0] + dx;
+                            if (x < 0 || x >= G) continue;
+                            long b = x + (long)G * y + (long)G * G * z;
+                            for (long s = g->start[b]; s < g->start[b + 1]; s++) {
+                                long j = g->order[s];
+                                if (j == q) continue;
+                                double d = dist2(p, pts + j * dim, dim);
+                                if (have && d > kth) continue;
+                                if (cnt == cap) {
+                                    cap *= 2;
+                                    buf = (om_cand *)realloc(buf, cap * sizeof(om_cand));
+                                }
+                                buf[cnt].d = d;
+                                buf[cnt].i = (uint32_t)j;
+                                cnt++;
+                            }
+                        }
+                    }
+                }
+                if (cnt >= K) {
+                    qsort(buf, cnt, sizeof(om_cand), cmp_cand);
+                    cnt = K;
+                    kth = buf[K - 1].d;
+                    have = 1;
+                }
+            }
+            if (!have) qsort(buf, cnt, sizeof(om_cand), cmp_cand);
+            for (int k = 0; k < K; k++) out[t * K + k] = k < cnt ? buf[k].i : UINT32_MAX;
+        }
+        free(buf);
+    }
+    return 0;
+}

@@ -27,7 +27,7 @@ EXPORTED = [
     "pgpu_launch_count", "pgpu_fp64_peak", "pgpu_riemann_hll", "pgpu_dt_cfl_static",
     "pgpu_kbudget_enable", "pgpu_kbudget_classes", "pgpu_kbudget_stats", "pgpu_kbudget_weights",
     "pgpu_mlp_forward", "pgpu_mlp_grad", "pgpu_fp32_peak", "pgpu_batch_init", "pgpu_batch_dt", "pgpu_autotune",
-    "pgpu_set_tuning",
+    "pgpu_set_tuning", "pgpu_download_points", "pgpu_walked_slots", "pgpu_sample_cells",
 ]
 
 
@@ -120,6 +120,9 @@ def load(path: str = LIB_PATH):
     L.pgpu_kbudget_weights.argtypes = [vp, vp, vp]
     L.pgpu_mlp_forward.argtypes = [vp, vp, i64, vp, vp]
     L.pgpu_mlp_grad.argtypes = [vp, vp, vp, i64, vp, vp]
+    L.pgpu_download_points.argtypes = [vp, vp]
+    L.pgpu_walked_slots.argtypes = [vp, vp, i64, vp]
+    L.pgpu_sample_cells.argtypes = [vp, vp, i64] + [vp] * 11 + [i64]
     for name in EXPORTED:
         getattr(L, name)  # raises AttributeError if a declared symbol is missing
     _LIB = L

@@ -52,6 +52,25 @@ class Mesh:
         return int(len(self.neighbor))
 
 
+@dataclass
+class SampledCells:
+    """Cells of the current mesh read back by query slot (pgpu_sample_cells):
+    extended ids, the neighbour row of the main clipping pass (n x k, list_len
+    used), per-cell outputs (physical units) and the cells' faces as CSR."""
+    slots: np.ndarray
+    ext_id: np.ndarray
+    list_len: np.ndarray
+    lists: np.ndarray
+    status: np.ndarray
+    cert_k: np.ndarray
+    volumes: np.ndarray
+    centroid: np.ndarray
+    face_ptr: np.ndarray
+    neighbor: np.ndarray
+    normal: np.ndarray
+    area: np.ndarray
+
+
 class Context:
     """One device context: a CUDA stream plus the device buffers of one mesh/simulation.
 
@@ -137,7 +156,7 @@ class Context:
         return self.download_mesh() if download else None
 
     def compute_mesh(self, pts_unit: np.ndarray, download: bool = True) -> Mesh | None:
-        """voronoi::compute_mesh (src/voronoi/voronoi.cpp:103-151) on points in the unit box."""
+        """voronoi::compute_mesh (src/voronoi/voronoi.cpp:17-64) on points in the unit box."""
         pts = _c64(pts_unit)
         nf = C.c_int64()
         check(self._h, self._L.pgpu_compute_mesh(self._h, _ptr(pts), len(pts), C.byref(nf)), "pgpu_compute_mesh")
@@ -149,7 +168,7 @@ class Context:
         return ns.value, nh.value, nf.value
 
     def download_mesh(self) -> Mesh:
-        """The device mesh in VMesh layout (unpermute_vmesh, src/voronoi/voronoi.cpp:298-419)."""
+        """The device mesh in VMesh layout (unpermute_vmesh, src/voronoi/voronoi.cpp:212-333)."""
         n, nh, F = self.mesh_sizes()
         m = Mesh(self.dim, n, nh, np.zeros((n, 3)), np.zeros(n), np.zeros(n, np.uint64), np.zeros(n, np.uint64),
                  np.zeros(F, np.int32), np.zeros((F, 3)), np.zeros(F), np.zeros(n - nh, np.uint64),
@@ -159,6 +178,47 @@ class Context:
             _ptr(m.normal), _ptr(m.area), _ptr(m.ghost_ids), _ptr(m.status), _ptr(m.cert_k), _ptr(m.centroid)),
             "pgpu_download_mesh")
         return m
+
+    def download_volumes(self) -> np.ndarray:
+        """Volumes of the current mesh's cells in input order (hydro ids first), physical units."""
+        n, _, _ = self.mesh_sizes()
+        vol = np.zeros(n)
+        check(self._h, self._L.pgpu_download_mesh(self._h, None, _ptr(vol), *([None] * 9)), "pgpu_download_mesh")
+        return vol
+
+    def download_points(self) -> np.ndarray:
+        """The extended unit-box point set of the current mesh (hydro points, then ghosts)."""
+        n, _, _ = self.mesh_sizes()
+        out = np.zeros((n, self.dim))
+        check(self._h, self._L.pgpu_download_points(self._h, _ptr(out)), "pgpu_download_points")
+        return out
+
+    def walked_slots(self) -> np.ndarray:
+        """Query slots of the cells the last build certified by the grid walk."""
+        cnt = C.c_int64()
+        check(self._h, self._L.pgpu_walked_slots(self._h, None, 0, C.byref(cnt)), "pgpu_walked_slots")
+        out = np.zeros(max(cnt.value, 1), np.uint32)
+        check(self._h, self._L.pgpu_walked_slots(self._h, _ptr(out), len(out), C.byref(cnt)), "pgpu_walked_slots")
+        return out[: cnt.value]
+
+    def sample_cells(self, slots) -> SampledCells:
+        """Cells of the current mesh by query slot, with their neighbour rows and faces."""
+        slots = _c64(slots, np.uint32)
+        n = len(slots)
+        ext = np.zeros(n, np.uint32)
+        ln = np.zeros(n, np.uint16)
+        rows = np.zeros((n, self.k), np.uint32)
+        st, ck = np.zeros(n, np.int32), np.zeros(n, np.int32)
+        vol, cen = np.zeros(n), np.zeros((n, 3))
+        fp = np.zeros(n + 1, np.uint64)
+        args = [_ptr(ext), _ptr(ln), _ptr(rows), _ptr(st), _ptr(ck), _ptr(vol), _ptr(cen), _ptr(fp)]
+        check(self._h, self._L.pgpu_sample_cells(self._h, _ptr(slots), n, *args, None, None, None, 0),
+              "pgpu_sample_cells")
+        F = int(fp[-1])
+        nb, nrm, ar = np.zeros(max(F, 1), np.int32), np.zeros((max(F, 1), 3)), np.zeros(max(F, 1))
+        check(self._h, self._L.pgpu_sample_cells(self._h, _ptr(slots), n, *args, _ptr(nb), _ptr(nrm), _ptr(ar),
+                                                 max(F, 1)), "pgpu_sample_cells")
+        return SampledCells(slots, ext, ln, rows, st, ck, vol, cen, fp.astype(np.int64), nb[:F], nrm[:F], ar[:F])
 
     def upload_mesh(self, m) -> None:
         """Makes a host VMesh (any object with the Mesh fields) the device mesh."""

@@ -363,6 +363,106 @@ int pgpu_mesh_sizes(pgpu_ctx* c, int64_t* n_seeds, int64_t* n_hydro, int64_t* nu
     return c->have_mesh ? PGPU_OK : PGPU_ESTATE;
 }
 
+// ------------------------------------------------------- mesh checkers
+int pgpu_download_points(pgpu_ctx* c, double* ext_unit) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_mesh || c->mesh_uploaded) return fail(c, PGPU_ESTATE, "pgpu_download_points: no mesh built here");
+    if (!ext_unit) return fail(c, PGPU_EINVAL, "pgpu_download_points: NULL output");
+    const int64_t n = c->n_ext;
+    if (n <= 0) return PGPU_OK;
+    DevBuf tmp;
+    CK(pgpu::ensure_bytes(tmp, (size_t)n * c->prm.dim * sizeof(double) + 16));
+    cudaError_t e = pgpu::launch_unpack_points(c, c->ext.p, n, (double*)tmp.p);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(ext_unit, tmp.p, (size_t)n * c->prm.dim * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    free_buf(tmp);
+    CK(e);
+    return PGPU_OK;
+}
+
+int pgpu_walked_slots(pgpu_ctx* c, uint32_t* out, int64_t cap, int64_t* count) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_mesh) return fail(c, PGPU_ESTATE, "pgpu_walked_slots: no mesh");
+    if (count) *count = c->n_pruned;
+    if (!out || c->n_pruned == 0) return PGPU_OK;
+    if (cap < c->n_pruned) return fail(c, PGPU_ECAPACITY, "pgpu_walked_slots: output too small");
+    CK(cudaMemcpyAsync(out, c->fb_qs.p, c->n_pruned * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return PGPU_OK;
+}
+
+int pgpu_sample_cells(pgpu_ctx* c, const uint32_t* slots, int64_t n, uint32_t* ext_id, uint16_t* list_len,
+                      uint32_t* lists, int32_t* status, int32_t* cert_k, double* volumes, double* centroid,
+                      uint64_t* face_ptr, int32_t* neighbor, double* normal, double* area, int64_t face_cap) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (!c->have_mesh || c->mesh_uploaded) return fail(c, PGPU_ESTATE, "pgpu_sample_cells: no mesh built here");
+    if (n < 0 || (n > 0 && (!slots || !ext_id || !list_len || !lists || !status || !cert_k || !volumes ||
+                            !centroid || !face_ptr)))
+        return fail(c, PGPU_EINVAL, "pgpu_sample_cells: bad arguments");
+    for (int64_t i = 0; i < n; i++)
+        if ((int64_t)slots[i] >= c->n_query) return fail(c, PGPU_EINVAL, "pgpu_sample_cells: slot out of range");
+    face_ptr[0] = 0;
+    if (n == 0) return PGPU_OK;
+    const int K = c->prm.k;  // row width of the output
+    // one staging allocation: slots, ext ids, face counts, face offsets, rows, lengths, per-cell outputs
+    const size_t o_slot = 0, o_ext = o_slot + 4 * n, o_fc = o_ext + 4 * n, o_ptr = (o_fc + 4 * n + 15) / 16 * 16,
+                 o_vol = o_ptr + 8 * (n + 1), o_cen = o_vol + 8 * n, o_st = o_cen + 24 * n, o_ck = o_st + 4 * n,
+                 o_rows = o_ck + 4 * n, o_len = o_rows + 4 * (size_t)n * K, bytes = o_len + 2 * n + 16;
+    DevBuf tmp;
+    CK(pgpu::ensure_bytes(tmp, bytes));
+    char* b = (char*)tmp.p;
+    std::vector<uint32_t> fc(n);
+    cudaError_t e = cudaMemcpyAsync(b + o_slot, slots, 4 * n, cudaMemcpyHostToDevice, c->stream);
+    if (!e)
+        e = pgpu::launch_sample_cells(c, (const uint32_t*)(b + o_slot), n, (uint32_t*)(b + o_ext),
+                                      (uint16_t*)(b + o_len), (uint32_t*)(b + o_rows), (int32_t*)(b + o_st),
+                                      (int32_t*)(b + o_ck), (double*)(b + o_vol), (double*)(b + o_cen),
+                                      (uint32_t*)(b + o_fc));
+    if (!e) e = cudaMemcpyAsync(ext_id, b + o_ext, 4 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaMemcpyAsync(list_len, b + o_len, 2 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaMemcpyAsync(lists, b + o_rows, 4 * (size_t)n * K, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaMemcpyAsync(status, b + o_st, 4 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaMemcpyAsync(cert_k, b + o_ck, 4 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaMemcpyAsync(volumes, b + o_vol, 8 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaMemcpyAsync(centroid, b + o_cen, 24 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaMemcpyAsync(fc.data(), b + o_fc, 4 * n, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaStreamSynchronize(c->stream);
+    if (e) {
+        free_buf(tmp);
+        CK(e);
+    }
+    for (int64_t i = 0; i < n; i++) face_ptr[i + 1] = face_ptr[i] + fc[i];
+    const int64_t F = (int64_t)face_ptr[n];
+    if (!neighbor || !normal || !area || F > face_cap) {
+        free_buf(tmp);
+        if (neighbor || normal || area)
+            return fail(c, PGPU_ECAPACITY, "pgpu_sample_cells: face arrays smaller than face_ptr[n]");
+        return PGPU_OK;
+    }
+    DevBuf fb;
+    e = pgpu::ensure_bytes(fb, (size_t)F * 36 + 64);
+    if (!e) e = cudaMemcpyAsync(b + o_ptr, face_ptr, 8 * (n + 1), cudaMemcpyHostToDevice, c->stream);
+    char* f = (char*)fb.p;
+    const size_t f_nrm = 0, f_area = f_nrm + 24 * (size_t)F, f_nb = f_area + 8 * (size_t)F;
+    if (!e)
+        e = pgpu::launch_sample_faces(c, (const uint32_t*)(b + o_ext), (const uint32_t*)(b + o_fc),
+                                      (const uint64_t*)(b + o_ptr), n, (int32_t*)(f + f_nb), (double*)(f + f_nrm),
+                                      (double*)(f + f_area));
+    if (!e && F) e = cudaMemcpyAsync(neighbor, f + f_nb, 4 * (size_t)F, cudaMemcpyDeviceToHost, c->stream);
+    if (!e && F) e = cudaMemcpyAsync(normal, f + f_nrm, 24 * (size_t)F, cudaMemcpyDeviceToHost, c->stream);
+    if (!e && F) e = cudaMemcpyAsync(area, f + f_area, 8 * (size_t)F, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaStreamSynchronize(c->stream);
+    free_buf(fb);
+    free_buf(tmp);
+    CK(e);
+    return PGPU_OK;
+}
+
 int pgpu_download_mesh(pgpu_ctx* c, double* seeds, double* volumes, uint64_t* face_counts, uint64_t* face_ptr,
                        int32_t* neighbor, double* normal, double* area, uint64_t* ghost_ids, int32_t* status,
                        int32_t* cert_k, double* centroid) {
@@ -371,18 +471,20 @@ int pgpu_download_mesh(pgpu_ctx* c, double* seeds, double* volumes, uint64_t* fa
     if (!c->have_mesh) return fail(c, PGPU_ESTATE, "pgpu_download_mesh: no mesh");
     const int64_t n = c->n_ext, F = c->num_faces, ng = c->n_ext - c->n_hydro;
     cudaError_t e = cudaSuccess;
-    uint32_t* nptr = ensure<uint32_t>(c->dl_ptr, n + 1, &e);
-    int32_t* nb = ensure<int32_t>(c->dl_a, F + 1, &e);
-    double* nrm = ensure<double>(c->dl_b, 3 * F + 3, &e);
-    double* ar = ensure<double>(c->dl_c, F + 1, &e);
-    CK(e);
-    CK(pgpu::launch_mesh_compact(c, nptr, nb, nrm, ar));
     std::vector<uint32_t> hptr(n + 1), hcnt(n + 1);
-    CK(cudaMemcpyAsync(hptr.data(), nptr, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+    if (face_ptr || neighbor || normal || area) {  // the face arrays in CSR order
+        uint32_t* nptr = ensure<uint32_t>(c->dl_ptr, n + 1, &e);
+        int32_t* nb = ensure<int32_t>(c->dl_a, F + 1, &e);
+        double* nrm = ensure<double>(c->dl_b, 3 * F + 3, &e);
+        double* ar = ensure<double>(c->dl_c, F + 1, &e);
+        CK(e);
+        CK(pgpu::launch_mesh_compact(c, nptr, nb, nrm, ar));
+        CK(cudaMemcpyAsync(hptr.data(), nptr, (n + 1) * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
+        if (neighbor && F) CK(cudaMemcpyAsync(neighbor, nb, F * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+        if (normal && F) CK(cudaMemcpyAsync(normal, nrm, 3 * F * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        if (area && F) CK(cudaMemcpyAsync(area, ar, F * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    }
     CK(cudaMemcpyAsync(hcnt.data(), c->fcnt.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, c->stream));
-    if (neighbor && F) CK(cudaMemcpyAsync(neighbor, nb, F * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
-    if (normal && F) CK(cudaMemcpyAsync(normal, nrm, 3 * F * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-    if (area && F) CK(cudaMemcpyAsync(area, ar, F * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (volumes && n) CK(cudaMemcpyAsync(volumes, c->vol.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (cert_k && n) CK(cudaMemcpyAsync(cert_k, c->certk.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
     if (status && n) CK(cudaMemcpyAsync(status, c->status.p, n * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));

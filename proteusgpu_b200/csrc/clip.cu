@@ -1,7 +1,7 @@
 // Voronoi cells by half-space clipping with the security-radius certificate,
 // fused with the extraction of faces, areas, volumes and centroids
 // (replaces cpu_compute_cell + ConvexCell + extract_cell_to_vmesh,
-// src/voronoi/voronoi.cpp:201-241, src/voronoi/cell.cpp:42-669; the method is
+// src/voronoi/voronoi.cpp:115-155, src/voronoi/cell.cpp:42-669; the method is
 // Ray, Sokolov, Lefebvre, Levy, "Meshless Voronoi on the GPU", ACM TOG 2018).
 //
 // One warp per cell.  The cell lives in shared memory in dual form: planes
@@ -198,7 +198,7 @@ struct ClipParams {
 };
 
 // Cell outputs of a cell that was not extracted (the reference leaves volume 0
-// and no faces, voronoi.cpp:236-238).
+// and no faces, voronoi.cpp:150-152).
 __device__ __forceinline__ void store_failed(const ClipParams& P, int lane, uint32_t e, int status) {
     if (lane == 0) {
         if (status == ST_SECURITY_RADIUS_NOT_REACHED && (int64_t)e < P.n_hydro) atomicAdd(P.uncertified, 1u);
@@ -768,12 +768,12 @@ __global__ void __launch_bounds__(CW * 32) k_clip(ClipParams P) {
         if (clip_by<D>(W, lane, z, bx, by, bz, sx, sy, sz, P.robust, nb_v, nb_t, status, v_dist, fail_vdist) ==
             CLIP_FAIL)
             break;
-        if (d2B > 4 * v_dist) {  // security radius reached (voronoi.cpp:224)
+        if (d2B > 4 * v_dist) {  // security radius reached (voronoi.cpp:138)
             certk = k + 1;
             break;
         }
     }
-    // final certificate with the K-th neighbour (voronoi.cpp:231-233)
+    // final certificate with the K-th neighbour (voronoi.cpp:145-147)
     {
         const double vdf = status == ST_SUCCESS ? v_dist : fail_vdist;
         const uint32_t zK = kl[K - 1];

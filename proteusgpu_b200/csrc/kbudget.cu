@@ -1,7 +1,7 @@
 // Learned neighbour budget: a per-cell K proposal beside the reference's fixed
 // _K_ (Config.sh; knn::solve, src/knn/knn.cpp:225-315, always returns K
 // neighbours and the clip walks them until the security radius closes,
-// src/voronoi/voronoi.cpp:215-233).
+// src/voronoi/voronoi.cpp:129-147).
 //
 // Each hydro cell gets 8 features from the previous mesh and the new grid:
 //   0 log2(1 + certified K of the previous step) / 8

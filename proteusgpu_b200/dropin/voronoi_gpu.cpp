@@ -63,7 +63,7 @@ VMesh* compute_mesh(POINT_TYPE* pts_data, int num_points) {
 
 // Cells of the knn problem's (grid-sorted) points; the mesh is in that sorted
 // order, with neighbour ids in it, as the reference's compute_cells leaves it
-// before unpermute_vmesh (voronoi.cpp:154-197).
+// before unpermute_vmesh (voronoi.cpp:68-111).
 void compute_cells(int N_seedpts, knn_problem* knn, std::vector<Status>& stat, VMesh* mesh) {
     pgpu_ctx* c = pgpu_dropin::context();
     int64_t nf = 0;
@@ -128,7 +128,7 @@ void free_vmesh(VMesh* m) {
 }
 
 // Reorders a mesh whose cells and neighbour ids are in sorted order into input
-// order (the contract of voronoi.cpp:298-419); faces stay contiguous per cell.
+// order (the contract of voronoi.cpp:212-333); faces stay contiguous per cell.
 void unpermute_vmesh(VMesh* m, const unsigned int* sorted_to_original) {
     const hsize_t n = m->n_seeds;
     if (n == 0 || !sorted_to_original) return;
@@ -179,7 +179,7 @@ void unpermute_vmesh(VMesh* m, const unsigned int* sorted_to_original) {
 }
 
 #ifdef USE_HDF5
-// VMesh -> MeshCellData for the HDF5 writer (the contract of voronoi.cpp:425-507):
+// VMesh -> MeshCellData for the HDF5 writer (the contract of voronoi.cpp:339-421):
 // hydro cells only, flat seed and normal arrays of DIMENSION components.
 void vmesh_to_meshdata(VMesh* m, MeshCellData& d) {
     const int n = (int)m->n_hydro;

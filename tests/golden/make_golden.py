@@ -2,7 +2,7 @@
 
 The reference has no golden vectors of its own (its CI only builds and runs a
 dry run), so the fixtures here are outputs of the reference's own hot-path code,
-compiled from its sources by oracle/Makefile (``make -C oracle ref``) and run
+compiled from its sources by oracle/Makefile (``make -C oracle ref REF=<reference tree>``) and run
 in-process through oracle/ref_driver.cpp on small seeded inputs.
 
 Run from the repository root in a checkout where the reference tree is

@@ -66,6 +66,29 @@ def test_static_dt_matches_context_dt(dim):
     assert abs(_static_dt(L, dim, gamma, 0.1, dev, nh, stream) - want / 3.0) <= 1e-14 * want
 
 
+def test_static_dt_allocates_nothing_at_its_largest_size():
+    """Repeated calls at the largest accepted n leave the device's free memory unchanged
+    (cudaMemGetInfo before and after), and every call returns the same step."""
+    torch = pytest.importorskip("torch")
+    n, gamma, cfl = MAX_CELLS, 5.0 / 3.0, 0.3
+    g = torch.Generator(device="cuda:0").manual_seed(5)
+    rho = torch.rand(n, dtype=torch.float64, device="cuda:0", generator=g) + 0.5
+    v = torch.randn(n * 3, dtype=torch.float64, device="cuda:0", generator=g) * 0.3
+    E = torch.rand(n, dtype=torch.float64, device="cuda:0", generator=g) + 1.0
+    vol = torch.rand(n, dtype=torch.float64, device="cuda:0", generator=g) * 1e-7 + 1e-8
+    torch.cuda.synchronize()
+    L = _lib.load()
+    stream = torch.cuda.current_stream().cuda_stream
+    first = _static_dt(L, 3, gamma, cfl, (rho, v, E, vol), n, stream)  # the first call does the set-up
+    torch.cuda.synchronize()
+    free0, _total = torch.cuda.mem_get_info(0)
+    vals = [_static_dt(L, 3, gamma, cfl, (rho, v, E, vol), n, stream) for _ in range(20)]
+    torch.cuda.synchronize()
+    free1, _total = torch.cuda.mem_get_info(0)
+    assert free1 == free0, f"device free memory changed by {free0 - free1} bytes"
+    assert all(x == first for x in vals) and first > 0.0
+
+
 def test_static_dt_rejects_sizes_beyond_its_scratch():
     L = _lib.load()
     dt = C.c_double(-1.0)
