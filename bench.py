@@ -45,6 +45,8 @@ CONFIGS = {
     "sedov3d_1m": dict(dim=3, n=1_048_576, seed=2, k=190, buff=0.04, boundary="periodic", cfl=0.3),
     "sedov3d_256k": dict(dim=3, n=262_144, seed=2, k=190, buff=0.04 * 4 ** (1 / 3), boundary="periodic", cfl=0.3),
     "sod2d_10k": dict(dim=2, n=10_000, seed=1, k=16, buff=0.04, boundary="reflective", cfl=0.3),
+    # 2D Kelvin-Helmholtz shear on a jittered 2048^2 periodic lattice (learned-K configuration)
+    "kh2d_4m": dict(dim=2, n=4_194_304, seed=3, k=48, buff=0.04, boundary="periodic", cfl=0.3, ic="kh"),
     # 256 independent 2D simulations (Sod with walls / Sedov / Kelvin-Helmholtz, gamma 1.4 or 5/3),
     # point counts log-uniform in [1e3, 2e5], advanced together
     "batched2d_256": dict(dim=2, n=None, seed=5, k=32, buff=None, boundary="mixed", cfl=0.3, batch=True,
@@ -78,6 +80,8 @@ def parse():
                     help="time only the headline form and the plain baseline (not fp32_clip, learned_fp64)")
     ap.add_argument("--headline-only", action="store_true",
                     help="time only the headline form (profiling runs; no speed-up against the plain form)")
+    ap.add_argument("--skip-extras", action="store_true",
+                    help="omit the other configurations' short measurements (default run only)")
     ap.add_argument("--skip-oracle", action="store_true",
                     help="omit the oracle checks (sampled cells at full size, density error of a full oracle run)")
     return ap.parse_args()
@@ -89,6 +93,8 @@ def make_ic(cfg):
         return ics.batch_2d(cfg["n_inst"], cfg["seed"])
     if cfg.get("ic") == "clustered":
         return ics.clustered_3d(n=cfg["n"], seed=cfg["seed"])
+    if cfg.get("ic") == "kh":
+        return ics.kh_2d(n_side=int(round(cfg["n"] ** 0.5)), seed=cfg["seed"])
     if cfg["dim"] == 3:
         return ics.sedov_3d(n=cfg["n"], seed=cfg["seed"])
     return ics.sod_2d(n_side=int(round(cfg["n"] ** 0.5)), seed=cfg["seed"])
@@ -157,7 +163,17 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- CPU reference
-def cpu_reference_step_rate(steps: int, cfg: dict, n_sample: int = 20000, nthreads: int | None = None):
+# The reference cannot run the 16.8M-point workload itself: knn::init sizes its neighbour
+# lists as len_pts * _K_ * sizeof(int) with int operands (src/knn/knn.cpp:110), which
+# overflows beyond 2^31 / 190 = 11.3M extended points (20.9M here), so the allocation fails
+# and the run faults.  Its CPU baseline is therefore a bounded sample of the same distribution.
+REFERENCE_FULL_SIZE_LIMIT = ("the reference cannot run this workload at full size: src/knn/knn.cpp:110 "
+                             "computes len_pts * _K_ in int (20.9M extended points x 190 > 2^31), the "
+                             "neighbour-list allocation fails and the process faults")
+CPU_SAMPLE_POINTS = 65536
+
+
+def cpu_reference_step_rate(steps: int, cfg: dict, n_sample: int = CPU_SAMPLE_POINTS, nthreads: int | None = None):
     """Cell-updates/s of the reference's own CPU code (oracle/_ref, compiled from its sources) on a
     bounded sample of the workload: per step and simulation compute_periodic_mesh (KNN + clipping +
     extraction) + dt_CFL + hydro_step.  3D: n_sample points of the same distribution, the ghost layer
@@ -178,13 +194,22 @@ def cpu_reference_step_rate(steps: int, cfg: dict, n_sample: int = 20000, nthrea
             items.append((ic, float(bf)))
             tot += ic.n
         desc = f"first {len(items)} instances of the batch ({tot} 2D points, periodic), K={K}"
+    elif dim == 2:
+        # the 2D workloads at n_sample points or fewer (the reference box is periodic only)
+        ns = min(cfg["n"], n_sample)
+        sub = dict(cfg, n=ns)
+        ic = make_ic(sub)
+        buff = min(cfg["buff"] * (cfg["n"] / ns) ** (1 / 2), 0.15)
+        items, tot = [(ic, buff)], ic.n
+        desc = (f"{ic.name}, {ic.n} points{' (the whole workload)' if ns == cfg['n'] else ''}, periodic, "
+                f"K={K}, buff {buff:.3f}")
     else:
         clustered = cfg.get("ic") == "clustered"
         ic = ics.clustered_3d(n=n_sample, seed=cfg["seed"]) if clustered else ics.sedov_3d(n=n_sample, seed=2)
         buff = min(cfg["buff"] * (cfg["n"] / n_sample) ** (1 / 3), 0.15)
         items, tot = [(ic, buff)], n_sample
-        desc = (f"3D Sedov, {n_sample} {'clustered' if clustered else 'uniform'} points, K={K}, "
-                f"buff {buff:.3f}")
+        desc = (f"3D Sedov, {n_sample} {'clustered' if clustered else 'uniform'} points (the workload's "
+                f"distribution: same clumps, fewer points), K={K}, buff {buff:.3f}")
     kind = "reference"
     try:
         import refbuild as rb
@@ -429,7 +454,7 @@ def run_ours(args, rank, world, local_rank):
     names = [HEADLINE] if args.headline_only else [PLAIN_FORM, HEADLINE] if args.skip_forms else list(FORMS)
     res = {}
     ref_state = None  # the plain form runs first; every other form is compared with it
-    want_check = not args.skip_oracle and rank == 0 and not cfg.get("batch") and cfg["dim"] == 3
+    want_check = not args.skip_oracle and world == 1 and not cfg.get("batch") and cfg["dim"] == 3
     for f in names:
         res[f] = time_form(args, cfg, ic, local_rank, dist, f, want_e2e=(f == HEADLINE and not args.skip_e2e),
                            want_clocks=(f == HEADLINE), want_state=PLAIN_FORM in names,
@@ -445,6 +470,9 @@ def run_ours(args, rank, world, local_rank):
         oracle_check = dict(res[HEADLINE].pop("checks"))
         oracle_check["form"] = HEADLINE
         oracle_check["density_run"] = density_check(cfg, HEADLINE, res[HEADLINE].get("weights"))
+    extras = None
+    if world == 1 and not args.skip_extras and args.config == "clustered3d_16m":
+        extras = run_extras(args, local_rank)
     _barrier(dist)
     if dist:
         dist.destroy_process_group()
@@ -526,29 +554,14 @@ def run_ours(args, rank, world, local_rank):
         v, kind, cores, sample, t_step = cpu_reference_step_rate(steps=2, cfg=cfg)
         cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample,
                "s_per_step": t_step}
-    dist_name = "clustered (70% in 64 Gaussian clumps)" if cfg.get("ic") == "clustered" else "uniform"
-    if cfg.get("batch"):
-        wl = (f"{args.config}: {cfg['n_inst']} independent 2D simulations (Sod with walls / Sedov / "
-              f"Kelvin-Helmholtz, gamma 1.4 or 5/3, seed {cfg['seed']}), {n} points in all, point counts "
-              "log-uniform in [1e3, 2e5], one launch per stage")
-    elif D == 3:
-        wl = (f"{args.config}: 3D Sedov-Taylor blast, {cfg['n']} {dist_name} points (seed {cfg['seed']}), "
-              f"moving mesh, {cfg['boundary']} box")
-    else:
-        wl = args.config
+    if cpu and cfg.get("n") and D == 3 and cfg["n"] > 9_000_000:
+        cpu["full_size"] = REFERENCE_FULL_SIZE_LIMIT
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms"] / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": wl, "n_points": n, "k": cfg["k"], "buff": cfg["buff"],
-                   "form": "learned-K (BF16 MLP proposal, plain-K fallback) + FP32 local-frame clipping "
-                           "(FP64 re-clip, FP64 extraction, hydro and sums)",
-                   "baseline_form": f"plain: fixed K={cfg['k']}, FP64 clipping",
-                   "flux": "physical (outward normal, pair-symmetric area)",
-                   "l2": "inputs larger than L2: per-step KNN lists alone are "
-                         f"{stats['n_hydro'] * cfg['k'] * 4 / 2 ** 20:.0f} MiB at the plain K",
-                   "parallelism": f"replicas x{world}"},
+        "config": workload_config(args, cfg, n, world),
         "speedup_vs_plain_gpu": value / rate(base) if base else None,
         # the headline's state after the timed steps against the plain FP64 GPU form's (same IC,
         # same steps): 0 cells differing and 0 L1 error = the same meshes and fluxes every step
@@ -561,12 +574,167 @@ def run_ours(args, rank, world, local_rank):
         "stages_ms": dict(zip(STAGES, stage)),
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"], "forms": forms,
         "clocks": head["clocks"],
+        # the other configurations, one short measurement each with its own oracle check
+        "configs": extras,
         "mesh": {"n_ext": stats["n_ext"], "faces": stats["num_faces"], "cert_k_max": stats["cert_k_max"],
                  "failed_cells": stats["failed_cells"], "knn_candidates_per_query":
                      stats["knn_candidates"] / max(stats["n_hydro"], 1)},
         "peaks": {"fp64_tflops": fp64.value, "fp32_tflops": fp32.value, "hbm_gbs": hbm},
     }
     return out
+
+
+def _form_rate(n, steps, ms):
+    return n * steps / (ms / 1e3)
+
+
+def run_extras(args, local_rank):
+    """The other configurations beside the headline workload, each measured briefly with
+    the same step (headline form and plain form, CUDA events, inputs resident) and checked
+    against the oracle:
+      sedov3d_1m     3D Sedov, 1,048,576 uniform points, K = 190: sampled cells of the first
+                     mesh and of a mesh after the timed steps
+      kh2d_4m        2D Kelvin-Helmholtz, 4,194,304 points: the learned budget trained on the
+                     first 50 steps (classes 12-48), then timed; sampled cells
+      sod2d_10k      2D Sod with walls, 10,000 points: the whole run to t = 0.2 on the GPU,
+                     the oracle's run of the same steps, and the reference's CPU run of it
+      batched2d_256  256 2D simulations in one launch per stage: instances against the
+                     oracle's solo runs of them
+    Each entry also carries the reference CPU rate of its sample (cpu_reference_step_rate)."""
+    import types
+    check = _oracle_check_module()
+    out = {}
+    for name in ("sedov3d_1m", "kh2d_4m", "sod2d_10k", "batched2d_256"):
+        t0 = time.perf_counter()
+        cfg = CONFIGS[name]
+        try:
+            ic = make_ic(cfg)
+            n = ic.n
+            e = {"workload": workload_config(args, cfg, n, 1, name)["workload"], "n_points": n, "k": cfg["k"]}
+            if name == "sod2d_10k":
+                e.update(_sod_full_run(cfg, ic, local_rank, check))
+            else:
+                ke = min(max(args.steps, 1), 10)
+                res = {}
+                for f in (PLAIN_FORM, HEADLINE):
+                    w = 51 if (name == "kh2d_4m" and FORMS[f]["kbudget"]) else 3
+                    a = types.SimpleNamespace(steps=ke, warmup=w)
+                    res[f] = time_form(a, cfg, ic, local_rank, None, f, want_state=True,
+                                       want_check=(cfg["dim"] == 3 or name == "kh2d_4m") and f == HEADLINE)
+                    res[f]["steps_run"] = w + 1 + ke
+                h, b = res[HEADLINE], res[PLAIN_FORM]
+                e.update({"value": _form_rate(n, ke, h["ms"]), "ms_per_step": h["ms"] / ke,
+                          "plain_value": _form_rate(n, ke, b["ms"]),
+                          "speedup_vs_plain_gpu": b["ms"] / h["ms"], "steps": ke,
+                          "warmup": {f: res[f]["steps_run"] - 1 - ke for f in res},
+                          "stages_ms": dict(zip(STAGES, h["stage"])), "launches": h["launches"],
+                          "vs_plain": compare_states(b["state"], h["state"])})
+                if h.get("kbudget"):
+                    kb = h["kbudget"]
+                    e["learned_k"] = {"mean_k": kb["mean_k"], "plain_k": cfg["k"], "misses": kb["misses"],
+                                      "miss_rate": kb["misses"] / max(kb["cells"], 1),
+                                      "train_steps": kb["steps_trained"]}
+                if "checks" in h:
+                    e["oracle"] = h["checks"]
+                if name == "batched2d_256":
+                    e["oracle"] = _batch_instances_vs_oracle(cfg, ic, h, check)
+            v, kind, cores, sample, t_step = cpu_reference_step_rate(
+                steps=1 if name != "sod2d_10k" else e.get("steps_to_t_end", 1), cfg=cfg)
+            e["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+        except Exception as exc:  # one configuration's failure is reported, not fatal
+            e = {"error": f"{type(exc).__name__}: {exc}"}
+        e["seconds"] = time.perf_counter() - t0
+        out[name] = e
+    return out
+
+
+def _sod_full_run(cfg, ic, local_rank, check):
+    """2D Sod to t = 0.2: both forms' whole runs timed (CUDA events; a dt read back per step
+    to stop at t_end), and the oracle's run of the same number of steps."""
+    import torch
+    from proteusgpu_b200 import Context
+    t_end = 0.2
+    runs = {}
+    for f in (PLAIN_FORM, HEADLINE):
+        spec = FORMS[f]
+        with Context(dim=2, k=cfg["k"], buff=cfg["buff"], boundary=cfg["boundary"], flux="physical",
+                     gamma=ic.gamma, device=local_rank, precision=spec["precision"], predicates="robust") as ctx:
+            if spec["kbudget"]:
+                ctx.kbudget_enable(train_steps=5, iters_per_step=64, quantile=0.98, seed=1)
+            ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+            stream = torch.cuda.ExternalStream(ctx.stream)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ev0.record(stream)
+            t, steps, dts = 0.0, 0, []
+            while t < t_end and steps < 10000:
+                dts.append(ctx.sim_step(cfg["cfl"]))
+                t += dts[-1]
+                steps += 1
+            ev1.record(stream)
+            torch.cuda.synchronize()
+            vol = ctx.download_volumes()[: ic.n]
+            x, m, p, e = ctx.sim_get()
+            runs[f] = {"ms": ev0.elapsed_time(ev1), "steps": steps, "state": (dts, x, m, p, e, vol)}
+    steps = runs[HEADLINE]["steps"]
+    ora = check.oracle_moving_run(ic, cfg["k"], cfg["buff"], cfg["boundary"], steps, cfl=cfg["cfl"], robust=True)
+    h, b = runs[HEADLINE], runs[PLAIN_FORM]
+    return {"value": _form_rate(ic.n, steps, h["ms"]), "ms_per_step": h["ms"] / steps,
+            "plain_value": _form_rate(ic.n, b["steps"], b["ms"]), "speedup_vs_plain_gpu":
+                (b["ms"] / b["steps"]) / (h["ms"] / steps), "steps_to_t_end": steps, "t_end": t_end,
+            "timed": "the whole run from the initial condition to t_end (one dt read back per step)",
+            "oracle": {HEADLINE: check.state_errors(h["state"], ora),
+                       PLAIN_FORM: check.state_errors(b["state"], ora)}}
+
+
+def _batch_instances_vs_oracle(cfg, B, h, check, n_check=3):
+    """The batch's headline-form state after its steps, instance by instance for the
+    n_check smallest instances, against the oracle's solo runs of them (each with its
+    own ghost layer, gamma and boundary; robust predicates as the batch uses)."""
+    x, m, p, e = h["state"]
+    counts = B.counts
+    off = np.concatenate([[0], np.cumsum(counts)])
+    steps = h["steps_run"]
+    out = {"steps": steps, "instances": []}
+    for i in np.argsort(counts)[:n_check]:
+        ic, bf = B.instances[i], float(B.buff[i])
+        dts, xo, mo, po, eo, vo = check.oracle_moving_run(ic, cfg["k"], bf, ic.boundary, steps, cfl=cfg["cfl"],
+                                                          robust=True)
+        sl = slice(off[i], off[i + 1])
+        l1 = lambda a, b: float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))  # noqa: E731
+        out["instances"].append({"instance": int(i), "n": int(counts[i]), "ic": ic.name, "boundary": ic.boundary,
+                                 "mass_l1_rel": l1(m[sl], mo), "energy_l1_rel": l1(e[sl], eo),
+                                 "position_max_abs": float(np.abs(x[sl] - xo).max()),
+                                 "momentum_l1_rel": l1(p[sl], po)})
+    return out
+
+
+def workload_config(args, cfg, n, world, name=None):
+    """The `config` object of both arms' lines: the workload, its sizes and the forms."""
+    name = name or args.config
+    dist_name = "clustered (70% in 64 Gaussian clumps)" if cfg.get("ic") == "clustered" else "uniform"
+    if cfg.get("batch"):
+        wl = (f"{name}: {cfg['n_inst']} independent 2D simulations (Sod with walls / Sedov / "
+              f"Kelvin-Helmholtz, gamma 1.4 or 5/3, seed {cfg['seed']}), {n} points in all, point counts "
+              "log-uniform in [1e3, 2e5], one launch per stage")
+    elif cfg["dim"] == 3:
+        wl = (f"{name}: 3D Sedov-Taylor blast, {cfg['n']} {dist_name} points (seed {cfg['seed']}), "
+              f"moving mesh, {cfg['boundary']} box")
+    elif cfg.get("ic") == "kh":
+        wl = (f"{name}: 2D Kelvin-Helmholtz shear, {n} points on a jittered {int(round(n ** 0.5))}^2 lattice "
+              f"(seed {cfg['seed']}), moving mesh, periodic box")
+    else:
+        wl = (f"{name}: 2D Sod shock tube, {n} points on a jittered lattice (seed {cfg['seed']}), moving mesh, "
+              f"{cfg['boundary']} walls")
+    return {"workload": wl, "n_points": n, "k": cfg["k"], "buff": cfg["buff"],
+            "form": "learned-K (BF16 MLP proposal, plain-K fallback) + FP32 local-frame clipping "
+                    "(FP64 re-clip, FP64 extraction, hydro and sums)",
+            "baseline_form": f"plain: fixed K={cfg['k']}, FP64 clipping",
+            "flux": "physical (outward normal, pair-symmetric area)",
+            "l2": (f"inputs larger than L2: per-step KNN lists alone are {n * cfg['k'] * 4 / 2 ** 20:.0f} MiB "
+                   "at the plain K" if n * cfg["k"] * 4 > 126 * 2 ** 20 else
+                   "a small configuration: its working set fits in L2 (no flush between steps)"),
+            "parallelism": f"replicas x{world}"}
 
 
 def run_reference(args, rank):
@@ -582,12 +750,14 @@ def run_reference(args, rank):
         v_all.append(v)
     v = float(np.mean(v_all))
     cfg = CONFIGS[args.config]
+    cpu = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+    if cfg.get("n") and cfg["dim"] == 3 and cfg["n"] > 9_000_000:
+        cpu["full_size"] = REFERENCE_FULL_SIZE_LIMIT
     return {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
             "warmup": warm, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": f"{args.config} (bounded sample on the host cores)", "n_points": cfg["n"],
-                       "k": cfg["k"]},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
+            "config": workload_config(args, cfg, make_ic(cfg).n if cfg.get("batch") else cfg["n"], args.gpus),
+            "cpu_baseline": cpu,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 

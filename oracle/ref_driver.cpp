@@ -201,6 +201,49 @@ REF_API void* ref_mesh_wrap(long n_seeds, long n_hydro, long num_faces, const do
 
 REF_API void ref_mesh_free(void* m) { voronoi::free_vmesh((VMesh*)m); }
 
+// Sets the VMesh seeds (n_seeds x 3 doubles) of a mesh made by ref_mesh_wrap.
+REF_API void ref_mesh_set_seeds(void* m, const double* seeds) {
+    VMesh* mesh = (VMesh*)m;
+    for (hsize_t i = 0; i < mesh->n_seeds; i++) {
+        mesh->seeds[i].x = seeds[3 * i];
+        mesh->seeds[i].y = seeds[3 * i + 1];
+        mesh->seeds[i].z = seeds[3 * i + 2];
+    }
+}
+
+// voronoi::vmesh_to_meshdata (voronoi.cpp:339-421 in the reference build; the
+// drop-in's own definition where this driver is linked with the drop-in units)
+// and every field of the MeshCellData it fills (io/output.h:14-48): header as
+// (dimension, extent, n, k, nmax, seed, store_edge_coords), the dims arrays as
+// (seeds rows, seeds cols, normal rows, normal cols), then the vectors.  The
+// caller sizes cell_ids / volumes / face_counts by n_hydro, seeds by
+// n_hydro x D, neighbor / area by num_faces and normal by num_faces x D.
+// Returns the number of faces in the MeshCellData.
+REF_API long ref_meshdata(void* m, double* header7, long* dims4, int* cell_ids, double* seeds, double* volumes,
+                          int* face_counts, int* neighbor, double* normal, double* area) {
+    MeshCellData d;
+    voronoi::vmesh_to_meshdata((VMesh*)m, d);
+    header7[0] = d.header.dimension;
+    header7[1] = d.header.extent;
+    header7[2] = d.header.n;
+    header7[3] = d.header.k;
+    header7[4] = d.header.nmax;
+    header7[5] = d.header.seed;
+    header7[6] = d.header.store_edge_coords ? 1.0 : 0.0;
+    dims4[0] = d.seeds_dims.size() > 0 ? (long)d.seeds_dims[0] : -1;
+    dims4[1] = d.seeds_dims.size() > 1 ? (long)d.seeds_dims[1] : -1;
+    dims4[2] = d.faces.normal_dims.size() > 0 ? (long)d.faces.normal_dims[0] : -1;
+    dims4[3] = d.faces.normal_dims.size() > 1 ? (long)d.faces.normal_dims[1] : -1;
+    for (size_t i = 0; i < d.cell_ids.size(); i++) cell_ids[i] = d.cell_ids[i];
+    for (size_t i = 0; i < d.seeds.size(); i++) seeds[i] = d.seeds[i];
+    for (size_t i = 0; i < d.volumes.size(); i++) volumes[i] = d.volumes[i];
+    for (size_t i = 0; i < d.face_counts.size(); i++) face_counts[i] = d.face_counts[i];
+    for (size_t f = 0; f < d.faces.neighbor_cell.size(); f++) neighbor[f] = d.faces.neighbor_cell[f];
+    for (size_t f = 0; f < d.faces.normal.size(); f++) normal[f] = d.faces.normal[f];
+    for (size_t f = 0; f < d.faces.area.size(); f++) area[f] = d.faces.area[f];
+    return (long)d.faces.area.size();
+}
+
 // knn::init + knn::solve (knn.cpp:16-234) on n points in [0,1]^D.  Writes the
 // K neighbour lists translated to input ids (query in input order, UINT_MAX
 // kept for unfilled slots).  Returns N_grid, or -1 when it is below 16.

@@ -71,6 +71,9 @@ def _bind(lib):
     lib.ref_dt_cfl.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp]
     lib.ref_dt_cfl.restype = C.c_double
     lib.ref_hydro_step.argtypes = [C.c_void_p, C.c_double, _dp, _dp, _dp]
+    lib.ref_mesh_set_seeds.argtypes = [C.c_void_p, _dp]
+    lib.ref_meshdata.argtypes = [C.c_void_p, _dp, _lp, _ip, _dp, _dp, _ip, _ip, _dp, _dp]
+    lib.ref_meshdata.restype = C.c_long
     return lib
 
 
@@ -201,3 +204,30 @@ def hydro_step(dim: int, k: int, handle, dt: float, rho, vel, energy, gamma: flo
     vflat = v.reshape(-1)
     lib.ref_hydro_step(handle, dt, r, vflat, e)
     return r, vflat.reshape(v.shape), e
+
+
+def set_seeds(dim: int, k: int, handle, seeds) -> None:
+    """Sets the seeds (n_seeds x 3) of a VMesh made by wrap_mesh."""
+    load(dim, k).ref_mesh_set_seeds(handle, np.ascontiguousarray(seeds, np.float64).reshape(-1))
+
+
+def meshdata(dim: int, k: int, handle) -> dict:
+    """voronoi::vmesh_to_meshdata of a live VMesh and every field of its MeshCellData."""
+    lib = load(dim, k)
+    ns, nh, nf = C.c_long(), C.c_long(), C.c_long()
+    lib.ref_mesh_sizes(handle, C.byref(ns), C.byref(nh), C.byref(nf))
+    n, F = nh.value, nf.value
+    hdr, dims = np.zeros(7), np.zeros(4, np.int64)
+    out = dict(cell_ids=np.zeros(max(n, 1), np.int32), seeds=np.zeros(max(n * dim, 1)),
+               volumes=np.zeros(max(n, 1)), face_counts=np.zeros(max(n, 1), np.int32),
+               neighbor_cell=np.zeros(max(F, 1), np.int32), normal=np.zeros(max(F * dim, 1)),
+               area=np.zeros(max(F, 1)))
+    nfd = lib.ref_meshdata(handle, hdr, dims, out["cell_ids"], out["seeds"], out["volumes"], out["face_counts"],
+                           out["neighbor_cell"], out["normal"], out["area"])
+    for key, size in (("cell_ids", n), ("seeds", n * dim), ("volumes", n), ("face_counts", n),
+                      ("neighbor_cell", nfd), ("normal", nfd * dim), ("area", nfd)):
+        out[key] = out[key][:size]
+    out["header"] = dict(zip(("dimension", "extent", "n", "k", "nmax", "seed", "store_edge_coords"), hdr.tolist()))
+    out["seeds_dims"] = dims[:2].tolist()
+    out["normal_dims"] = dims[2:].tolist()
+    return out
