@@ -87,6 +87,32 @@ def parse():
     return ap.parse_args()
 
 
+class Workload:
+    """A workload's initial condition as the device generates it: its generator spec
+    (pgpu_ic_spec) and sizes, without host arrays."""
+
+    def __init__(self, spec, n, dim, gamma):
+        self.spec, self.n, self.dim, self.gamma = spec, n, dim, gamma
+
+
+def make_workload(cfg):
+    """The initial condition of a configuration for the GPU arm: a Workload (generated on
+    the device), or the host-generated Batch of a batched configuration."""
+    from proteusgpu_b200 import ics
+    if cfg.get("batch"):
+        return make_ic(cfg)
+    if cfg.get("ic") == "clustered":
+        spec = ics.clustered_3d_spec(n=cfg["n"], seed=cfg["seed"])
+    elif cfg.get("ic") == "kh":
+        spec = ics.kh_2d_spec(n_side=int(round(cfg["n"] ** 0.5)), seed=cfg["seed"])
+    elif cfg["dim"] == 3:
+        spec = ics.sedov_spec(3, cfg["n"], cfg["seed"])
+    else:
+        spec = ics.sod_2d_spec(n_side=int(round(cfg["n"] ** 0.5)), seed=cfg["seed"])
+    n = spec["n_side"] ** spec["dim"] if "n_side" in spec else spec["n"]
+    return Workload(spec, n, spec["dim"], spec["gamma"])
+
+
 def make_ic(cfg):
     from proteusgpu_b200 import ics
     if cfg.get("batch"):
@@ -320,16 +346,18 @@ def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks
     if spec["kbudget"]:
         # the warm-up steps but the last train the proposal; the last one already uses it
         ctx.kbudget_enable(train_steps=max(1, args.warmup - 1), iters_per_step=256, quantile=0.98, seed=1)
+    # the initial condition is generated on the device (pgpu_sim_init_ic / pgpu_batch_init_ic):
+    # the same arrays, bit for bit, as proteusgpu_b200/ics.py builds on the host
     if batch:
-        ctx.batch_init(ic.counts, ic.buff, ic.gamma, ic.boundary, ic.concat("pos"), ic.concat("rho"),
-                       ic.concat("vel"), ic.concat("energy"), ic.concat("deposit"))
+        ctx.batch_init_ic([b.spec for b in ic.instances], ic.buff, ic.boundary)
     else:
-        ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+        ctx.sim_init_ic(ic.spec)
     checks = {}
     if want_check:
         t0 = time.perf_counter()
+        pos0 = ctx.sim_get()[0]  # the initial positions, which the first mesh was built from
         checks["first_mesh"] = _oracle_check_module().sampled_cells(
-            ctx, n_random=20000, n_walked=2000, pos_before=ic.pos, buff=cfg["buff"], boundary=cfg["boundary"],
+            ctx, n_random=20000, n_walked=2000, pos_before=pos0, buff=cfg["buff"], boundary=cfg["boundary"],
             seed=11)
         checks["first_mesh"]["seconds"] = time.perf_counter() - t0
     for _ in range(max(args.warmup, 0)):
@@ -449,7 +477,7 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local_rank))
-    ic = make_ic(cfg)
+    ic = make_workload(cfg)
     n = ic.n
     names = [HEADLINE] if args.headline_only else [PLAIN_FORM, HEADLINE] if args.skip_forms else list(FORMS)
     res = {}
@@ -608,7 +636,7 @@ def run_extras(args, local_rank):
         t0 = time.perf_counter()
         cfg = CONFIGS[name]
         try:
-            ic = make_ic(cfg)
+            ic = make_ic(cfg) if name in ("sod2d_10k", "batched2d_256") else make_workload(cfg)
             n = ic.n
             e = {"workload": workload_config(args, cfg, n, 1, name)["workload"], "n_points": n, "k": cfg["k"]}
             if name == "sod2d_10k":
@@ -617,7 +645,9 @@ def run_extras(args, local_rank):
                 ke = min(max(args.steps, 1), 10)
                 res = {}
                 for f in (PLAIN_FORM, HEADLINE):
-                    w = 51 if (name == "kh2d_4m" and FORMS[f]["kbudget"]) else 3
+                    # the learned form trains on the first 50 steps of the Kelvin-Helmholtz run; the
+                    # plain form runs the same steps, so that both time (and compare) the same states
+                    w = 51 if name == "kh2d_4m" else 3
                     a = types.SimpleNamespace(steps=ke, warmup=w)
                     res[f] = time_form(a, cfg, ic, local_rank, None, f, want_state=True,
                                        want_check=(cfg["dim"] == 3 or name == "kh2d_4m") and f == HEADLINE)

@@ -205,6 +205,49 @@ int pgpu_hydro_step(pgpu_ctx *ctx, double dt);
 int pgpu_dt_cfl_static(int dim, double gamma, double cfl, const double *rho, const double *v, const double *E,
                        const double *volumes, int64_t n, void *stream, double *dt);
 
+/* -------------------------------------------------- initial conditions ---
+ * Extension (the reference reads its initial conditions from HDF5 files written
+ * by its create*.py scripts, src/io/input.cpp:121-309).  The benchmark
+ * workloads' initial conditions generated on the device from a seed, bit for
+ * bit the ones proteusgpu_b200/ics.py builds on the host (a counter-based
+ * generator and fixed operation sequences for ln, exp, sin, cos and the
+ * normals, so both sides compute the same doubles):
+ *   PGPU_IC_SOD        2D Sod tube on a jittered n_side^2 lattice (rho 1 / 0.125,
+ *                      P 1 / 0.1), split along the line through the centre with
+ *                      normal (split_cos, split_sin);
+ *   PGPU_IC_SEDOV      uniform points (dim 2 or 3), rho 1, P p0, and a blast of
+ *                      e_blast over the 32 points nearest the centre;
+ *   PGPU_IC_KH         2D Kelvin-Helmholtz shear on a jittered n_side^2 lattice
+ *                      (density ratio rho_ratio, vx +-0.5, P 2.5, seeded vy);
+ *   PGPU_IC_CLUSTERED  3D: a fraction frac_clumped of n points in n_clumps
+ *                      Gaussian clumps (widths log-uniform in [0.005, 0.05]),
+ *                      the rest uniform, and the blast as PGPU_IC_SEDOV. */
+#define PGPU_IC_SOD 0
+#define PGPU_IC_SEDOV 1
+#define PGPU_IC_KH 2
+#define PGPU_IC_CLUSTERED 3
+typedef struct {
+    int32_t kind;       /* PGPU_IC_* */
+    int32_t dim;        /* 2, or 3 for PGPU_IC_SEDOV / PGPU_IC_CLUSTERED */
+    int64_t n;          /* points (PGPU_IC_SEDOV, PGPU_IC_CLUSTERED) */
+    int32_t n_side;     /* lattice side (PGPU_IC_SOD, PGPU_IC_KH): n_side^2 points */
+    int32_t n_clumps;   /* PGPU_IC_CLUSTERED */
+    uint64_t seed;
+    double gamma, jitter, split_cos, split_sin, p0, e_blast, rho_ratio, frac_clumped;
+} pgpu_ic_spec;
+
+/* The initial condition of spec in host arrays (pos n x dim, rho, v n x dim, E,
+ * deposit: energy per cell of the blast, zero elsewhere); any may be NULL. */
+int pgpu_ic_generate(pgpu_ctx *ctx, const pgpu_ic_spec *spec, double *pos, double *rho, double *v, double *E,
+                     double *deposit);
+/* pgpu_sim_init from the initial condition of spec generated on the device: no
+ * host arrays; the spec's dim must be the context's. */
+int pgpu_sim_init_ic(pgpu_ctx *ctx, const pgpu_ic_spec *spec);
+/* pgpu_batch_init from n_inst specs (gamma from each spec), each generated on the
+ * device; buff and boundary per instance as pgpu_batch_init takes them. */
+int pgpu_batch_init_ic(pgpu_ctx *ctx, int n_inst, const pgpu_ic_spec *specs, const double *buff,
+                       const int *boundary);
+
 /* -------------------------------------------------- moving-mesh stepping ---
  * Extension (the reference's time loop, src/main.cpp:50-63, keeps its mesh
  * fixed).  The simulation state is conserved mass, momentum and energy per

@@ -28,7 +28,37 @@ EXPORTED = [
     "pgpu_kbudget_enable", "pgpu_kbudget_classes", "pgpu_kbudget_stats", "pgpu_kbudget_weights",
     "pgpu_mlp_forward", "pgpu_mlp_grad", "pgpu_fp32_peak", "pgpu_batch_init", "pgpu_batch_dt", "pgpu_autotune",
     "pgpu_set_tuning", "pgpu_download_points", "pgpu_walked_slots", "pgpu_sample_cells",
+    "pgpu_ic_generate", "pgpu_sim_init_ic", "pgpu_batch_init_ic",
 ]
+
+IC_KINDS = {"sod": 0, "sedov": 1, "kh": 2, "clustered": 3}
+
+
+class ICSpec(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("dim", C.c_int32), ("n", C.c_int64), ("n_side", C.c_int32),
+                ("n_clumps", C.c_int32), ("seed", C.c_uint64), ("gamma", C.c_double), ("jitter", C.c_double),
+                ("split_cos", C.c_double), ("split_sin", C.c_double), ("p0", C.c_double), ("e_blast", C.c_double),
+                ("rho_ratio", C.c_double), ("frac_clumped", C.c_double)]
+
+
+def ic_spec(spec: dict) -> ICSpec:
+    """The pgpu_ic_spec of a generator's spec dict (ics.IC.spec)."""
+    s = ICSpec()
+    s.kind = IC_KINDS[spec["kind"]]
+    s.dim = spec["dim"]
+    s.n = spec.get("n", 0)
+    s.n_side = spec.get("n_side", 0)
+    s.n_clumps = spec.get("n_clumps", 0)
+    s.seed = spec["seed"]
+    s.gamma = spec["gamma"]
+    s.jitter = spec.get("jitter", 0.1)
+    s.split_cos = spec.get("split_cos", 1.0)
+    s.split_sin = spec.get("split_sin", 0.0)
+    s.p0 = spec.get("p0", 1e-5)
+    s.e_blast = spec.get("e_blast", 1.0)
+    s.rho_ratio = spec.get("rho_ratio", 2.0)
+    s.frac_clumped = spec.get("frac_clumped", 0.7)
+    return s
 
 
 class Params(C.Structure):
@@ -120,6 +150,9 @@ def load(path: str = LIB_PATH):
     L.pgpu_kbudget_weights.argtypes = [vp, vp, vp]
     L.pgpu_mlp_forward.argtypes = [vp, vp, i64, vp, vp]
     L.pgpu_mlp_grad.argtypes = [vp, vp, vp, i64, vp, vp]
+    L.pgpu_ic_generate.argtypes = [vp, C.POINTER(ICSpec), vp, vp, vp, vp, vp]
+    L.pgpu_sim_init_ic.argtypes = [vp, C.POINTER(ICSpec)]
+    L.pgpu_batch_init_ic.argtypes = [vp, C.c_int, vp, vp, vp]
     L.pgpu_download_points.argtypes = [vp, vp]
     L.pgpu_walked_slots.argtypes = [vp, vp, i64, vp]
     L.pgpu_sample_cells.argtypes = [vp, vp, i64] + [vp] * 11 + [i64]

@@ -258,6 +258,32 @@ class Context:
         check(self._h, self._L.pgpu_sim_init(self._h, _ptr(pos), _ptr(rho), _ptr(v), _ptr(E), _ptr(dep), len(pos)),
               "pgpu_sim_init")
 
+    def ic_generate(self, spec: dict):
+        """The initial condition of a generator spec (ics.IC.spec) made on the device and
+        copied back: (pos, rho, vel, energy, deposit)."""
+        s = _lib.ic_spec(spec)
+        n = s.n_side ** s.dim if spec["kind"] in ("sod", "kh") else s.n
+        pos, rho, v, E, dep = np.zeros((n, s.dim)), np.zeros(n), np.zeros((n, s.dim)), np.zeros(n), np.zeros(n)
+        check(self._h, self._L.pgpu_ic_generate(self._h, C.byref(s), _ptr(pos), _ptr(rho), _ptr(v), _ptr(E),
+                                                _ptr(dep)), "pgpu_ic_generate")
+        return pos, rho, v, E, dep
+
+    def sim_init_ic(self, spec: dict) -> None:
+        """pgpu_sim_init from the initial condition of spec generated on the device."""
+        s = _lib.ic_spec(spec)
+        check(self._h, self._L.pgpu_sim_init_ic(self._h, C.byref(s)), "pgpu_sim_init_ic")
+
+    def batch_init_ic(self, specs, buff, boundary) -> None:
+        """pgpu_batch_init from per-instance generator specs, each generated on the device."""
+        nb = len(specs)
+        arr = (_lib.ICSpec * nb)(*[_lib.ic_spec(sp) for sp in specs])
+        bf = np.ascontiguousarray(np.broadcast_to(np.asarray(buff, np.float64), (nb,)))
+        bd = np.ascontiguousarray([_lib.BOUNDARY[b] if isinstance(b, str) else int(b) for b in
+                                   np.broadcast_to(np.asarray(boundary, object), (nb,))], np.int32)
+        check(self._h, self._L.pgpu_batch_init_ic(self._h, nb, C.cast(arr, C.c_void_p), _ptr(bf), _ptr(bd)),
+              "pgpu_batch_init_ic")
+        self._n_inst = nb
+
     def batch_init(self, counts, buff, gamma, boundary, pos, rho, v, E, deposit=None) -> None:
         """Independent simulations advanced together (extension): instance b owns the
         next counts[b] rows of pos/rho/v/E; buff, gamma, boundary ("periodic" or

@@ -86,7 +86,7 @@ int upload_points(pgpu_ctx* c, const double* pts, int64_t n) {
     cudaError_t e = cudaSuccess;
     double* d = ensure<double>(c->pos, (size_t)n * D + 1, &e);
     CK(e);
-    if (n > 0) CK(cudaMemcpyAsync(d, pts, (size_t)n * D * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (n > 0) CK(cudaMemcpyAsync(d, pts, (size_t)n * D * sizeof(double), cudaMemcpyDefault, c->stream));
     return PGPU_OK;
 }
 
@@ -588,9 +588,10 @@ int pgpu_set_prim(pgpu_ctx* c, const double* rho, const double* v, const double*
     ensure<double>(c->energy, n + 1, &e);
     CK(e);
     if (n) {
-        CK(cudaMemcpyAsync(c->rho.p, rho, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->vel.p, v, n * D * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-        CK(cudaMemcpyAsync(c->energy.p, E, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        // host or device sources (the device-generated initial conditions come from device memory)
+        CK(cudaMemcpyAsync(c->rho.p, rho, n * sizeof(double), cudaMemcpyDefault, c->stream));
+        CK(cudaMemcpyAsync(c->vel.p, v, n * D * sizeof(double), cudaMemcpyDefault, c->stream));
+        CK(cudaMemcpyAsync(c->energy.p, E, n * sizeof(double), cudaMemcpyDefault, c->stream));
     }
     CK(cudaStreamSynchronize(c->stream));
     c->have_prim = true;
@@ -697,13 +698,147 @@ static int sim_init_common(pgpu_ctx* c, const double* pos, const double* rho, co
     if (deposit) {
         double* d = ensure<double>(c->dl_c, n + 1, &e);
         CK(e);
-        CK(cudaMemcpyAsync(d, deposit, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+        CK(cudaMemcpyAsync(d, deposit, n * sizeof(double), cudaMemcpyDefault, c->stream));
         dep = d;
     }
     CK(pgpu::launch_cons_from_prim(c, dep));
     CK(cudaStreamSynchronize(c->stream));
     c->have_sim = true;
     return PGPU_OK;
+}
+
+// ------------------------------------------------ device initial conditions
+static int ic_points(pgpu_ctx* c, const pgpu_ic_spec* s, int64_t* n_out) {
+    if (!s) return fail(c, PGPU_EINVAL, "initial condition: NULL spec");
+    int64_t n = 0;
+    const bool lattice = s->kind == PGPU_IC_SOD || s->kind == PGPU_IC_KH;
+    if (s->kind < PGPU_IC_SOD || s->kind > PGPU_IC_CLUSTERED || (s->dim != 2 && s->dim != 3) ||
+        (lattice && s->dim != 2) || (s->kind == PGPU_IC_CLUSTERED && (s->dim != 3 || s->n_clumps < 1 ||
+                                                                       s->n_clumps > 4096 ||
+                                                                       !(s->frac_clumped >= 0.0 &&
+                                                                         s->frac_clumped <= 1.0))) ||
+        !(s->gamma > 1.0))
+        return fail(c, PGPU_EINVAL, "initial condition: bad spec");
+    if (lattice) {
+        if (s->n_side < 1 || s->n_side > 65536) return fail(c, PGPU_EINVAL, "initial condition: bad n_side");
+        n = (int64_t)s->n_side * s->n_side;
+    } else {
+        n = s->n;
+    }
+    if (n < 1 || n >= (1ll << 27)) return fail(c, PGPU_ECAPACITY, "initial condition: point count outside [1, 2^27)");
+    *n_out = n;
+    return PGPU_OK;
+}
+
+// Device buffers of one generated initial condition (freed by the caller).
+struct IcBufs {
+    DevBuf pos, rho, vel, en, dep;
+    void release() {
+        free_buf(pos);
+        free_buf(rho);
+        free_buf(vel);
+        free_buf(en);
+        free_buf(dep);
+    }
+};
+
+static cudaError_t ic_alloc(IcBufs& b, int64_t n, int D) {
+    cudaError_t e = cudaSuccess;
+    if ((e = pgpu::ensure_bytes(b.pos, (size_t)n * D * sizeof(double) + 16))) return e;
+    if ((e = pgpu::ensure_bytes(b.rho, (size_t)n * sizeof(double) + 16))) return e;
+    if ((e = pgpu::ensure_bytes(b.vel, (size_t)n * D * sizeof(double) + 16))) return e;
+    if ((e = pgpu::ensure_bytes(b.en, (size_t)n * sizeof(double) + 16))) return e;
+    return pgpu::ensure_bytes(b.dep, (size_t)n * sizeof(double) + 16);
+}
+
+int pgpu_ic_generate(pgpu_ctx* c, const pgpu_ic_spec* s, double* pos, double* rho, double* v, double* E,
+                     double* deposit) {
+    int r = check_ctx(c);
+    if (r) return r;
+    int64_t n = 0;
+    if ((r = ic_points(c, s, &n))) return r;
+    const int D = s->dim;
+    IcBufs b;
+    cudaError_t e = ic_alloc(b, n, D);
+    const bool blast = s->kind == PGPU_IC_SEDOV || s->kind == PGPU_IC_CLUSTERED;
+    if (!e)
+        e = pgpu::ic_generate(c, s, n, (double*)b.pos.p, (double*)b.rho.p, (double*)b.vel.p, (double*)b.en.p,
+                              blast ? (double*)b.dep.p : nullptr);
+    if (!e && !blast) e = cudaMemsetAsync(b.dep.p, 0, (size_t)n * sizeof(double), c->stream);
+    const size_t nb = (size_t)n * sizeof(double);
+    if (!e && pos) e = cudaMemcpyAsync(pos, b.pos.p, nb * D, cudaMemcpyDeviceToHost, c->stream);
+    if (!e && rho) e = cudaMemcpyAsync(rho, b.rho.p, nb, cudaMemcpyDeviceToHost, c->stream);
+    if (!e && v) e = cudaMemcpyAsync(v, b.vel.p, nb * D, cudaMemcpyDeviceToHost, c->stream);
+    if (!e && E) e = cudaMemcpyAsync(E, b.en.p, nb, cudaMemcpyDeviceToHost, c->stream);
+    if (!e && deposit) e = cudaMemcpyAsync(deposit, b.dep.p, nb, cudaMemcpyDeviceToHost, c->stream);
+    if (!e) e = cudaStreamSynchronize(c->stream);
+    b.release();
+    CK(e);
+    return PGPU_OK;
+}
+
+int pgpu_sim_init_ic(pgpu_ctx* c, const pgpu_ic_spec* s) {
+    int r = check_ctx(c);
+    if (r) return r;
+    int64_t n = 0;
+    if ((r = ic_points(c, s, &n))) return r;
+    if (s->dim != c->prm.dim) return fail(c, PGPU_EINVAL, "pgpu_sim_init_ic: spec dim differs from the context's");
+    IcBufs b;
+    cudaError_t e = ic_alloc(b, n, s->dim);
+    const bool blast = s->kind == PGPU_IC_SEDOV || s->kind == PGPU_IC_CLUSTERED;
+    if (!e)
+        e = pgpu::ic_generate(c, s, n, (double*)b.pos.p, (double*)b.rho.p, (double*)b.vel.p, (double*)b.en.p,
+                              blast ? (double*)b.dep.p : nullptr);
+    if (!e) e = pgpu::set_single_instance(c, n);
+    if (e) {
+        b.release();
+        CK(e);
+    }
+    r = sim_init_common(c, (const double*)b.pos.p, (const double*)b.rho.p, (const double*)b.vel.p,
+                        (const double*)b.en.p, blast ? (const double*)b.dep.p : nullptr, n);
+    cudaStreamSynchronize(c->stream);
+    b.release();
+    return r;
+}
+
+int pgpu_batch_init_ic(pgpu_ctx* c, int n_inst, const pgpu_ic_spec* specs, const double* buff, const int* boundary) {
+    int r = check_ctx(c);
+    if (r) return r;
+    if (n_inst < 1 || n_inst > 65535 || !specs || !buff || !boundary)
+        return fail(c, PGPU_EINVAL, "pgpu_batch_init_ic: bad arguments");
+    std::vector<int64_t> counts(n_inst);
+    std::vector<double> gam(n_inst);
+    int64_t n = 0;
+    for (int b = 0; b < n_inst; b++) {
+        if ((r = ic_points(c, &specs[b], &counts[b]))) return r;
+        if (specs[b].dim != c->prm.dim) return fail(c, PGPU_EINVAL, "pgpu_batch_init_ic: spec dim differs");
+        gam[b] = specs[b].gamma;
+        n += counts[b];
+    }
+    if (n >= (1ll << 27)) return fail(c, PGPU_ECAPACITY, "pgpu_batch_init_ic: too many points");
+    const int D = c->prm.dim;
+    IcBufs all;
+    cudaError_t e = ic_alloc(all, n, D);
+    int64_t off = 0;
+    for (int b = 0; b < n_inst && !e; b++) {
+        const bool blast = specs[b].kind == PGPU_IC_SEDOV || specs[b].kind == PGPU_IC_CLUSTERED;
+        double* dep = (double*)all.dep.p + off;
+        if (!blast) e = cudaMemsetAsync(dep, 0, counts[b] * sizeof(double), c->stream);
+        if (!e)
+            e = pgpu::ic_generate(c, &specs[b], counts[b], (double*)all.pos.p + off * D, (double*)all.rho.p + off,
+                                  (double*)all.vel.p + off * D, (double*)all.en.p + off, blast ? dep : nullptr);
+        off += counts[b];
+    }
+    if (e) {
+        all.release();
+        CK(e);
+    }
+    r = pgpu_batch_init(c, n_inst, counts.data(), buff, gam.data(), boundary, (const double*)all.pos.p,
+                        (const double*)all.rho.p, (const double*)all.vel.p, (const double*)all.en.p,
+                        (const double*)all.dep.p);
+    cudaStreamSynchronize(c->stream);
+    all.release();
+    return r;
 }
 
 int pgpu_sim_step(pgpu_ctx* c, double cfl, double fixed_dt, double* dt_out) {

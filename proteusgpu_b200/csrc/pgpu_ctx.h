@@ -226,6 +226,9 @@ cudaError_t launch_mesh_compact(pgpu_ctx* c, uint32_t* new_ptr, int32_t* nb_out,
 cudaError_t launch_seeds(pgpu_ctx* c, double* out, bool no_scale);
 cudaError_t launch_knn_rows(pgpu_ctx* c, uint32_t* out);
 cudaError_t launch_unpack_points(pgpu_ctx* c, const void* pts, int64_t n, double* out);
+// ics.cu: a generated initial condition into device arrays (dep may be NULL)
+cudaError_t ic_generate(pgpu_ctx* c, const pgpu_ic_spec* s, int64_t n, double* pos, double* rho, double* vel,
+                        double* en, double* dep);
 // sampled query slots: ext ids, main-clip neighbour rows (width knn_stride or k), per-cell outputs
 cudaError_t launch_sample_cells(pgpu_ctx* c, const uint32_t* slots, int64_t n, uint32_t* ext_out, uint16_t* len_out,
                                 uint32_t* rows_out, int32_t* st_out, int32_t* ck_out, double* vol_out,
