@@ -45,6 +45,15 @@ extern "C" {
 /* flux conventions */
 #define PGPU_FLUX_REFERENCE 0 /* stored (inward) normal, each cell's own face area: riemann.cpp:7-45 as is */
 #define PGPU_FLUX_PHYSICAL 1  /* outward normal, face-pair-symmetric area: conservative to round-off */
+/* Moving-mesh steps only (extension), periodic boxes: the faces move with the
+ * generators (velocity (v_i + v_j)/2) and the Riemann problem is solved in the
+ * face's frame; outward normal, pair-symmetric area, exactly conservative.
+ * ALE1: first order; ALE2: second order (MUSCL-Hancock: least-squares
+ * gradients, slope limiter, half-step prediction, face states at the
+ * generators' midpoint).  pgpu_hydro_step (the reference's static step)
+ * treats them as PGPU_FLUX_PHYSICAL. */
+#define PGPU_FLUX_ALE1 2
+#define PGPU_FLUX_ALE2 3
 
 /* plane-vertex predicate near zero (|det| below the reference's error bound, cell.cpp:187-218) */
 #define PGPU_PRED_REFERENCE 0 /* as the reference: the cell fails with NEEDS_EXACT_PREDICATES */

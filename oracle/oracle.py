@@ -34,7 +34,8 @@ class _Mesh(C.Structure):
                 ("neighbor", C.POINTER(C.c_int)), ("normal", C.POINTER(C.c_double)),
                 ("area", C.POINTER(C.c_double)), ("ghost_ids", C.POINTER(C.c_long)),
                 ("ghost_code", C.POINTER(C.c_int)), ("status", C.POINTER(C.c_int)),
-                ("cert_k", C.POINTER(C.c_int)), ("centroid", C.POINTER(C.c_double))]
+                ("cert_k", C.POINTER(C.c_int)), ("centroid", C.POINTER(C.c_double)),
+                ("ext", C.POINTER(C.c_double)), ("unit_scale", C.c_double)]
 
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -75,6 +76,9 @@ def lib():
         L.om_set_fallback_k.argtypes = [C.c_int]
         L.om_set_boundary_mode.argtypes = [C.c_int]
         L.om_set_expand_k.argtypes = [C.c_int]
+        L.om_step_ale.argtypes = [C.POINTER(_Mesh), C.c_int, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp,
+                                  _dp, C.POINTER(C.c_long)]
+        L.om_step_ale.restype = C.c_double
         L.om_grid_new.argtypes = [C.c_int, _dp, C.c_long]
         L.om_grid_new.restype = C.c_void_p
         L.om_grid_free.argtypes = [C.c_void_p]
@@ -288,4 +292,19 @@ def step_moving(mesh: Mesh, cfl: float, gamma: float, boundary: int, x, mass, mo
     unp = C.c_long(0)
     dt = lib().om_step_moving(C.byref(mesh._c), cfl, fixed_dt, gamma, boundary, x.reshape(-1), m,
                               p.reshape(-1), e, C.byref(unp))
+    return dt, x, m, p, e, unp.value
+
+
+def step_ale(mesh: Mesh, order: int, cfl: float, gamma: float, x, mass, mom, energy, fixed_dt: float = 0.0):
+    """One moving-face step (order 1, or 2: MUSCL-Hancock) on copies, periodic boxes;
+    returns (dt, x, mass, mom, energy, n_unpaired).  The mesh must come from build_mesh."""
+    x = np.array(x, np.float64, copy=True)
+    m = np.array(mass, np.float64, copy=True)
+    p = np.array(mom, np.float64, copy=True)
+    e = np.array(energy, np.float64, copy=True)
+    unp = C.c_long(0)
+    dt = lib().om_step_ale(C.byref(mesh._c), order, cfl, fixed_dt, gamma, x.reshape(-1), m, p.reshape(-1), e,
+                           C.byref(unp))
+    if dt < 0:
+        raise ValueError("om_step_ale needs a mesh from build_mesh of a periodic box and order 1 or 2")
     return dt, x, m, p, e, unp.value

@@ -65,6 +65,9 @@ typedef struct {
     int *status;        /* n_seeds */
     int *cert_k;        /* n_seeds; 1-based neighbour index where the certificate closed, 0 if never */
     double *centroid;   /* n_seeds * 3, physical coordinates */
+    double *ext;        /* n_seeds * dim: the unit-box points the mesh was built on (om_build_mesh
+                           only; NULL otherwise) */
+    double unit_scale;  /* 1 + 2 buff: unit box -> physical (om_build_mesh only) */
 } om_mesh;
 
 /* ---- ghosts -------------------------------------------------------------- */
@@ -178,6 +181,35 @@ long om_hydro_step_ref(const om_mesh *mesh, double dt, double gamma, double *rho
  * If fixed_dt > 0 it is used instead of the CFL step.  Returns dt. */
 double om_step_moving(const om_mesh *mesh, double cfl, double fixed_dt, double gamma, int boundary,
                       double *x, double *mass, double *mom, double *energy, long *n_unpaired);
+
+/* Extension: one moving-mesh step with moving faces (the faces move with the
+ * generators, so the Riemann problem is solved in the face's frame), first or
+ * second order, on conserved variables, for periodic boxes (the mesh from
+ * om_build_mesh, which keeps its unit-box points).  order 1: the cells'
+ * primitives as face states (no gradients, no prediction); order 2:
+ * MUSCL-Hancock on the moving Voronoi mesh (Springel 2010, MNRAS 401, 791,
+ * sections 3.2-3.3), with the least-squares gradients of Pakmor et al. 2016
+ * (MNRAS 455, 1134) and the moving-face flux of Pakmor et al. 2011:
+ *   primitives W = (rho, v, P) per cell; dt = CFL min (reference formula);
+ *   gradients: per variable, min_g sum_faces (A/|d|^2) (W_j - W_i - g.d)^2 with
+ *     d = x_j - x_i (the neighbour's image), solved by the 2x2 / 3x3 normal
+ *     equations, then limited by alpha = min(1, min_faces psi), psi = (W_max -
+ *     W_i) / (g.d/2) or (W_min - W_i) / (g.d/2) by the sign of g.d (W_max, W_min
+ *     over the cell and its neighbours);
+ *   half-step prediction in the frame of the cell (which moves with v):
+ *     rho' = rho - dt/2 rho div v, v' = v - dt/2 grad P / rho, P' = P - dt/2 gamma P div v;
+ *   face states at the midpoint of the generators: W_L = W'_i + g_i.d/2,
+ *     W_R = W'_j - g_j.d/2 (first order, W' alone, when either has rho or P <= 0);
+ *   the face moves with w = (v_i + v_j)/2: HLL on the states boosted by -w along
+ *     the outward normal, then back to the lab frame: F_rho, F_m + w F_rho,
+ *     F_E + w.F_m + |w|^2 F_rho / 2;
+ *   Q_i -= dt sum F A_sym;  x_i += v_i dt, wrapped.
+ * For a face whose other cell has the lower hydro id, d and the area are those
+ * the lower id computes for the same face (negated), so both cells evaluate the
+ * same face states and every face flux cancels exactly between them.
+ * Returns dt, or -1 when the mesh has no unit-box points or is not periodic. */
+double om_step_ale(const om_mesh *mesh, int order, double cfl, double fixed_dt, double gamma, double *x,
+                   double *mass, double *mom, double *energy, long *n_unpaired);
 
 /* Face-pair symmetric areas (extension): out[f] = area of the same face as seen from
  * the lower hydro id.  Returns the number of faces with no partner found. */

@@ -660,6 +660,7 @@ void om_mesh_free(om_mesh *m) {
     free(m->status);
     free(m->cert_k);
     free(m->centroid);
+    free(m->ext);
     memset(m, 0, sizeof(*m));
 }
 
@@ -907,7 +908,8 @@ int om_build_mesh(int dim, int boundary, double buff, int K, const double *pts, 
             om_mesh_free(&b);
         }
     }
-    free(ext);
+    /* kept: the second-order step measures generator offsets in the unit box */
+    m->ext = (double *)realloc(ext, (size_t)(ntot > 0 ? ntot : 1) * dim * sizeof(double));
     m->ghost_ids = (long *)malloc((ntot - n + 1) * sizeof(long));
     m->ghost_code = (int *)malloc((ntot - n + 1) * sizeof(int));
     memcpy(m->ghost_ids, gsrc, (ntot - n) * sizeof(long));
@@ -917,6 +919,7 @@ int om_build_mesh(int dim, int boundary, double buff, int K, const double *pts, 
 
     /* scale back (periodic_mesh.cpp:146-166) */
     const double scale = 1. + (2 * buff);
+    m->unit_scale = scale;
     const double vscale = dim == 2 ? scale * scale : scale * scale * scale;
     const double ascale = dim == 2 ? scale : scale * scale;
     for (long i = 0; i < ntot; i++) {

@@ -319,3 +319,230 @@ double om_step_moving(const om_mesh *m, double cfl, double fixed_dt, double gamm
     free(E);
     return dt;
 }
+
+/* ---- second-order moving-mesh step (extension; see om.h) ---- */
+
+#define MUSCL_NV 5 /* rho, vx, vy, vz, P (vz unused in 2D) */
+
+typedef struct {
+    double w[MUSCL_NV];
+} wvec_t;
+
+/* partner face g of face f (cell i, neighbour image of h < i) in h's face list, or -1 */
+static long partner_face(const om_mesh *m, long i, long f) {
+    long e = m->neighbor[f];
+    long h = owner_of(m, e);
+    int want = reverse_code(code_of(m, e), m->dim, 1);
+    for (long q = 0; q < m->face_counts[h]; q++) {
+        long g = m->face_ptr[h] + q;
+        long e2 = m->neighbor[g];
+        if (e2 < 0) continue;
+        if (owner_of(m, e2) == i && code_of(m, e2) == want) return g;
+    }
+    return -1;
+}
+
+/* generator offset d (physical units) of face f of hydro cell i, seen from i */
+static void face_offset(const om_mesh *m, long i, long f, double *d) {
+    const int dim = m->dim;
+    const long e = m->neighbor[f];
+    for (int a = 0; a < 3; a++) d[a] = 0.0;
+    for (int a = 0; a < dim; a++) d[a] = (m->ext[e * dim + a] - m->ext[i * dim + a]) * m->unit_scale;
+}
+
+/* solves the symmetric normal equations M g = b (dim 2 or 3) by cofactors */
+static void solve_sym(int dim, const double *M, const double *b, double *g) {
+    /* M: xx, xy, xz, yy, yz, zz */
+    if (dim == 2) {
+        double det = M[0] * M[3] - M[1] * M[1];
+        g[0] = (M[3] * b[0] - M[1] * b[1]) / det;
+        g[1] = (M[0] * b[1] - M[1] * b[0]) / det;
+        g[2] = 0.0;
+        return;
+    }
+    double c00 = M[3] * M[5] - M[4] * M[4];
+    double c01 = M[2] * M[4] - M[1] * M[5];
+    double c02 = M[1] * M[4] - M[2] * M[3];
+    double c11 = M[0] * M[5] - M[2] * M[2];
+    double c12 = M[1] * M[2] - M[0] * M[4];
+    double c22 = M[0] * M[3] - M[1] * M[1];
+    double det = M[0] * c00 + M[1] * c01 + M[2] * c02;
+    g[0] = (c00 * b[0] + c01 * b[1] + c02 * b[2]) / det;
+    g[1] = (c01 * b[0] + c11 * b[1] + c12 * b[2]) / det;
+    g[2] = (c02 * b[0] + c12 * b[1] + c22 * b[2]) / det;
+}
+
+static inline double dot_d(const double *a, const double *b, int dim) {
+    double s = a[0] * b[0] + a[1] * b[1];
+    if (dim == 3) s = s + a[2] * b[2];
+    return s;
+}
+
+double om_step_ale(const om_mesh *m, int order, double cfl, double fixed_dt, double gamma, double *x, double *mass,
+                   double *mom, double *energy, long *n_unpaired) {
+    if (!m->ext || !(m->unit_scale > 0.0) || (order != 1 && order != 2)) return -1.0;
+    const int dim = m->dim;
+    const long nh = m->n_hydro;
+    const int nv = dim == 3 ? 5 : 4;       /* variables: rho, v (dim), P */
+    const int ip = dim == 3 ? 4 : 3;       /* index of P */
+    double *rho = (double *)malloc(nh * sizeof(double));
+    double *v = (double *)malloc(nh * dim * sizeof(double));
+    double *E = (double *)malloc(nh * sizeof(double));
+    wvec_t *W = (wvec_t *)calloc(nh, sizeof(wvec_t));
+    wvec_t *Wp = (wvec_t *)calloc(nh, sizeof(wvec_t));
+    double *G = (double *)calloc((size_t)nh * MUSCL_NV * 3, sizeof(double)); /* gradients, var-major */
+    for (long i = 0; i < nh; i++) {
+        double V = m->volumes[i];
+        rho[i] = mass[i] / V;
+        for (int k = 0; k < dim; k++) v[i * dim + k] = mom[i * dim + k] / mass[i];
+        E[i] = energy[i] / V;
+        prim_t s = load(rho, v, E, i, dim);
+        W[i].w[0] = s.rho;
+        for (int k = 0; k < dim; k++) W[i].w[1 + k] = s.v[k];
+        W[i].w[ip] = pressure(&s, dim, gamma);
+    }
+    double dt = fixed_dt > 0 ? fixed_dt : om_dt_cfl(m, cfl, gamma, rho, v, E);
+    long unp = 0;
+    /* gradients (least squares), limiter, half-step prediction; first order: none */
+    if (order == 1) memcpy(Wp, W, nh * sizeof(wvec_t));
+#pragma omp parallel for
+    for (long i = 0; i < (order == 2 ? nh : 0); i++) {
+        double M[6] = {0, 0, 0, 0, 0, 0}, b[MUSCL_NV][3], wmax[MUSCL_NV], wmin[MUSCL_NV];
+        for (int k = 0; k < nv; k++) {
+            b[k][0] = b[k][1] = b[k][2] = 0.0;
+            wmax[k] = wmin[k] = W[i].w[k];
+        }
+        for (long j = 0; j < m->face_counts[i]; j++) {
+            long f = m->face_ptr[i] + j;
+            if (m->neighbor[f] < 0) continue;
+            long h = owner_of(m, m->neighbor[f]);
+            double d[3];
+            face_offset(m, i, f, d);
+            double wgt = m->area[f] / dot_d(d, d, dim);
+            M[0] += wgt * d[0] * d[0];
+            M[1] += wgt * d[0] * d[1];
+            M[3] += wgt * d[1] * d[1];
+            if (dim == 3) {
+                M[2] += wgt * d[0] * d[2];
+                M[4] += wgt * d[1] * d[2];
+                M[5] += wgt * d[2] * d[2];
+            }
+            for (int k = 0; k < nv; k++) {
+                double dw = W[h].w[k] - W[i].w[k];
+                for (int a = 0; a < dim; a++) b[k][a] += wgt * dw * d[a];
+                wmax[k] = dmax(wmax[k], W[h].w[k]);
+                wmin[k] = dmin(wmin[k], W[h].w[k]);
+            }
+        }
+        double *g = G + (size_t)i * MUSCL_NV * 3;
+        for (int k = 0; k < nv; k++) solve_sym(dim, M, b[k], g + 3 * k);
+        /* limiter */
+        double alpha[MUSCL_NV];
+        for (int k = 0; k < nv; k++) alpha[k] = 1.0;
+        for (long j = 0; j < m->face_counts[i]; j++) {
+            long f = m->face_ptr[i] + j;
+            if (m->neighbor[f] < 0) continue;
+            double d[3];
+            face_offset(m, i, f, d);
+            for (int k = 0; k < nv; k++) {
+                double dw = dot_d(g + 3 * k, d, dim) * 0.5;
+                double psi = 1.0;
+                if (dw > 0.0)
+                    psi = (wmax[k] - W[i].w[k]) / dw;
+                else if (dw < 0.0)
+                    psi = (wmin[k] - W[i].w[k]) / dw;
+                alpha[k] = dmin(alpha[k], psi);
+            }
+        }
+        for (int k = 0; k < nv; k++)
+            for (int a = 0; a < 3; a++) g[3 * k + a] = alpha[k] * g[3 * k + a];
+        /* half-step prediction in the frame moving with the cell */
+        double div = g[3 * 1 + 0] + g[3 * 2 + 1];
+        if (dim == 3) div = div + g[3 * 3 + 2];
+        const double hdt = 0.5 * dt;
+        const double r = W[i].w[0], P = W[i].w[ip];
+        Wp[i].w[0] = r - hdt * (r * div);
+        for (int a = 0; a < dim; a++) Wp[i].w[1 + a] = W[i].w[1 + a] - hdt * (g[3 * ip + a] / r);
+        Wp[i].w[ip] = P - hdt * (gamma * P * div);
+    }
+    /* fluxes and update */
+#pragma omp parallel for reduction(+ : unp)
+    for (long i = 0; i < nh; i++) {
+        prim_t tot;
+        memset(&tot, 0, sizeof(tot));
+        const double *gi = G + (size_t)i * MUSCL_NV * 3;
+        for (long j = 0; j < m->face_counts[i]; j++) {
+            long f = m->face_ptr[i] + j;
+            long e = m->neighbor[f];
+            if (e < 0) continue;
+            long h = owner_of(m, e);
+            double d[3], A = m->area[f];
+            face_offset(m, i, f, d);
+            if (h < i) {
+                long g2 = partner_face(m, i, f);
+                if (g2 >= 0) {
+                    double dh[3];
+                    face_offset(m, h, g2, dh);
+                    for (int a = 0; a < 3; a++) d[a] = -dh[a];
+                    A = m->area[g2];
+                } else {
+                    unp++;
+                }
+            }
+            const double *gh = G + (size_t)h * MUSCL_NV * 3;
+            wvec_t L = Wp[i], R = Wp[h];
+            if (order == 2) {
+                for (int k = 0; k < nv; k++) {
+                    L.w[k] = Wp[i].w[k] + dot_d(gi + 3 * k, d, dim) * 0.5;
+                    R.w[k] = Wp[h].w[k] - dot_d(gh + 3 * k, d, dim) * 0.5;
+                }
+                if (!(L.w[0] > 0.0 && L.w[ip] > 0.0 && R.w[0] > 0.0 && R.w[ip] > 0.0)) {
+                    L = Wp[i];
+                    R = Wp[h];
+                }
+            }
+            double w[3] = {0, 0, 0};
+            for (int a = 0; a < dim; a++) w[a] = (v[i * dim + a] + v[h * dim + a]) * 0.5;
+            prim_t sl, sr;
+            memset(&sl, 0, sizeof(sl));
+            memset(&sr, 0, sizeof(sr));
+            sl.rho = L.w[0];
+            sr.rho = R.w[0];
+            for (int a = 0; a < dim; a++) {
+                sl.v[a] = L.w[1 + a] - w[a];
+                sr.v[a] = R.w[1 + a] - w[a];
+            }
+            sl.E = L.w[ip] / (gamma - 1.0) + 0.5 * sl.rho * dot_d(sl.v, sl.v, dim);
+            sr.E = R.w[ip] / (gamma - 1.0) + 0.5 * sr.rho * dot_d(sr.v, sr.v, dim);
+            double nout[3] = {-m->normal[3 * f], -m->normal[3 * f + 1], -m->normal[3 * f + 2]};
+            prim_t fl = hll(sl, sr, nout, dim, gamma);
+            /* back to the lab frame */
+            double wm = dot_d(w, fl.v, dim), ww = dot_d(w, w, dim);
+            fl.E = fl.E + wm + 0.5 * ww * fl.rho;
+            for (int a = 0; a < dim; a++) fl.v[a] = fl.v[a] + w[a] * fl.rho;
+            tot.rho += fl.rho * A;
+            tot.v[0] += fl.v[0] * A;
+            tot.v[1] += fl.v[1] * A;
+            if (dim == 3) tot.v[2] += fl.v[2] * A;
+            tot.E += fl.E * A;
+        }
+        mass[i] = mass[i] - dt * tot.rho;
+        for (int k = 0; k < dim; k++) mom[i * dim + k] = mom[i * dim + k] - dt * tot.v[k];
+        energy[i] = energy[i] - dt * tot.E;
+    }
+    for (long i = 0; i < nh; i++)
+        for (int k = 0; k < dim; k++) {
+            double p = x[i * dim + k] + v[i * dim + k] * dt;
+            if (p < 0.0) p += 1.0;
+            if (p >= 1.0) p -= 1.0;
+            x[i * dim + k] = p;
+        }
+    if (n_unpaired) *n_unpaired = unp;
+    free(rho);
+    free(v);
+    free(E);
+    free(W);
+    free(Wp);
+    free(G);
+    return dt;
+}

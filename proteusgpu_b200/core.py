@@ -76,8 +76,10 @@ class Context:
 
     dim, k: the reference's compile-time dimension and _K_ (Config.sh:4-34),
     here runtime parameters.  boundary: "periodic" (reference) or "reflective".
-    flux: "reference" (stored inward normal, own face area, as riemann.cpp) or
-    "physical" (outward normal, face-pair-symmetric area).  predicates:
+    flux: "reference" (stored inward normal, own face area, as riemann.cpp),
+    "physical" (outward normal, face-pair-symmetric area), or, for moving-mesh
+    steps in periodic boxes, "ale1" / "ale2" (faces moving with the generators,
+    first / second order).  predicates:
     "reference" (a near-degenerate predicate fails the cell, cell.cpp:216-218) or
     "robust" (the vertex is kept).  k_fallback: moving-mesh steps recompute cells
     whose certificate does not close within k neighbours with this budget.
@@ -92,7 +94,7 @@ class Context:
         L.pgpu_default_params(C.byref(p))
         p.dim, p.k, p.buff, p.gamma, p.device = dim, k, buff, gamma, device
         p.boundary = {"periodic": 0, "reflective": 1}[boundary]
-        p.flux_mode = {"reference": 0, "physical": 1}[flux]
+        p.flux_mode = {"reference": 0, "physical": 1, "ale1": 2, "ale2": 3}[flux]
         p.predicates = {"reference": 0, "robust": 1}[predicates]
         p.k_fallback = k_fallback
         p.precision = {"fp64": 0, "fp32": 1}[precision]

@@ -199,7 +199,8 @@ int pgpu_create(const pgpu_params* p, pgpu_ctx** out) {
     if (!(p->buff >= 0.0 && p->buff < 0.5)) return PGPU_EINVAL;
     if (!(p->gamma > 1.0)) return PGPU_EINVAL;
     if (p->boundary != PGPU_PERIODIC && p->boundary != PGPU_REFLECTIVE) return PGPU_EINVAL;
-    if (p->flux_mode != PGPU_FLUX_REFERENCE && p->flux_mode != PGPU_FLUX_PHYSICAL) return PGPU_EINVAL;
+    if (p->flux_mode < PGPU_FLUX_REFERENCE || p->flux_mode > PGPU_FLUX_ALE2) return PGPU_EINVAL;
+    if (p->flux_mode >= PGPU_FLUX_ALE1 && p->boundary != PGPU_PERIODIC) return PGPU_EINVAL;
     if (p->predicates != PGPU_PRED_REFERENCE && p->predicates != PGPU_PRED_ROBUST) return PGPU_EINVAL;
     if (p->precision != PGPU_CLIP_FP64 && p->precision != PGPU_CLIP_FP32) return PGPU_EINVAL;
     if (p->k_fallback != 0 && (p->k_fallback <= p->k || p->k_fallback > pgpu::MAX_K)) return PGPU_EINVAL;
@@ -233,7 +234,7 @@ void pgpu_destroy(pgpu_ctx* c) {
                       &c->qs,    &c->knn,     &c->vol,      &c->fptr,   &c->fcnt,      &c->status,     &c->certk,
                       &c->centroid, &c->f_nb, &c->f_own,    &c->f_geo,  &c->scan_tmp,  &c->scalars,    &c->rho,
                       &c->vel,   &c->energy,  &c->rho2,     &c->vel2,   &c->energy2,   &c->mass,       &c->mom,
-                      &c->en,    &c->w4,      &c->we,       &c->red_tmp, &c->dl_ptr,   &c->dl_a,       &c->dl_b,
+                      &c->en,    &c->w4,      &c->we,       &c->ale_wp, &c->ale_grad, &c->red_tmp, &c->dl_ptr,   &c->dl_a,       &c->dl_b,
                       &c->dl_c,  &c->kq,      &c->kb.w,     &c->kb.wbf,  &c->kb.adam_m, &c->kb.adam_v, &c->kb.part,
                       &c->kb.feat, &c->kb.hist_vol, &c->kb.miss, &c->kb.ksum, &c->kb.labels, &c->kb.tmp_out,
                       &c->bin_lvl, &c->sub_off, &c->sub_cnt, &c->sub_start, &c->sort_big, &c->sort_keys,
@@ -666,8 +667,12 @@ int pgpu_batch_init(pgpu_ctx* c, int n_inst, const int64_t* counts, const double
             return fail(c, PGPU_EINVAL, "pgpu_batch_init: bad instance parameters");
         n += counts[b];
     }
-    if (c->prm.flux_mode != PGPU_FLUX_PHYSICAL)
-        return fail(c, PGPU_EINVAL, "pgpu_batch_init: batches use PGPU_FLUX_PHYSICAL");
+    if (c->prm.flux_mode == PGPU_FLUX_REFERENCE)
+        return fail(c, PGPU_EINVAL, "pgpu_batch_init: batches use PGPU_FLUX_PHYSICAL or a moving-face mode");
+    if (c->prm.flux_mode >= PGPU_FLUX_ALE1)
+        for (int b = 0; b < n_inst; b++)
+            if (boundary[b] != PGPU_PERIODIC)
+                return fail(c, PGPU_EINVAL, "pgpu_batch_init: moving-face modes need periodic instances");
     CK(pgpu::set_instances(c, n_inst, counts, buff, gamma, boundary));
     return sim_init_common(c, pos, rho, v, E, deposit, n);
 }

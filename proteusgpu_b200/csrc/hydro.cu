@@ -287,6 +287,273 @@ __global__ void k_flux_update(const double4* __restrict__ w4, const double* __re
     }
 }
 
+// ---- moving faces (extension): the faces move with the generators, so the
+// Riemann problem is solved in the face's frame (Pakmor et al. 2011); second
+// order by MUSCL-Hancock with least-squares gradients (Springel 2010,
+// Pakmor et al. 2016).  Periodic boxes.  Primitives W = (rho, v, P), NV = D + 2.
+// The operation order follows the oracle's om_step_ale.
+template <int D>
+__device__ __forceinline__ void ale_prim(const double4* __restrict__ w4, const double* __restrict__ we, uint32_t h,
+                                         double gamma, double* W) {
+    const double4 a = w4[h];
+    const Prim s = {a.x, a.y, a.z, a.w, we[h]};
+    W[0] = s.rho;
+    W[1] = s.vx;
+    W[2] = s.vy;
+    if (D == 3) W[3] = s.vz;
+    W[D + 1] = pressure<D>(s, gamma);
+}
+
+template <int D>
+__device__ __forceinline__ double dotd(const double* a, const double* b) {
+    double s = a[0] * b[0] + a[1] * b[1];
+    if (D == 3) s = s + a[2] * b[2];
+    return s;
+}
+
+// generator offset of a face: the neighbour's image minus the cell, physical units
+template <int D>
+__device__ __forceinline__ void ale_offset(const typename PointOf<D>::type* __restrict__ ext, int32_t nb, uint32_t i,
+                                           double scale, double* d) {
+    const typename PointOf<D>::type pe = ext[nb], pc = ext[i];
+    d[0] = (pe.x - pc.x) * scale;
+    d[1] = (pe.y - pc.y) * scale;
+    d[2] = D == 3 ? (pz(pe) - pz(pc)) * scale : 0.0;
+}
+
+// Per cell: least-squares gradients of W, the limiter, and the half-step prediction in
+// the cell's frame: wp[i * NV + k], grad[(i * NV + k) * D + a].
+template <int D>
+__global__ void k_ale_grad(const double4* __restrict__ w4, const double* __restrict__ we,
+                           const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fcnt,
+                           const uint32_t* __restrict__ f_own, const int32_t* __restrict__ f_nb,
+                           const double4* __restrict__ f_geo, const typename PointOf<D>::type* __restrict__ ext,
+                           int64_t n, const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst,
+                           const unsigned long long* __restrict__ dt_inst, double fixed_dt,
+                           double* __restrict__ wp, double* __restrict__ grad, const uint32_t* __restrict__ order,
+                           const uint32_t* __restrict__ perm) {
+    constexpr int NV = D + 2, IP = D + 1;
+    const int64_t t = (int64_t)blockIdx.x * HT + threadIdx.x;
+    if (t >= n) return;
+    const int64_t i = order ? (int64_t)perm[order[t]] : t;
+    const int b = inst[i];
+    const double gamma = ip[b].gamma, scale = ip[b].scale_out;
+    const double dt = fixed_dt > 0 ? fixed_dt : __longlong_as_double((long long)dt_inst[b]);
+    double Wi[NV];
+    ale_prim<D>(w4, we, (uint32_t)i, gamma, Wi);
+    double* gi = grad + (size_t)i * NV * D;
+    if (!(Wi[0] >= 0.0)) {  // no mesh cell this step
+        for (int k = 0; k < NV; k++) {
+            wp[i * NV + k] = Wi[k];
+            for (int a = 0; a < D; a++) gi[k * D + a] = 0.0;
+        }
+        return;
+    }
+    double M[6] = {0, 0, 0, 0, 0, 0}, bb[NV][3], wmax[NV], wmin[NV];
+    for (int k = 0; k < NV; k++) {
+        bb[k][0] = bb[k][1] = bb[k][2] = 0.0;
+        wmax[k] = wmin[k] = Wi[k];
+    }
+    const uint32_t fp = fptr[i], nf = fcnt[i];
+    for (uint32_t q = 0; q < nf; q++) {
+        const uint32_t own = f_own[fp + q];
+        if (own == BOX_FACE) continue;
+        const uint32_t h = own & OWNER_MASK;
+        if (w4[h].x < 0.0) continue;
+        double d[3], Wh[NV];
+        ale_offset<D>(ext, f_nb[fp + q], (uint32_t)i, scale, d);
+        ale_prim<D>(w4, we, h, gamma, Wh);
+        const double wgt = f_geo[fp + q].w / dotd<D>(d, d);
+        M[0] += wgt * d[0] * d[0];
+        M[1] += wgt * d[0] * d[1];
+        M[3] += wgt * d[1] * d[1];
+        if (D == 3) {
+            M[2] += wgt * d[0] * d[2];
+            M[4] += wgt * d[1] * d[2];
+            M[5] += wgt * d[2] * d[2];
+        }
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            const double dw = Wh[k] - Wi[k];
+            for (int a = 0; a < D; a++) bb[k][a] += wgt * dw * d[a];
+            wmax[k] = dmax_ref(wmax[k], Wh[k]);
+            wmin[k] = dmin_ref(wmin[k], Wh[k]);
+        }
+    }
+    double g[NV][3];
+#pragma unroll
+    for (int k = 0; k < NV; k++) {
+        if (D == 2) {
+            const double det = M[0] * M[3] - M[1] * M[1];
+            g[k][0] = (M[3] * bb[k][0] - M[1] * bb[k][1]) / det;
+            g[k][1] = (M[0] * bb[k][1] - M[1] * bb[k][0]) / det;
+            g[k][2] = 0.0;
+        } else {
+            const double c00 = M[3] * M[5] - M[4] * M[4];
+            const double c01 = M[2] * M[4] - M[1] * M[5];
+            const double c02 = M[1] * M[4] - M[2] * M[3];
+            const double c11 = M[0] * M[5] - M[2] * M[2];
+            const double c12 = M[1] * M[2] - M[0] * M[4];
+            const double c22 = M[0] * M[3] - M[1] * M[1];
+            const double det = M[0] * c00 + M[1] * c01 + M[2] * c02;
+            g[k][0] = (c00 * bb[k][0] + c01 * bb[k][1] + c02 * bb[k][2]) / det;
+            g[k][1] = (c01 * bb[k][0] + c11 * bb[k][1] + c12 * bb[k][2]) / det;
+            g[k][2] = (c02 * bb[k][0] + c12 * bb[k][1] + c22 * bb[k][2]) / det;
+        }
+    }
+    // limiter: the reconstructed value at every face midpoint stays within the
+    // neighbourhood's extrema
+    double alpha[NV];
+    for (int k = 0; k < NV; k++) alpha[k] = 1.0;
+    for (uint32_t q = 0; q < nf; q++) {
+        const uint32_t own = f_own[fp + q];
+        if (own == BOX_FACE) continue;
+        if (w4[own & OWNER_MASK].x < 0.0) continue;
+        double d[3];
+        ale_offset<D>(ext, f_nb[fp + q], (uint32_t)i, scale, d);
+#pragma unroll
+        for (int k = 0; k < NV; k++) {
+            const double dw = dotd<D>(g[k], d) * 0.5;
+            double psi = 1.0;
+            if (dw > 0.0)
+                psi = (wmax[k] - Wi[k]) / dw;
+            else if (dw < 0.0)
+                psi = (wmin[k] - Wi[k]) / dw;
+            alpha[k] = dmin_ref(alpha[k], psi);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+        for (int a = 0; a < 3; a++) g[k][a] = alpha[k] * g[k][a];
+    double div = g[1][0] + g[2][1];
+    if (D == 3) div = div + g[3][2];
+    const double hdt = 0.5 * dt;
+    const double r = Wi[0], P = Wi[IP];
+    wp[i * NV] = r - hdt * (r * div);
+    for (int a = 0; a < D; a++) wp[i * NV + 1 + a] = Wi[1 + a] - hdt * (g[IP][a] / r);
+    wp[i * NV + IP] = P - hdt * (gamma * P * div);
+#pragma unroll
+    for (int k = 0; k < NV; k++)
+        for (int a = 0; a < D; a++) gi[k * D + a] = g[k][a];
+}
+
+// Per cell: moving-face HLL fluxes (face states reconstructed to the generators'
+// midpoint with ORDER 2), the conserved update and the drift.  For a face whose
+// other cell has the lower hydro id, the offset and area are that cell's (its
+// partner face's), so both cells evaluate the same face and the fluxes cancel.
+template <int D, int ORDER>
+__global__ void k_ale_flux(const double4* __restrict__ w4, const double* __restrict__ we,
+                           const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fcnt,
+                           const uint32_t* __restrict__ f_own, const int32_t* __restrict__ f_nb,
+                           const double4* __restrict__ f_geo, const typename PointOf<D>::type* __restrict__ ext,
+                           int64_t n, const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst,
+                           const unsigned long long* __restrict__ dt_inst, double fixed_dt,
+                           const double* __restrict__ wp, const double* __restrict__ grad, double* __restrict__ mass,
+                           double* __restrict__ mom, double* __restrict__ en, double* __restrict__ pos,
+                           DevScalars* __restrict__ sc, const uint32_t* __restrict__ order,
+                           const uint32_t* __restrict__ perm) {
+    constexpr int NV = D + 2, IP = D + 1;
+    const int64_t t = (int64_t)blockIdx.x * HT + threadIdx.x;
+    if (t >= n) return;
+    const int64_t i = order ? (int64_t)perm[order[t]] : t;
+    const int b = inst[i];
+    const double gamma = ip[b].gamma, scale = ip[b].scale_out;
+    const double dt = fixed_dt > 0 ? fixed_dt : __longlong_as_double((long long)dt_inst[b]);
+    const double4 wi = w4[i];
+    const bool alive = wi.x >= 0.0;
+    double tr = 0, tx = 0, ty = 0, tz = 0, te = 0;
+    const uint32_t fp = fptr[i], nf = alive ? fcnt[i] : 0u;
+    unsigned nbox = 0, nunp = 0;
+    double Wi[NV];
+    if (ORDER == 1) ale_prim<D>(w4, we, (uint32_t)i, gamma, Wi);
+    for (uint32_t q = 0; q < nf; q++) {
+        const uint32_t own = f_own[fp + q];
+        if (own == BOX_FACE) {
+            nbox++;
+            continue;
+        }
+        const uint32_t h = own & OWNER_MASK, code = own >> OWNER_BITS;
+        const double4 wh = w4[h];
+        if (wh.x < 0.0) continue;  // the neighbour has no mesh cell this step: a wall
+        double d[3];
+        double A = f_geo[fp + q].w;
+        ale_offset<D>(ext, f_nb[fp + q], (uint32_t)i, scale, d);
+        if (h < (uint32_t)i) {
+            const uint32_t want = pack_owner((uint32_t)i, reverse_code(code, D, true));
+            const uint32_t hp = fptr[h], hn = fcnt[h];
+            bool found = false;
+            for (uint32_t r = 0; r < hn; r++)
+                if (f_own[hp + r] == want) {
+                    double dh[3];
+                    ale_offset<D>(ext, f_nb[hp + r], h, scale, dh);
+                    d[0] = -dh[0];
+                    d[1] = -dh[1];
+                    d[2] = -dh[2];
+                    A = f_geo[hp + r].w;
+                    found = true;
+                    break;
+                }
+            if (!found) nunp++;
+        }
+        double L[NV], R[NV];
+        if (ORDER == 1) {
+            for (int k = 0; k < NV; k++) L[k] = Wi[k];
+            ale_prim<D>(w4, we, h, gamma, R);
+        } else {
+            const double* gi = grad + (size_t)i * NV * D;
+            const double* gh = grad + (size_t)h * NV * D;
+            double gk[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int k = 0; k < NV; k++) {
+                for (int a = 0; a < D; a++) gk[a] = gi[k * D + a];
+                L[k] = wp[i * NV + k] + dotd<D>(gk, d) * 0.5;
+                for (int a = 0; a < D; a++) gk[a] = gh[k * D + a];
+                R[k] = wp[(size_t)h * NV + k] - dotd<D>(gk, d) * 0.5;
+            }
+            if (!(L[0] > 0.0 && L[IP] > 0.0 && R[0] > 0.0 && R[IP] > 0.0)) {
+                for (int k = 0; k < NV; k++) {
+                    L[k] = wp[i * NV + k];
+                    R[k] = wp[(size_t)h * NV + k];
+                }
+            }
+        }
+        double w[3] = {(wi.y + wh.y) * 0.5, (wi.z + wh.z) * 0.5, D == 3 ? (wi.w + wh.w) * 0.5 : 0.0};
+        Prim sl = {L[0], L[1] - w[0], L[2] - w[1], D == 3 ? L[3] - w[2] : 0.0, 0.0};
+        Prim sr = {R[0], R[1] - w[0], R[2] - w[1], D == 3 ? R[3] - w[2] : 0.0, 0.0};
+        const double vl[3] = {sl.vx, sl.vy, sl.vz}, vr[3] = {sr.vx, sr.vy, sr.vz};
+        sl.E = L[IP] / (gamma - 1.0) + 0.5 * sl.rho * dotd<D>(vl, vl);
+        sr.E = R[IP] / (gamma - 1.0) + 0.5 * sr.rho * dotd<D>(vr, vr);
+        const double4 g = f_geo[fp + q];
+        Flux fl = hll<D>(sl, sr, -g.x, -g.y, -g.z, gamma);
+        const double fm[3] = {fl.mx, fl.my, fl.mz};
+        const double wm = dotd<D>(w, fm), ww = dotd<D>(w, w);
+        fl.E = fl.E + wm + 0.5 * ww * fl.rho;
+        fl.mx = fl.mx + w[0] * fl.rho;
+        fl.my = fl.my + w[1] * fl.rho;
+        if (D == 3) fl.mz = fl.mz + w[2] * fl.rho;
+        tr += fl.rho * A;
+        tx += fl.mx * A;
+        ty += fl.my * A;
+        if (D == 3) tz += fl.mz * A;
+        te += fl.E * A;
+    }
+    if (nbox) atomicAdd(&sc->box_faces, nbox);
+    if (nunp) atomicAdd(&sc->unpaired, nunp);
+    mass[i] = mass[i] - dt * tr;
+    mom[i * D] = mom[i * D] - dt * tx;
+    mom[i * D + 1] = mom[i * D + 1] - dt * ty;
+    if (D == 3) mom[i * D + 2] = mom[i * D + 2] - dt * tz;
+    en[i] = en[i] - dt * te;
+    const double vv[3] = {wi.y, wi.z, wi.w};
+#pragma unroll
+    for (int a = 0; a < D; a++) {
+        double p = pos[i * D + a] + vv[a] * dt;
+        if (p < 0.0) p += 1.0;
+        if (p >= 1.0) p -= 1.0;
+        pos[i * D + a] = p;
+    }
+}
+
 // Deterministic sums (mass, momentum, energy) over hydro cells: fixed block
 // partials, then one ordered pass.
 template <int D>
@@ -349,7 +616,7 @@ cudaError_t launch_hydro_ref(pgpu_ctx* c, double dt) {
     double* e2 = ensure<double>(c->energy2, n + 1, &e);
     if (e) return e;
     DevScalars* sc = (DevScalars*)c->scalars.p;
-    const bool phys = c->prm.flux_mode == PGPU_FLUX_PHYSICAL;
+    const bool phys = c->prm.flux_mode != PGPU_FLUX_REFERENCE;
     if (n > 0) {
 #define PGPU_HREF(DD, PH)                                                                                         \
     k_hydro_ref<DD, PH><<<nblk(n, HT), HT, 0, c->stream>>>(                                                      \
@@ -433,10 +700,74 @@ cudaError_t launch_prim_dt(pgpu_ctx* c, double cfl, double fixed_dt) {
     return cudaGetLastError();
 }
 
+// moving faces: gradients (second order), then fluxes + update + drift
+static cudaError_t launch_ale(pgpu_ctx* c, double fixed_dt) {
+    const int D = c->prm.dim;
+    const int64_t n = c->n_hydro;
+    const int order2 = c->prm.flux_mode == PGPU_FLUX_ALE2;
+    const int NV = D + 2;
+    cudaError_t e = cudaSuccess;
+    double* wp = ensure<double>(c->ale_wp, (size_t)n * NV + 1, &e);
+    double* gr = ensure<double>(c->ale_grad, (size_t)n * NV * D + 1, &e);
+    if (e) return e;
+    DevScalars* sc = (DevScalars*)c->scalars.p;
+    const uint32_t* order = c->have_mesh && !c->all_cells && c->n_query == n ? (const uint32_t*)c->qs.p : nullptr;
+    const InstPar* ip = (const InstPar*)c->inst.d_par.p;
+    const uint16_t* inst = (const uint16_t*)c->inst.d_inst_h.p;
+    const unsigned long long* dti = (const unsigned long long*)c->inst.d_dt.p;
+    const double4* w4 = (const double4*)c->w4.p;
+    const double* we = (const double*)c->we.p;
+    const uint32_t* fptr = (const uint32_t*)c->fptr.p;
+    const uint32_t* fcnt = (const uint32_t*)c->fcnt.p;
+    const uint32_t* fown = (const uint32_t*)c->f_own.p;
+    const int32_t* fnb = (const int32_t*)c->f_nb.p;
+    const double4* fgeo = (const double4*)c->f_geo.p;
+    const uint32_t* perm = (const uint32_t*)c->perm.p;
+    int launches = 0;
+    if (D == 2) {
+        const double2* ext = (const double2*)c->ext.p;
+        if (order2) {
+            k_ale_grad<2><<<nblk(n, HT), HT, 0, c->stream>>>(w4, we, fptr, fcnt, fown, fnb, fgeo, ext, n, ip, inst,
+                                                             dti, fixed_dt, wp, gr, order, perm);
+            k_ale_flux<2, 2><<<nblk(n, HT), HT, 0, c->stream>>>(w4, we, fptr, fcnt, fown, fnb, fgeo, ext, n, ip, inst,
+                                                                dti, fixed_dt, wp, gr, (double*)c->mass.p,
+                                                                (double*)c->mom.p, (double*)c->en.p,
+                                                                (double*)c->pos.p, sc, order, perm);
+            launches = 2;
+        } else {
+            k_ale_flux<2, 1><<<nblk(n, HT), HT, 0, c->stream>>>(w4, we, fptr, fcnt, fown, fnb, fgeo, ext, n, ip, inst,
+                                                                dti, fixed_dt, wp, gr, (double*)c->mass.p,
+                                                                (double*)c->mom.p, (double*)c->en.p,
+                                                                (double*)c->pos.p, sc, order, perm);
+            launches = 1;
+        }
+    } else {
+        const double4* ext = (const double4*)c->ext.p;
+        if (order2) {
+            k_ale_grad<3><<<nblk(n, HT), HT, 0, c->stream>>>(w4, we, fptr, fcnt, fown, fnb, fgeo, ext, n, ip, inst,
+                                                             dti, fixed_dt, wp, gr, order, perm);
+            k_ale_flux<3, 2><<<nblk(n, HT), HT, 0, c->stream>>>(w4, we, fptr, fcnt, fown, fnb, fgeo, ext, n, ip, inst,
+                                                                dti, fixed_dt, wp, gr, (double*)c->mass.p,
+                                                                (double*)c->mom.p, (double*)c->en.p,
+                                                                (double*)c->pos.p, sc, order, perm);
+            launches = 2;
+        } else {
+            k_ale_flux<3, 1><<<nblk(n, HT), HT, 0, c->stream>>>(w4, we, fptr, fcnt, fown, fnb, fgeo, ext, n, ip, inst,
+                                                                dti, fixed_dt, wp, gr, (double*)c->mass.p,
+                                                                (double*)c->mom.p, (double*)c->en.p,
+                                                                (double*)c->pos.p, sc, order, perm);
+            launches = 1;
+        }
+    }
+    count_launches(launches);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_flux_update(pgpu_ctx* c, double fixed_dt) {
     const int D = c->prm.dim;
     const int64_t n = c->n_hydro;
     if (n <= 0) return cudaSuccess;
+    if (c->prm.flux_mode == PGPU_FLUX_ALE1 || c->prm.flux_mode == PGPU_FLUX_ALE2) return launch_ale(c, fixed_dt);
     DevScalars* sc = (DevScalars*)c->scalars.p;
     const bool phys = c->prm.flux_mode == PGPU_FLUX_PHYSICAL;
     // the current mesh's query list covers exactly the hydro cells, in spatial order

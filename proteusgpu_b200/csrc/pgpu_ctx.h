@@ -162,6 +162,7 @@ struct pgpu_ctx {
     pgpu::DevBuf rho, vel, energy, rho2, vel2, energy2;  // primitives (drop-in hydro)
     pgpu::DevBuf mass, mom, en;   // conserved (moving mesh)
     pgpu::DevBuf w4, we;          // per-step primitives (rho, v) and E
+    pgpu::DevBuf ale_wp, ale_grad; // moving-face modes: predicted primitives and their gradients
     pgpu::DevBuf red_tmp;         // reduction partials
     // download staging
     pgpu::DevBuf dl_ptr, dl_a, dl_b, dl_c;

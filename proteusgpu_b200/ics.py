@@ -339,6 +339,20 @@ def kh_2d(n_side: int = 2048, seed: int = 3, gamma: float = 5.0 / 3.0, rho_ratio
     return _finish(IC("kh2d", 2, pos, rho, vel, energy, gamma, "periodic", spec=spec))
 
 
+def sound_wave_2d(n_side: int, amp: float = 1e-3, seed: int = 1, gamma: float = 5.0 / 3.0) -> IC:
+    """A right-moving plane sound wave along x in a periodic box on a jittered lattice:
+    rho = 1 + amp s, vx = c amp s, P = 1 + gamma amp s, s = sin(2 pi x), c = sqrt(gamma).
+    To first order in amp it travels unchanged at speed c (convergence tests)."""
+    pos = jittered_lattice(n_side, 2, 0.1, np.random.default_rng(seed))
+    c = math.sqrt(gamma)
+    s = np.sin(2.0 * math.pi * pos[:, 0])
+    rho = 1.0 + amp * s
+    vel = np.stack([c * amp * s, np.zeros(len(pos))], axis=1)
+    P = 1.0 + gamma * amp * s
+    energy = P / (gamma - 1.0) + 0.5 * rho * vel[:, 0] ** 2
+    return _finish(IC("wave2d", 2, pos, rho, vel, energy, gamma, "periodic"))
+
+
 def clump_params(seed: int, n_clumps: int = 64):
     """Centres (uniform in the box) and widths (log-uniform in [0.005, 0.05]) of the clumps."""
     c = np.arange(n_clumps, dtype=np.int64)
