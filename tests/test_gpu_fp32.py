@@ -77,3 +77,19 @@ def test_fp32_moving_mesh_steps():
             res.append((dts,) + ctx.sim_get())
     for a, b in zip(res[0], res[1]):
         assert np.array_equal(np.asarray(a), np.asarray(b))
+
+
+@pytest.mark.parametrize("sep", [1e-6, 1e-7, 1e-8])
+def test_fp32_near_coincident_seeds(sep):
+    """Pairs of seeds sep apart (500 pairs among 20,000 uniform points, random
+    directions): tiny faces whose global-frame FP64 determinants carry a large
+    rounding relative to the face.  The FP32 form must still equal the FP64 form."""
+    rng = np.random.default_rng(41)
+    pts = ics.uniform_points(20000, 3, 40)
+    d = rng.normal(size=(500, 3))
+    d *= sep / np.linalg.norm(d, axis=1)[:, None]
+    twins = np.clip(pts[:500] + d, 0.0, np.nextafter(1.0, 0.0))
+    pts = np.concatenate([pts, twins])
+    g64, s64, g32, s32 = both(3, 190, pts, buff=0.1)
+    assert_identical(g64, g32)
+    assert_same_topology(g64, om.build_mesh(pts, 190, buff=0.1))
