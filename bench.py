@@ -284,7 +284,9 @@ HEADLINE, PLAIN_FORM = "learned_fp32", "plain_fp64"
 
 # DRAM bytes per cell of one k_clip32 launch (read + write / cells), from an ncu capture
 # of the clustered 1,048,576-cell case on learned-K lists, used for `traffic`.
-CLIP32_DRAM_BYTES_PER_CELL = (665.013248e6 + 770.234112e6) / 1_048_576
+CLIP32_DRAM_BYTES_PER_CELL = (669.431296e6 + 774.266112e6) / 1_048_576
+# and of one k_flux_update launch on the same case (the hydro stage's dominant kernel)
+FLUX_DRAM_BYTES_PER_CELL = (1293.150976e6 + 146.343168e6) / 1_048_576
 
 
 def _barrier(dist):
@@ -574,7 +576,10 @@ def run_ours(args, rank, world, local_rank):
                 "traffic": None, "peak_source": f"MEASURED_PEAKS.json hbm_gbs ({hbm_src})"}
     hyd = n_query * W["hydro_bytes_per_cell"] / (stage[4] * 1e-3) / 1e9
     roof_hydro = {"kernel": "k_prim_dt + k_flux_update", "bound": "hbm", "achieved": hyd, "peak": hbm,
-                  "unit": "GB/s", "frac": hyd / hbm, "traffic": None,
+                  "unit": "GB/s", "frac": hyd / hbm,
+                  "traffic": FLUX_DRAM_BYTES_PER_CELL * n_query if D == 3 else None,
+                  "traffic_note": "k_flux_update DRAM bytes per launch: ncu capture of the clustered 1,048,576-cell "
+                                  "case scaled by cells (1,372 B per cell against 683 compulsory)",
                   "work": f"{W['hydro_bytes_per_cell']} compulsory bytes per cell-update"}
 
     cpu = None

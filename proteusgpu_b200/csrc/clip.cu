@@ -1161,19 +1161,6 @@ __device__ __forceinline__ void vertex_h32(const float4* hp, uint32_t t, float4&
                      per3f(p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z));
 }
 
-// One cofactor of vertex_h32<3> (comp 0..3: V.x, V.y, V.z, V.w) and its permanent:
-// the same arguments in the same order, so a vertex computed by four lanes is
-// bit-identical to one computed by one.
-__device__ __forceinline__ void cofactor_h32(const float4* hp, uint32_t t, int comp, float& cof, float& per) {
-    const float4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)], p3 = hp[tri_c(t)];
-    const float a0 = comp == 0 ? p1.w : p1.x, a1 = comp == 1 ? p1.w : p1.y, a2 = comp == 2 ? p1.w : p1.z;
-    const float b0 = comp == 0 ? p2.w : p2.x, b1 = comp == 1 ? p2.w : p2.y, b2 = comp == 2 ? p2.w : p2.z;
-    const float c0 = comp == 0 ? p3.w : p3.x, c1 = comp == 1 ? p3.w : p3.y, c2 = comp == 2 ? p3.w : p3.z;
-    const float d = det3f(a0, a1, a2, b0, b1, b2, c0, c1, c2);
-    cof = comp == 3 ? d : -d;
-    per = per3f(a0, a1, a2, b0, b1, b2, c0, c1, c2);
-}
-
 // Squared distance to the seed (the origin of the local frame) of a vertex given
 // in homogeneous coordinates.
 __device__ __forceinline__ float vd2_of(const float4& V) {
@@ -1433,32 +1420,15 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
                 W.P32[kp[j]] = kb[j];
                 W.D32[kp[j]] = kr[j];
             }
-        // new vertices after the kept ones: in 3D four lanes each (one cofactor and its
-        // permanent per lane, eight vertices per pass), in 2D one lane each
-        if (D == 3) {
-            for (int q0 = 0; q0 < n_new; q0 += 8) {
-                const int q = q0 + (lane >> 2), comp = lane & 3;
-                if (q < n_new) {
-                    const uint32_t tv = stage[q];
-                    float cof, per;
-                    cofactor_h32(hp, tv, comp, cof, per);
-                    reinterpret_cast<float*>(&W.V32[kept + q])[comp] = cof;
-                    reinterpret_cast<float*>(&W.P32[kept + q])[comp] = per;
-                    if (comp == 0) W.tri[kept + q] = tv;
-                }
-            }
-            __syncwarp();
-            for (int q = lane; q < n_new; q += 32) W.D32[kept + q] = vd2_of(W.V32[kept + q]);
-        } else {
-            for (int q = lane; q < n_new; q += 32) {
-                const uint32_t tv = stage[q];
-                float4 V, Pb;
-                vertex_h32<D>(hp, tv, V, Pb);
-                W.tri[kept + q] = tv;
-                W.V32[kept + q] = V;
-                W.P32[kept + q] = Pb;
-                W.D32[kept + q] = vd2_of(V);
-            }
+        // new vertices after the kept ones, one lane each
+        for (int q = lane; q < n_new; q += 32) {
+            const uint32_t tv = stage[q];
+            float4 V, Pb;
+            vertex_h32<D>(hp, tv, V, Pb);
+            W.tri[kept + q] = tv;
+            W.V32[kept + q] = V;
+            W.P32[kept + q] = Pb;
+            W.D32[kept + q] = vd2_of(V);
         }
         if (lane == 0) W.vid[cur] = (int)z;
         nb_v++;

@@ -194,13 +194,6 @@ __global__ void k_prim_dt(const double* __restrict__ mass, const double* __restr
     }
 }
 
-// a double4 read with the streaming (evict-first) cache hint, as two 16-byte loads
-__device__ __forceinline__ double4 ldcs4(const double4* p) {
-    const double2 a = __ldcs(reinterpret_cast<const double2*>(p));
-    const double2 b = __ldcs(reinterpret_cast<const double2*>(p) + 1);
-    return make_double4(a.x, a.y, b.x, b.y);
-}
-
 template <int D, bool PHYSICAL, int MIRROR>
 __global__ void k_flux_update(const double4* __restrict__ w4, const double* __restrict__ we,
                               const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fcnt,
@@ -228,10 +221,8 @@ __global__ void k_flux_update(const double4* __restrict__ w4, const double* __re
     const uint32_t fp = fptr[i], nf = alive ? fcnt[i] : 0u;
     unsigned nbox = 0, nunp = 0;
     for (uint32_t q = 0; q < nf; q++) {
-        // the cell's own face records are read once: streaming loads (evict first), so
-        // that they do not push the neighbour states out of the caches
-        const uint32_t own = __ldcs(f_own + fp + q);
-        const double4 g = ldcs4(f_geo + fp + q);
+        const uint32_t own = f_own[fp + q];
+        const double4 g = f_geo[fp + q];
         uint32_t h = (uint32_t)i;
         uint32_t code = 0;
         double A = g.w;

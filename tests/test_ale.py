@@ -20,6 +20,7 @@ from helpers import rel_err
 from proteusgpu_b200 import Context, ics
 
 K, BUFF = 16, 0.1
+AMP = 1e-6  # small enough that the wave's own steepening stays far below the schemes' errors
 
 
 def _oracle_run(ic, mode, t_end=None, steps=None, cfl=0.3, k=K, buff=BUFF):
@@ -46,14 +47,14 @@ def _oracle_run(ic, mode, t_end=None, steps=None, cfl=0.3, k=K, buff=BUFF):
 def _wave_error(ic, x, M, t):
     m = om.build_mesh(x, K, buff=BUFF, hydro_only=True, expand_k=1 << 12)
     V = m.volumes[: ic.n]
-    exact = 1.0 + 1e-3 * np.sin(2.0 * math.pi * (m.centroid[: ic.n, 0] - math.sqrt(ic.gamma) * t))
-    return float(np.sum(np.abs(M / V - exact) * V) / 1e-3)
+    exact = 1.0 + AMP * np.sin(2.0 * math.pi * (m.centroid[: ic.n, 0] - math.sqrt(ic.gamma) * t))
+    return float(np.sum(np.abs(M / V - exact) * V) / AMP)
 
 
 def test_moving_faces_converge_at_first_and_second_order():
     err = {mode: [] for mode in ("static", 1, 2)}
     for ns in (16, 32, 64):
-        ic = ics.sound_wave_2d(ns)
+        ic = ics.sound_wave_2d(ns, amp=AMP)
         for mode in err:
             _, x, M, _, _, t = _oracle_run(ic, mode, t_end=0.5)
             err[mode].append(_wave_error(ic, x, M, t))
@@ -120,7 +121,7 @@ def test_gpu_moving_faces_converge():
     """The same convergence on the device: density L1 error of the sound wave."""
     err = {}
     for ns in (32, 64, 128):
-        ic = ics.sound_wave_2d(ns)
+        ic = ics.sound_wave_2d(ns, amp=AMP)
         for flux in ("physical", "ale2"):
             with Context(dim=2, k=K, buff=BUFF, boundary="periodic", flux=flux, gamma=ic.gamma) as ctx:
                 ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy)
