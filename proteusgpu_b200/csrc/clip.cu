@@ -53,7 +53,8 @@ struct WarpCell {
         };
         struct {                     // k_clip32 while clipping
             float4 V32[MAX_T];       // homogeneous vertex coordinates (rx, ry, rz, rw)
-            float4 P32[MAX_T];       // permanents of the same minors (their rounding bounds)
+            float2 P32[MAX_T];       // bounds of their rounding: (largest permanent of the x, y, z
+                                     // cofactors' minors, permanent of the w cofactor's)
             float D32[MAX_T];        // squared distance of the vertex to the seed
         };
     };
@@ -1102,7 +1103,8 @@ __global__ void __launch_bounds__(CLIP_WARPS * 32)
 // in single precision in a frame centred on its seed: a neighbour b = B - seed
 // gives the plane (-b, |b|^2 / 2), the box planes get w + n.seed.  Every
 // plane-vertex determinant is accepted only when it exceeds a bound on its
-// rounding error, 64 u times the permanent of the absolute entries (u = 2^-24);
+// rounding error, 64 u times an upper bound of the permanent of the absolute
+// entries (u = 2^-24);
 // otherwise, and on any overflow or inconsistent cavity, the cell is handed to
 // the FP64 kernel (status ST_RECLIP).  Certified cells are extracted in FP64:
 // the plane equations are recomputed from the points with the reference's
@@ -1136,10 +1138,13 @@ __device__ __forceinline__ float per3f(float a11, float a12, float a13, float a2
 // Homogeneous coordinates of a vertex in the local frame -- the cofactors of the
 // plane-vertex determinant: det4(p1, p2, p3, e) = e . V (and det3 in 2D) -- and
 // the permanents of the same minors, which bound their rounding errors.  The
-// entries of a plane differ in scale (normal ~ h, offset ~ h^2), so each
-// cofactor keeps its own bound: |e| . P is the permanent of the full matrix.
+// entries of a plane differ in scale (normal ~ h, offset ~ h^2), so the offset's
+// cofactor keeps its own permanent and the three normal cofactors share their
+// largest: (|e.x| + |e.y| + |e.z|) P_xyz + |e.w| P_w bounds the permanent of the
+// full matrix (8 bytes a vertex instead of 16, for 28 warps per SM).
 template <int D>
-__device__ __forceinline__ void vertex_h32(const float4* hp, uint32_t t, float4& V, float4& Pb) {
+__device__ __forceinline__ void vertex_h32(const float4* hp, uint32_t t, float4& V, float2& Pb2) {
+    float4 Pb;
     const float4 p1 = hp[tri_a(t)], p2 = hp[tri_b(t)];
     if (D == 2) {
         V.x = -det2f(p1.w, p1.y, p2.w, p2.y);
@@ -1148,6 +1153,7 @@ __device__ __forceinline__ void vertex_h32(const float4* hp, uint32_t t, float4&
         V.w = det2f(p1.x, p1.y, p2.x, p2.y);
         Pb = make_float4(per2f(p1.w, p1.y, p2.w, p2.y), per2f(p1.x, p1.w, p2.x, p2.w), 0.0f,
                          per2f(p1.x, p1.y, p2.x, p2.y));
+        Pb2 = make_float2(fmaxf(Pb.x, Pb.y), Pb.w);
         return;
     }
     const float4 p3 = hp[tri_c(t)];
@@ -1159,6 +1165,7 @@ __device__ __forceinline__ void vertex_h32(const float4* hp, uint32_t t, float4&
                      per3f(p1.x, p1.w, p1.z, p2.x, p2.w, p2.z, p3.x, p3.w, p3.z),
                      per3f(p1.x, p1.y, p1.w, p2.x, p2.y, p2.w, p3.x, p3.y, p3.w),
                      per3f(p1.x, p1.y, p1.z, p2.x, p2.y, p2.z, p3.x, p3.y, p3.z));
+    Pb2 = make_float2(fmaxf(fmaxf(Pb.x, Pb.y), Pb.z), Pb.w);
 }
 
 // Squared distance to the seed (the origin of the local frame) of a vertex given
@@ -1172,9 +1179,10 @@ __device__ __forceinline__ float vd2_of(const float4& V) {
 // 1 = in conflict, 2 = undecided in FP32.  The bound covers the cofactors'
 // rounding, the dot product's and the planes' own entry errors (all first order
 // in the permanent |e| . P).
-__device__ __forceinline__ int conflict_h32(const float4& V, const float4& P, const float4& e) {
+__device__ __forceinline__ int conflict_h32(const float4& V, const float2& P, const float4& e) {
     const float t = fmaf(e.w, V.w, fmaf(e.z, V.z, fmaf(e.y, V.y, e.x * V.x)));
-    const float per = fmaf(fabsf(e.w), P.w, fmaf(fabsf(e.z), P.z, fmaf(fabsf(e.y), P.y, fabsf(e.x) * P.x)));
+    // |e.x| P.x + |e.y| P.y + |e.z| P.z + |e.w| P.w <= (|e.x| + |e.y| + |e.z|) max(P.x, P.y, P.z) + |e.w| P.w
+    const float per = fmaf(fabsf(e.w), P.y, (fabsf(e.x) + fabsf(e.y) + fabsf(e.z)) * P.x);
     if (!(fabsf(t) > F32_BOUND * per)) return 2;
     return t > 0.0f ? 1 : 0;
 }
@@ -1216,8 +1224,9 @@ __device__ __forceinline__ double4 plane64(int p, int vid, const typename PointO
     return make_double4(dx, dy, dz, -dot / 2.0);
 }
 
+// 28 warps per SM: 72 registers a thread and ~7.8 KB of shared memory a warp
 template <int D, int CW>
-__global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
+__global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
     using PT = typename PointOf<D>::type;
     __shared__ WarpCell cells[CW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -1393,7 +1402,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
         }
         uint32_t kt[3];
         float4 kd[3];
-        float4 kb[3];
+        float2 kb[3];
         float kr[3];
         int kp[3];
         int before = 0;
@@ -1406,7 +1415,7 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
             const bool keep = (kmj >> lane) & 1u;
             kt[j] = keep ? W.tri[i] : 0u;
             kd[j] = keep ? W.V32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            kb[j] = keep ? W.P32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            kb[j] = keep ? W.P32[i] : make_float2(0.f, 0.f);
             kr[j] = keep ? W.D32[i] : 0.0f;
             kp[j] = keep ? before + __popc(kmj & ((1u << lane) - 1u)) : -1;
             before += __popc(kmj);
@@ -1423,7 +1432,8 @@ __global__ void __launch_bounds__(CW * 32) k_clip32(ClipParams P) {
         // new vertices after the kept ones, one lane each
         for (int q = lane; q < n_new; q += 32) {
             const uint32_t tv = stage[q];
-            float4 V, Pb;
+            float4 V;
+            float2 Pb;
             vertex_h32<D>(hp, tv, V, Pb);
             W.tri[kept + q] = tv;
             W.V32[kept + q] = V;

@@ -258,8 +258,10 @@ __device__ __forceinline__ bool box_range(const SubGrid& g, uint32_t slot0, int 
     return true;
 }
 
+// 32 warps per SM: at most 64 registers a thread (the search is latency bound on its
+// warp-collective chains; more resident warps hide more of them)
 template <int D, int KW>
-__global__ void __launch_bounds__(KW * 32)
+__global__ void __launch_bounds__(KW * 32, 32 / KW)
     k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
           const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
           int K, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
