@@ -54,15 +54,18 @@ CONFIGS = {
 }
 
 # Algorithmic work per unit, counted with the oracle's
-# instrumented restatement of the reference's search and clipping on the same
-# distributions (3D uniform K=190; 2D jittered lattice K=16).
-#   KNN: candidates per query x flops per squared distance (3D: 8, 2D: 5)
+# instrumented restatement of the reference's search and clipping on the workloads'
+# distributions: 3D clustered (100,000 cells of the 1,048,576-point clustered set, K=190
+# lists), 3D uniform (K=190), 2D jittered lattice (K=16).
+#   KNN: candidates per query x flops per squared distance (3D: 8, 2D: 5); the bench
+#        uses the candidates the run itself evaluated (the learned budgets' own search)
 #   clip: predicates per cell x 45 (det4x4) + vertices created per cell x 59   (3D)
 #         predicates per cell x 14 (det3x3) + vertices created per cell x 11   (2D)
 #   hydro (flux+update+drift): compulsory HBM bytes per cell-update
 WORK = {
-    3: dict(knn_flop_per_query=969.6 * 8, clip_flop_per_cell=924.7 * 45 + 70.8 * 59, hydro_bytes_per_cell=683),
-    2: dict(knn_flop_per_query=73.5 * 5, clip_flop_per_cell=34.3 * 14 + 12.0 * 11, hydro_bytes_per_cell=272),
+    (3, "clustered"): dict(knn_flop_per_cand=8, clip_flop_per_cell=1118.5 * 45 + 71.0 * 59, hydro_bytes_per_cell=683),
+    (3, "uniform"): dict(knn_flop_per_cand=8, clip_flop_per_cell=924.7 * 45 + 70.8 * 59, hydro_bytes_per_cell=683),
+    (2, "uniform"): dict(knn_flop_per_cand=5, clip_flop_per_cell=34.3 * 14 + 12.0 * 11, hydro_bytes_per_cell=272),
 }
 STAGES = ["ghosts", "sort", "knn", "clip", "hydro"]
 
@@ -540,7 +543,7 @@ def run_ours(args, rank, world, local_rank):
 
     # roofline of the headline's dominant stage
     D = cfg["dim"]
-    W = WORK[D]
+    W = WORK[(D, "clustered" if cfg.get("ic") == "clustered" else "uniform")]
     stage, stats = head["stage"], head["stats"]
     dom = STAGES[int(np.argmax(stage))]
     fp64, fp32 = ctypes.c_double(), ctypes.c_double()
@@ -549,27 +552,30 @@ def run_ours(args, rank, world, local_rank):
     L.pgpu_fp32_peak(local_rank, ctypes.c_float(200.0), ctypes.byref(fp32))
     hbm, hbm_src = measured_peaks()
     n_query = stats["n_hydro"]
-    if dom == "clip":
-        peak = fp32.value
-        # the main clip pass (k_clip32 and the FP64 re-clip of its undecided cells), timed
-        # by CUDA events on the context's stream; the fallback and the grid walk excluded
-        main_ms = stats["clip_split_ms"][0] or stage[3]
-        ach = n_query * W["clip_flop_per_cell"] / (main_ms * 1e-3) / 1e12
-        roof = {"kernel": "k_clip32 (+ FP64 re-clip of undecided cells)", "bound": "fp32", "achieved": ach,
-                "peak": peak, "unit": "TFLOP/s", "frac": ach / peak,
-                "traffic": CLIP32_DRAM_BYTES_PER_CELL * n_query if D == 3 else None,
-                "traffic_note": "DRAM bytes per launch: ncu capture of the clustered 1,048,576-cell case "
-                                "(learned-K lists) scaled by cells",
-                "timed": "main clip pass (CUDA events): k_clip32 + FP64 re-clip",
-                "peak_source": "FP32 FMA rate measured in this run (pgpu_fp32_peak)",
-                "work": f"{W['clip_flop_per_cell']:.0f} algorithmic flop per cell x {n_query} cells"}
-    elif dom == "knn":
-        peak = fp64.value
-        ach = n_query * W["knn_flop_per_query"] / (stage[2] * 1e-3) / 1e12
-        roof = {"kernel": "k_knn", "bound": "fp64", "achieved": ach, "peak": peak, "unit": "TFLOP/s",
-                "frac": ach / peak, "traffic": None,
+    # the main clip pass (k_clip32 and the FP64 re-clip of its undecided cells), timed by
+    # CUDA events on the context's stream; the fallback and the grid walk excluded
+    main_ms = stats["clip_split_ms"][0] or stage[3]
+    ach = n_query * W["clip_flop_per_cell"] / (main_ms * 1e-3) / 1e12
+    roof_clip = {"kernel": "k_clip32 (+ FP64 re-clip of undecided cells)", "bound": "fp32", "achieved": ach,
+                 "peak": fp32.value, "unit": "TFLOP/s", "frac": ach / fp32.value,
+                 "traffic": CLIP32_DRAM_BYTES_PER_CELL * n_query if D == 3 else None,
+                 "traffic_note": "DRAM bytes per launch: ncu capture of the clustered 1,048,576-cell case "
+                                 "(learned-K lists) scaled by cells",
+                 "timed": "main clip pass (CUDA events): k_clip32 + FP64 re-clip",
+                 "peak_source": "FP32 FMA rate measured in this run (pgpu_fp32_peak)",
+                 "work": f"{W['clip_flop_per_cell']:.0f} algorithmic flop per cell (the oracle's count on this "
+                         f"distribution) x {n_query} cells"}
+    cand = stats["knn_candidates"] / max(n_query, 1)
+    ach = n_query * cand * W["knn_flop_per_cand"] / (stage[2] * 1e-3) / 1e12
+    roof_knn = {"kernel": "k_knn", "bound": "fp64", "achieved": ach, "peak": fp64.value, "unit": "TFLOP/s",
+                "frac": ach / fp64.value, "traffic": None,
                 "peak_source": "FP64 FMA rate measured in this run (pgpu_fp64_peak)",
-                "work": f"{W['knn_flop_per_query']:.0f} algorithmic flop per query x {n_query} queries"}
+                "work": f"{cand:.1f} candidates per query (this run's) x {W['knn_flop_per_cand']} flop x "
+                        f"{n_query} queries"}
+    if dom == "clip":
+        roof = roof_clip
+    elif dom == "knn":
+        roof = roof_knn
     else:
         ach = n_query * W["hydro_bytes_per_cell"] / (stage[STAGES.index(dom)] * 1e-3) / 1e9
         roof = {"kernel": dom, "bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
@@ -603,7 +609,7 @@ def run_ours(args, rank, world, local_rank):
         # the oracle's checks: sampled cells of the full-size meshes, and the density error of a
         # whole run against the oracle's own run (oracle/check.py; outside the timed region)
         "oracle_check": oracle_check,
-        "roofline": roof, "roofline_hydro": roof_hydro,
+        "roofline": roof, "roofline_knn": roof_knn if dom != "knn" else None, "roofline_hydro": roof_hydro,
         "stages_ms": dict(zip(STAGES, stage)),
         "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": head["launches"], "forms": forms,
         "clocks": head["clocks"],
