@@ -31,6 +31,8 @@
 // atomic add; placement varies run to run, contents do not.
 #include <math_constants.h>
 
+#include <type_traits>
+
 #include "pgpu_common.cuh"
 #include "pgpu_ctx.h"
 
@@ -69,6 +71,60 @@ struct WarpCell {
         double vpos[MAX_T][3];
     } u;
 };
+
+// k_clip32's cell in 3D: the FP32 clipping arrays and the FP64 extraction arrays share
+// memory (clipping is over when extraction begins): 6.9 KB a warp instead of 7.9 KB,
+// for 32 resident warps per SM.
+struct WarpCell32 {
+    int vid[MAX_P];
+    uint32_t tri[MAX_T];
+    union {
+        struct {  // FP32 clipping
+            float4 hp32[MAX_P];
+            float4 V32[MAX_T];
+            float2 P32[MAX_T];
+            float D32[MAX_T];
+            unsigned long long emask[MAX_P];
+            uint32_t stage[MAX_P];
+            uint32_t rl[MAX_T];
+            unsigned char nxt[MAX_P];
+        } c;
+        struct {  // FP64 extraction
+            double4 hp[MAX_P];
+            double vpos[MAX_T][3];
+            double fvol[MAX_P];
+            double fcen[MAX_P][3];
+        } x;
+    };
+};
+
+// Member access shared by the kernels' two cell layouts.
+__device__ __forceinline__ double4* hp_of(WarpCell& W) { return W.hp; }
+__device__ __forceinline__ double4* hp_of(WarpCell32& W) { return W.x.hp; }
+__device__ __forceinline__ double (*vpos_of(WarpCell& W))[3] { return W.u.vpos; }
+__device__ __forceinline__ double (*vpos_of(WarpCell32& W))[3] { return W.x.vpos; }
+__device__ __forceinline__ uint32_t* rl_of(WarpCell& W) { return reinterpret_cast<uint32_t*>(W.u.b.stage_d2); }
+__device__ __forceinline__ uint32_t* rl_of(WarpCell32& W) { return W.c.rl; }
+__device__ __forceinline__ uint32_t* stage_of(WarpCell& W) { return W.u.b.stage; }
+__device__ __forceinline__ uint32_t* stage_of(WarpCell32& W) { return W.c.stage; }
+__device__ __forceinline__ unsigned long long* emask_of(WarpCell& W) { return W.u.b.emask; }
+__device__ __forceinline__ unsigned long long* emask_of(WarpCell32& W) { return W.c.emask; }
+__device__ __forceinline__ unsigned char* nxt_of(WarpCell& W) { return W.u.b.nxt; }
+__device__ __forceinline__ unsigned char* nxt_of(WarpCell32& W) { return W.c.nxt; }
+__device__ __forceinline__ double* fvol_of(WarpCell& W) { return W.fvol; }
+__device__ __forceinline__ double* fvol_of(WarpCell32& W) { return W.x.fvol; }
+__device__ __forceinline__ double (*fcen_of(WarpCell& W))[3] { return W.fcen; }
+__device__ __forceinline__ double (*fcen_of(WarpCell32& W))[3] { return W.x.fcen; }
+__device__ __forceinline__ float4* hp32_of(WarpCell& W) { return W.u.b.hp32; }
+__device__ __forceinline__ float4* hp32_of(WarpCell32& W) { return W.c.hp32; }
+__device__ __forceinline__ float4* V32_of(WarpCell& W) { return W.V32; }
+__device__ __forceinline__ float4* V32_of(WarpCell32& W) { return W.c.V32; }
+__device__ __forceinline__ float2* P32_of(WarpCell& W) { return W.P32; }
+__device__ __forceinline__ float2* P32_of(WarpCell32& W) { return W.c.P32; }
+__device__ __forceinline__ float* D32_of(WarpCell& W) { return W.D32; }
+__device__ __forceinline__ float* D32_of(WarpCell32& W) { return W.c.D32; }
+__device__ __forceinline__ const float* D32_of(const WarpCell& W) { return W.D32; }
+__device__ __forceinline__ const float* D32_of(const WarpCell32& W) { return W.c.D32; }
 
 __device__ __forceinline__ uint32_t tri_a(uint32_t t) { return t & 255u; }
 __device__ __forceinline__ uint32_t tri_b(uint32_t t) { return (t >> 8) & 255u; }
@@ -215,30 +271,32 @@ __device__ __forceinline__ void store_failed(const ClipParams& P, int lane, uint
 // Extraction (cell.cpp:416-669) of a certified cell held in W with FP64 planes:
 // vertices, faces in plane order, areas, volume, centroid; faces written at a
 // reserved slot, cell outputs at extended id e.
-template <int D>
-__device__ __forceinline__ void compute_vpos(WarpCell& W, int lane, int nb_t) {
+template <int D, class Cell>
+__device__ __forceinline__ void compute_vpos(Cell& W, int lane, int nb_t) {
     __syncwarp();
+    double (*vp)[3] = vpos_of(W);
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         int i = lane + 32 * j;
-        if (i < nb_t) vertex_pos<D>(W.hp, W.tri[i], W.u.vpos[i][0], W.u.vpos[i][1], W.u.vpos[i][2]);
+        if (i < nb_t) vertex_pos<D>(hp_of(W), W.tri[i], vp[i][0], vp[i][1], vp[i][2]);
     }
     __syncwarp();
 }
 
-template <int D>
-__device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams& P, int w, int lane, int nb_v, int nb_t,
+template <int D, class Cell>
+__device__ __forceinline__ void extract_and_store(Cell& W, const ClipParams& P, int w, int lane, int nb_v, int nb_t,
                                                   uint32_t e, int certk, double sx, double sy, double sz,
                                                   bool vpos_ready = false, double ox = 0.0, double oy = 0.0,
                                                   double oz = 0.0) {
     // (ox, oy, oz): origin of the frame the cell was clipped in, added to the centroid
     if (!vpos_ready) compute_vpos<D>(W, lane, nb_t);
+    double (*vp)[3] = vpos_of(W);
 
     double cell_vol = 0.0, cen[3] = {0.0, 0.0, 0.0};
-    if (D == 2) {
+    if constexpr (D == 2) {
         // compute_cell_area_2d (cell.cpp:475-498): vertices ordered by angle about their mean
         double cx = 0, cy = 0;
-        for (int i = 0; i < nb_t; i++) cx += W.u.vpos[i][0], cy += W.u.vpos[i][1];
+        for (int i = 0; i < nb_t; i++) cx += vp[i][0], cy += vp[i][1];
         cx /= nb_t;
         cy /= nb_t;
         // rank of each vertex by angle; lane-parallel, then lane 0 sums in order
@@ -246,7 +304,7 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
 #pragma unroll
         for (int j = 0; j < 3; j++) {
             int i = lane + 32 * j;
-            if (i < nb_t) W.vd2[i] = atan2(W.u.vpos[i][1] - cy, W.u.vpos[i][0] - cx);
+            if (i < nb_t) W.vd2[i] = atan2(vp[i][1] - cy, vp[i][0] - cx);
         }
         __syncwarp();
 #pragma unroll
@@ -267,8 +325,8 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
             double a = 0, mx = 0, my = 0, sa = 0;
             for (int i = 0; i < nb_t; i++) {
                 int j = (i + 1) % nb_t;
-                const double* pp = W.u.vpos[order_s[w][i]];
-                const double* qq = W.u.vpos[order_s[w][j]];
+                const double* pp = vp[order_s[w][i]];
+                const double* qq = vp[order_s[w][j]];
                 a += pp[0] * qq[1];
                 a -= qq[0] * pp[1];
                 double cr = (pp[0] - cx) * (qq[1] - cy) - (qq[0] - cx) * (pp[1] - cy);
@@ -285,6 +343,8 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
     // faces: lane handles planes p = lane and p = lane + 32
     bool valid[2] = {false, false};
     double area[2] = {0.0, 0.0};
+    double* fvol = fvol_of(W);
+    double (*fcen)[3] = fcen_of(W);
 #pragma unroll
     for (int pass = 0; pass < 2; pass++) {
         const int p = lane + 32 * pass;
@@ -299,8 +359,8 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
                 }
             }
             if (cnt >= 2) {
-                double ddx = W.u.vpos[v1][0] - W.u.vpos[v0][0];
-                double ddy = W.u.vpos[v1][1] - W.u.vpos[v0][1];
+                double ddx = vp[v1][0] - vp[v0][0];
+                double ddy = vp[v1][1] - vp[v0][1];
                 area[pass] = sqrt(ddx * ddx + ddy * ddy);
                 valid[pass] = true;
             }
@@ -330,7 +390,7 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
                 // Walk the polygon: after vertex (p, a, b) comes (p, b, c).  Fan
                 // triangles (v0, v_{i-1}, v_i) give the area and, with the seed,
                 // the signed volume and first moment (cell.cpp:611-627).
-                const double* v0 = W.u.vpos[fi[0]];
+                const double* v0 = vp[fi[0]];
                 const double a0 = v0[0] - sx, a1 = v0[1] - sy, a2 = v0[2] - sz;
                 int curv = 0;
                 double meas = 0.0;
@@ -347,8 +407,8 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
                         break;
                     }
                     if (st >= 2) {
-                        const double* vi = W.u.vpos[fi[curv]];
-                        const double* vj = W.u.vpos[fi[nx]];
+                        const double* vi = vp[fi[curv]];
+                        const double* vj = vp[fi[nx]];
                         double e1x = vi[0] - v0[0], e1y = vi[1] - v0[1], e1z = vi[2] - v0[2];
                         double e2x = vj[0] - v0[0], e2y = vj[1] - v0[1], e2z = vj[2] - v0[2];
                         double crx = e1y * e2z - e1z * e2y;
@@ -374,10 +434,10 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
                     area[pass] = meas;
                 }
             }
-            W.fvol[p] = valid[pass] ? fv : 0.0;
-            W.fcen[p][0] = valid[pass] ? fc0 : 0.0;
-            W.fcen[p][1] = valid[pass] ? fc1 : 0.0;
-            W.fcen[p][2] = valid[pass] ? fc2 : 0.0;
+            fvol[p] = valid[pass] ? fv : 0.0;
+            fcen[p][0] = valid[pass] ? fc0 : 0.0;
+            fcen[p][1] = valid[pass] ? fc1 : 0.0;
+            fcen[p][2] = valid[pass] ? fc2 : 0.0;
         }
     }
     const uint32_t vb0 = __ballot_sync(FULL, valid[0]);
@@ -386,10 +446,10 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
     __syncwarp();
     if (D == 3 && lane == 0) {
         for (int p = 0; p < nb_v; p++) {  // plane order, as the reference accumulates
-            cell_vol += W.fvol[p];
-            cen[0] += W.fcen[p][0];
-            cen[1] += W.fcen[p][1];
-            cen[2] += W.fcen[p][2];
+            cell_vol += fvol[p];
+            cen[0] += fcen[p][0];
+            cen[1] += fcen[p][1];
+            cen[2] += fcen[p][2];
         }
         const double sv = cell_vol;
         cell_vol = fabs(sv);
@@ -415,7 +475,7 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
             const uint32_t vb = pass == 0 ? vb0 : vb1;
             const int idx = (pass == 0 ? 0 : __popc(vb0)) + __popc(vb & ((1u << lane) - 1u));
             const size_t f = base + idx;
-            const double4 pe = W.hp[p];
+            const double4 pe = hp_of(W)[p];
             const double nlen = sqrt(pe.x * pe.x + pe.y * pe.y + pe.z * pe.z);  // compute_face_normal
             const int nbr = W.vid[p];
             P.f_nb[f] = nbr;
@@ -451,12 +511,12 @@ __device__ __forceinline__ void extract_and_store(WarpCell& W, const ClipParams&
 // else the directed edges are marked in the per-plane rows of emask.  Returns the
 // number of new vertices; src gets the OR of their first planes and, with
 // WANT_NXT, nxt[x] = y (for the FP64 kernel's cycle check).
-template <bool WANT_NXT>
-__device__ __forceinline__ int cavity_boundary3(WarpCell& W, int lane, const uint32_t (&cm)[3], int nb_t, int nb_r,
+template <bool WANT_NXT, class Cell>
+__device__ __forceinline__ int cavity_boundary3(Cell& W, int lane, const uint32_t (&cm)[3], int nb_t, int nb_r,
                                                 uint32_t cur, unsigned long long& src) {
-    uint32_t* rl = reinterpret_cast<uint32_t*>(W.u.b.stage_d2);  // removed triangles (scratch: MAX_T u32)
-    uint32_t* stage = W.u.b.stage;
-    unsigned long long* em = W.u.b.emask;
+    uint32_t* rl = rl_of(W);  // removed triangles (scratch: MAX_T u32)
+    uint32_t* stage = stage_of(W);
+    unsigned long long* em = emask_of(W);
     int before = 0;
 #pragma unroll
     for (int j = 0; j < 3; j++) {
@@ -502,7 +562,7 @@ __device__ __forceinline__ int cavity_boundary3(WarpCell& W, int lane, const uin
             const int pos = base + __popc(bal & ((1u << lane) - 1u));
             if (pos < MAX_P) stage[pos] = pack3(cur, x, y);
             if (x < 32u) slo |= 1u << x; else shi |= 1u << (x - 32u);
-            if (WANT_NXT) W.u.b.nxt[x] = (unsigned char)y;
+            if (WANT_NXT) nxt_of(W)[x] = (unsigned char)y;
         }
         base += __popc(bal);
     }
@@ -1190,12 +1250,14 @@ __device__ __forceinline__ int conflict_h32(const float4& V, const float2& P, co
 // The squared distances are >= +0 or NaN, so their bit patterns order as unsigned
 // integers (any NaN above every number): one integer max-reduction gives the
 // maximum, NaN when any is NaN.
-__device__ __forceinline__ float max_vd2f(const WarpCell& W, int n, int lane) {
+template <class Cell>
+__device__ __forceinline__ float max_vd2f(const Cell& W, int n, int lane) {
     uint32_t m = 0u;
+    const float* d32 = D32_of(W);
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         const int i = lane + 32 * j;
-        if (i < n) m = max(m, __float_as_uint(W.D32[i]));
+        if (i < n) m = max(m, __float_as_uint(d32[i]));
     }
     return __uint_as_float(__reduce_max_sync(FULL, m));
 }
@@ -1224,16 +1286,21 @@ __device__ __forceinline__ double4 plane64(int p, int vid, const typename PointO
     return make_double4(dx, dy, dz, -dot / 2.0);
 }
 
-// 28 warps per SM: 72 registers a thread and ~7.8 KB of shared memory a warp
+// Resident warps per SM: 32 in 3D (64 registers a thread, 6.9 KB of shared memory a
+// warp: the overlaid cell), 28 in 2D (72 registers, 7.8 KB).
 template <int D, int CW>
-__global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
+__global__ void __launch_bounds__(CW * 32, (D == 3 ? 32 : 28) / CW) k_clip32(ClipParams P) {
     using PT = typename PointOf<D>::type;
-    __shared__ WarpCell cells[CW];
+    using Cell = typename std::conditional<D == 3, WarpCell32, WarpCell>::type;
+    __shared__ Cell cells[CW];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t t = (int64_t)blockIdx.x * CW + w;
     if (t >= P.nq) return;  // warp-uniform
-    WarpCell& W = cells[w];
-    float4* hp = W.u.b.hp32;
+    Cell& W = cells[w];
+    float4* hp = hp32_of(W);
+    float4* V32 = V32_of(W);
+    float2* P32 = P32_of(W);
+    float* D32 = D32_of(W);
     const PT* spts = (const PT*)P.spts;
     const PT* ext = (const PT*)P.ext;
     const int64_t tq = P.slots ? (int64_t)P.slots[t] : t;
@@ -1261,8 +1328,8 @@ __global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
         W.vid[lane] = -1;
     }
     if (D == 3) {
-        W.u.b.emask[lane] = 0ull;
-        W.u.b.emask[lane + 32] = 0ull;
+        emask_of(W)[lane] = 0ull;
+        emask_of(W)[lane + 32] = 0ull;
     }
     const int ntri0 = D == 2 ? 4 : 8;
     if (lane < ntri0) {
@@ -1279,8 +1346,8 @@ __global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
     }
     __syncwarp();
     if (lane < ntri0) {
-        vertex_h32<D>(hp, W.tri[lane], W.V32[lane], W.P32[lane]);
-        W.D32[lane] = vd2_of(W.V32[lane]);
+        vertex_h32<D>(hp, W.tri[lane], V32[lane], P32[lane]);
+        D32[lane] = vd2_of(V32[lane]);
     }
     __syncwarp();
     int nb_v = 2 * D, nb_t = ntri0;
@@ -1327,7 +1394,7 @@ __global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
             const int i = lane + 32 * j;
             bool cf = false;
             if (i < nb_t) {
-                const int c = conflict_h32(W.V32[i], W.P32[i], eq);
+                const int c = conflict_h32(V32[i], P32[i], eq);
                 undecided |= c == 2;
                 cf = c == 1;
             }
@@ -1350,7 +1417,7 @@ __global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
         const int kept = nb_t - nb_r;
         int n_new = 0;
         bool bad = false;
-        uint32_t* stage = W.u.b.stage;  // new vertices, written at their final position
+        uint32_t* stage = stage_of(W);  // new vertices, written at their final position
         if (D == 2) {
             uint32_t lo = 0, hi = 0;
 #pragma unroll
@@ -1414,9 +1481,9 @@ __global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
             const uint32_t kmj = km[j] & vm;
             const bool keep = (kmj >> lane) & 1u;
             kt[j] = keep ? W.tri[i] : 0u;
-            kd[j] = keep ? W.V32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-            kb[j] = keep ? W.P32[i] : make_float2(0.f, 0.f);
-            kr[j] = keep ? W.D32[i] : 0.0f;
+            kd[j] = keep ? V32[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+            kb[j] = keep ? P32[i] : make_float2(0.f, 0.f);
+            kr[j] = keep ? D32[i] : 0.0f;
             kp[j] = keep ? before + __popc(kmj & ((1u << lane) - 1u)) : -1;
             before += __popc(kmj);
         }
@@ -1425,9 +1492,9 @@ __global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
         for (int j = 0; j < 3; j++)
             if (kp[j] >= 0) {
                 W.tri[kp[j]] = kt[j];
-                W.V32[kp[j]] = kd[j];
-                W.P32[kp[j]] = kb[j];
-                W.D32[kp[j]] = kr[j];
+                V32[kp[j]] = kd[j];
+                P32[kp[j]] = kb[j];
+                D32[kp[j]] = kr[j];
             }
         // new vertices after the kept ones, one lane each
         for (int q = lane; q < n_new; q += 32) {
@@ -1436,9 +1503,9 @@ __global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
             float2 Pb;
             vertex_h32<D>(hp, tv, V, Pb);
             W.tri[kept + q] = tv;
-            W.V32[kept + q] = V;
-            W.P32[kept + q] = Pb;
-            W.D32[kept + q] = vd2_of(V);
+            V32[kept + q] = V;
+            P32[kept + q] = Pb;
+            D32[kept + q] = vd2_of(V);
         }
         if (lane == 0) W.vid[cur] = (int)z;
         nb_v++;
@@ -1462,14 +1529,14 @@ __global__ void __launch_bounds__(CW * 32, 28 / CW) k_clip32(ClipParams P) {
 #pragma unroll
     for (int pass = 0; pass < 2; pass++) {
         const int p = lane + 32 * pass;
-        if (p < nb_v) W.hp[p] = plane64<D>(p, W.vid[p], ext, sx, sy, sz);
+        if (p < nb_v) hp_of(W)[p] = plane64<D>(p, W.vid[p], ext, sx, sy, sz);
     }
     compute_vpos<D>(W, lane, nb_t);
     double vm64 = 0.0;
 #pragma unroll
     for (int j = 0; j < 3; j++) {
         const int i = lane + 32 * j;
-        if (i < nb_t) vm64 = nan_max(vm64, seed_d2(W.u.vpos[i][0], W.u.vpos[i][1], W.u.vpos[i][2], sx, sy, sz));
+        if (i < nb_t) vm64 = nan_max(vm64, seed_d2(vpos_of(W)[i][0], vpos_of(W)[i][1], vpos_of(W)[i][2], sx, sy, sz));
     }
     vm64 = warp_max(vm64);
     // first k >= k_last (1-based) whose neighbour lies beyond twice the farthest vertex
