@@ -243,6 +243,10 @@ void pgpu_destroy(pgpu_ctx* c) {
     for (DevBuf* b : bufs) free_buf(*b);
     for (int i = 0; i < 9; i++)
         if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
+    for (int i = 0; i < 2; i++)
+        if (c->copy_ev[i]) cudaEventDestroy(c->copy_ev[i]);
+    if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }
@@ -851,6 +855,10 @@ int pgpu_sim_step(pgpu_ctx* c, double cfl, double fixed_dt, double* dt_out) {
     if (r) return r;
     if (!c->have_sim) return fail(c, PGPU_ESTATE, "pgpu_sim_step: call pgpu_sim_init first");
     if ((r = build_mesh(c, c->n_hydro, false, false))) return r;
+    if (c->copy_pending) {  // the conserved state uploaded beside the mesh build
+        CK(cudaStreamWaitEvent(c->stream, c->copy_ev[1], 0));
+        c->copy_pending = false;
+    }
     CK(pgpu::launch_prim_dt(c, cfl, fixed_dt));
     CK(pgpu::launch_flux_update(c, fixed_dt));
     mark(c, 5);
@@ -895,9 +903,32 @@ int pgpu_sim_get(pgpu_ctx* c, double* pos, double* mass, double* mom, double* en
 
 int pgpu_sim_step_host(pgpu_ctx* c, double cfl, double fixed_dt, double* pos, double* mass, double* mom,
                        double* energy, double* dt_out) {
-    int r = pgpu_sim_set(c, pos, mass, mom, energy);
+    int r = check_ctx(c);
     if (r) return r;
-    if ((r = pgpu_sim_step(c, cfl, fixed_dt, nullptr))) return r;
+    if (!c->have_sim) return fail(c, PGPU_ESTATE, "pgpu_sim_step_host: call pgpu_sim_init first");
+    // the positions go first (the mesh is built from them); the conserved state is read only
+    // once the mesh is built, so it is uploaded on a second stream meanwhile
+    c->copy_pending = false;
+    if (!c->copy_stream) {
+        CK(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+        for (int i = 0; i < 2; i++) CK(cudaEventCreateWithFlags(&c->copy_ev[i], cudaEventDisableTiming));
+    }
+    if ((r = pgpu_sim_set(c, pos, nullptr, nullptr, nullptr))) return r;
+    const int64_t n = c->n_hydro;
+    const int D = c->prm.dim;
+    CK(cudaEventRecord(c->copy_ev[0], c->stream));
+    CK(cudaStreamWaitEvent(c->copy_stream, c->copy_ev[0], 0));
+    if (mass) CK(cudaMemcpyAsync(c->mass.p, mass, n * sizeof(double), cudaMemcpyHostToDevice, c->copy_stream));
+    if (mom) CK(cudaMemcpyAsync(c->mom.p, mom, n * D * sizeof(double), cudaMemcpyHostToDevice, c->copy_stream));
+    if (energy) CK(cudaMemcpyAsync(c->en.p, energy, n * sizeof(double), cudaMemcpyHostToDevice, c->copy_stream));
+    CK(cudaEventRecord(c->copy_ev[1], c->copy_stream));
+    c->copy_pending = true;
+    r = pgpu_sim_step(c, cfl, fixed_dt, nullptr);
+    if (c->copy_pending) {  // the step ended before it used the state: let the upload finish
+        cudaStreamSynchronize(c->copy_stream);
+        c->copy_pending = false;
+    }
+    if (r) return r;
     if ((r = pgpu_sim_get(c, pos, mass, mom, energy))) return r;
     if (dt_out) {
         unsigned long long bits = 0;

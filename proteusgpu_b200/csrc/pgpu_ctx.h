@@ -119,6 +119,9 @@ struct KBudget {
 struct pgpu_ctx {
     pgpu_params prm{};
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_stream = nullptr;  // pgpu_sim_step_host: the conserved state's upload
+    cudaEvent_t copy_ev[2] = {};          // the main stream's entry point; the upload's end
+    bool copy_pending = false;            // the step must wait for copy_ev[1] before using the state
     std::string err;
     bool timing = false;
     cudaEvent_t ev[9] = {};    // 0-5: stage boundaries; 6-8: after the main clip, the fallback, the walk

@@ -83,3 +83,23 @@ def test_fallback_budget_matches_oracle():
     assert s1["refit_cells"] > 0
     assert rel_err(dg, do) <= 1e-12 and np.abs(xg - xo).max() <= 1e-13
     assert rel_err(mg, mo) <= 1e-10 and rel_err(eg, eo) <= 1e-10
+
+
+def test_step_host_equals_device_step():
+    """pgpu_sim_step_host (state in host memory, the conserved state uploaded beside the mesh
+    build) gives the same states as pgpu_sim_step on a device-resident state."""
+    torch = pytest.importorskip("torch")
+    ic = ics.sedov_3d(n=30000, seed=9)
+    out = []
+    for host in (False, True):
+        with Context(dim=3, k=190, buff=0.1, flux="physical", gamma=ic.gamma, precision="fp32") as ctx:
+            ctx.sim_init(ic.pos, ic.rho, ic.vel, ic.energy, ic.deposit)
+            if host:
+                arrs = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory().numpy() for a in ctx.sim_get()]
+                dts = [ctx.sim_step_host(0.3, 0.0, *arrs) for _ in range(3)]
+                out.append((dts, *[a.copy() for a in arrs]))
+            else:
+                dts = [ctx.sim_step(0.3) for _ in range(3)]
+                out.append((dts, *ctx.sim_get()))
+    for a, b in zip(*out):
+        assert np.array_equal(np.asarray(a), np.asarray(b))
