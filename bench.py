@@ -237,8 +237,9 @@ def cpu_reference_step_rate(steps: int, cfg: dict, n_sample: int = CPU_SAMPLE_PO
         ic = ics.clustered_3d(n=n_sample, seed=cfg["seed"]) if clustered else ics.sedov_3d(n=n_sample, seed=2)
         buff = min(cfg["buff"] * (cfg["n"] / n_sample) ** (1 / 3), 0.15)
         items, tot = [(ic, buff)], n_sample
+        same = "same clumps, fewer points" if clustered else "uniform in the box, fewer points"
         desc = (f"3D Sedov, {n_sample} {'clustered' if clustered else 'uniform'} points (the workload's "
-                f"distribution: same clumps, fewer points), K={K}, buff {buff:.3f}")
+                f"distribution: {same}), K={K}, buff {buff:.3f}")
     kind = "reference"
     try:
         import refbuild as rb
@@ -670,6 +671,9 @@ def run_extras(args, local_rank):
                           "warmup": {f: res[f]["steps_run"] - 1 - ke for f in res},
                           "stages_ms": dict(zip(STAGES, h["stage"])), "launches": h["launches"],
                           "vs_plain": compare_states(b["state"], h["state"])})
+                # the autotuner's choice for this workload (bin size, block shapes) and its gain
+                e["tuning"] = {k: h["tuning"].get(k) for k in ("ppb", "knn_warps", "clip_warps", "clip_thread",
+                                                               "knn_thread", "ms_default", "ms_tuned")}
                 if h.get("kbudget"):
                     kb = h["kbudget"]
                     e["learned_k"] = {"mean_k": kb["mean_k"], "plain_k": cfg["k"], "misses": kb["misses"],

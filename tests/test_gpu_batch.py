@@ -53,6 +53,16 @@ def test_batch_equals_solo_runs():
     _check_equal_to_solo(B, out, 3)
 
 
+def test_batch_of_64_instances_equals_solo_runs():
+    """64 instances of every kind (Sod with walls, Sedov, Kelvin-Helmholtz), both gammas, both
+    boundaries, 300 to 3000 points each: every one equals its solo run after 2 steps."""
+    B = ics.batch_2d(64, 17, 300, 3000)
+    assert len(B.instances) == 64 and len(set(B.boundary)) == 2
+    out = _batch(B, 2)
+    assert out[-1]["failed_cells"] == 0
+    _check_equal_to_solo(B, out, 2)
+
+
 def test_batch_learned_k_fp32_equals_plain_solo_runs():
     """The faster forms change no mesh: a learned-K + FP32 batch equals plain solo runs."""
     B = ics.batch_2d(4, 12, 2000, 15000)
