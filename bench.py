@@ -525,6 +525,7 @@ def run_ours(args, rank, world, local_rank):
                     "clip_split_ms": dict(zip(("main_clip", "fallback", "grid_walk"),
                                               r["stats"]["clip_split_ms"])),
                     "walked_cells": r["stats"]["pruned_cells"],
+                    "knn_exact_redone": r["stats"]["knn_redone"],
                     "speedup_vs_plain": rate(r) / rate(base) if base else None,
                     "tuning": {k: r["tuning"][k] for k in ("ppb", "knn_warps", "clip_warps", "clip_thread", "knn_thread",
                                                            "ms_default", "ms_tuned")}}

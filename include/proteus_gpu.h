@@ -301,7 +301,8 @@ typedef struct {
     int64_t walk_points, walk_boxes; /* that walk's work: points clipped, grid boxes visited */
     float clip_split_ms[3];     /* with timing on: the last build's clip stage as main clip (with the
                                    FP64 re-clip), fallback KNN + clip, grid walk */
-    int32_t pad_;
+    int32_t knn_redone;         /* queries of the last KNN stage searched a second time with exact keys
+                                   (a tie of FP32-rounded distances in the packed-key search) */
 } pgpu_stats;
 
 /* Statistics of the last step (synchronises the stream). */

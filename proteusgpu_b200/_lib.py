@@ -74,7 +74,7 @@ class Stats(C.Structure):
                 ("total_energy", C.c_double), ("total_mom", C.c_double * 3), ("cert_k_max", C.c_int32),
                 ("n_grid", C.c_int32), ("refit_cells", C.c_int64), ("uncertified_cells", C.c_int64),
                 ("reclip_cells", C.c_int64), ("pruned_cells", C.c_int64), ("walk_points", C.c_int64),
-                ("walk_boxes", C.c_int64), ("clip_split_ms", C.c_float * 3), ("pad_", C.c_int32)]
+                ("walk_boxes", C.c_int64), ("clip_split_ms", C.c_float * 3), ("knn_redone", C.c_int32)]
 
 
 class KBudgetInfo(C.Structure):

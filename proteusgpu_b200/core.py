@@ -349,7 +349,7 @@ class Context:
         s = _lib.Stats()
         check(self._h, self._L.pgpu_sim_stats(self._h, C.byref(s)), "pgpu_sim_stats")
         return {f: (list(getattr(s, f)) if f in ("total_mom", "clip_split_ms") else getattr(s, f))
-                for f, _ in s._fields_ if f != "pad_"}
+                for f, _ in s._fields_}
 
     # ---- learned neighbour budget (extension; the reference has one _K_ for all cells)
     def kbudget_enable(self, train_steps: int = 3, iters_per_step: int = 64, quantile: float = 0.99,

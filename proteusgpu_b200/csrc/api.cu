@@ -231,7 +231,7 @@ void pgpu_destroy(pgpu_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     DevBuf* bufs[] = {&c->knn_table, &c->fb_qs, &c->fb_knn, &c->pos,   &c->ext,     &c->gcnt,     &c->goff,   &c->ghost_src, &c->ghost_code, &c->bin_cnt,
                       &c->bin_start, &c->bin_key, &c->spts, &c->perm,  &c->inv,       &c->qflag,      &c->qoff,
-                      &c->qs,    &c->knn,     &c->vol,      &c->fptr,   &c->fcnt,      &c->status,     &c->certk,
+                      &c->qs,    &c->knn,     &c->knn_redo, &c->vol,      &c->fptr,   &c->fcnt,      &c->status,     &c->certk,
                       &c->centroid, &c->f_nb, &c->f_own,    &c->f_geo,  &c->scan_tmp,  &c->scalars,    &c->rho,
                       &c->vel,   &c->energy,  &c->rho2,     &c->vel2,   &c->energy2,   &c->mass,       &c->mom,
                       &c->en,    &c->w4,      &c->we,       &c->ale_wp, &c->ale_grad, &c->red_tmp, &c->dl_ptr,   &c->dl_a,       &c->dl_b,
@@ -973,6 +973,7 @@ int pgpu_sim_stats(pgpu_ctx* c, pgpu_stats* out) {
     out->walk_points = (int64_t)h.walk_points;
     out->walk_boxes = (int64_t)h.walk_boxes;
     for (int i = 0; i < 3; i++) out->clip_split_ms[i] = c->clip_ms[i];
+    out->knn_redone = (int32_t)h.knn_redo_total;
     return PGPU_OK;
 }
 

@@ -17,8 +17,11 @@
 // warp.  Candidates that beat the current K-th best queue in shared memory; a
 // full queue is bitonic-sorted across the warp with shuffles and merged row by
 // row (bitonic merge of the row with the reversed queue), in a loop that is not
-// unrolled so the kernel's code stays small.  Keys are (squared distance,
-// extended id): ties break by index.
+// unrolled so the kernel's code stays small.  Keys order by (squared distance,
+// extended id): ties break by index.  The search runs on packed 64-bit keys (the
+// distance rounded up to FP32 above the id); a query whose list a tie of rounded
+// distances could change is searched again with exact keys (k_knn_exact), so the
+// lists are the exact ones.
 //
 // The squared distance is the reference's dist2_point (src/knn/knn.h:64-75),
 // dx*dx + dy*dy (+ dz*dz) with dx = query - candidate, without FMA, so the
@@ -55,91 +58,167 @@ __device__ __forceinline__ uint32_t warp_incl_scan_u32(uint32_t v, int lane) {
     return v;
 }
 
-// Ascending bitonic sort of one (d, id) key per lane across the warp.
-__device__ __forceinline__ void bitonic_sort32(double& d, uint32_t& id, int lane) {
-#pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
-#pragma unroll
-        for (int j = k >> 1; j > 0; j >>= 1) {
-            double od = __shfl_xor_sync(FULL, d, j);
-            uint32_t oi = __shfl_xor_sync(FULL, id, j);
-            bool up = (lane & k) == 0;
-            bool lower = (lane & j) == 0;
-            bool take = (lower == up) ? key_less(od, oi, d, id) : key_less(d, id, od, oi);
-            if (take) {
-                d = od;
-                id = oi;
-            }
-        }
-    }
-}
+// Keys of the K-best rows.  Exact: (squared distance, extended id), compared
+// lexicographically.  Packed: one 64-bit integer, the squared distance rounded up to
+// FP32 in the high word and the id in the low word, so that an exchange takes two
+// shuffles and one integer compare instead of three shuffles and a pair compare.
+// Rounding up is monotone, so the packed order equals the exact one except between
+// keys whose rounded distances are equal; the packed search flags every such tie
+// that could change its list (see knn_query) and the query is searched again with
+// exact keys.  A packed K-th key's rounded distance bounds the exact one from
+// above, so box pruning against it keeps every box the exact search keeps.
+template <bool PK>
+struct KeyOps;
 
-// Ascending sort of a bitonic sequence held one key per lane.
-__device__ __forceinline__ void bitonic_merge32(double& d, uint32_t& id, int lane) {
-#pragma unroll
-    for (int j = 16; j > 0; j >>= 1) {
-        double od = __shfl_xor_sync(FULL, d, j);
-        uint32_t oi = __shfl_xor_sync(FULL, id, j);
-        bool lower = (lane & j) == 0;
-        bool take = lower ? key_less(od, oi, d, id) : key_less(d, id, od, oi);
-        if (take) {
-            d = od;
-            id = oi;
-        }
+template <>
+struct KeyOps<false> {
+    struct K {
+        double d;
+        uint32_t i;
+    };
+    static __device__ __forceinline__ K none() { return {CUDART_INF, NO_NEIGHBOR}; }
+    static __device__ __forceinline__ K make(double d, uint32_t i) { return {d, i}; }
+    static __device__ __forceinline__ bool lt(const K& a, const K& b) { return key_less(a.d, a.i, b.d, b.i); }
+    static __device__ __forceinline__ K shfl_xor(const K& a, int j) {
+        return {__shfl_xor_sync(FULL, a.d, j), __shfl_xor_sync(FULL, a.i, j)};
     }
-}
+    static __device__ __forceinline__ K shfl(const K& a, int src) {
+        return {__shfl_sync(FULL, a.d, src), __shfl_sync(FULL, a.i, src)};
+    }
+    static __device__ __forceinline__ uint32_t id(const K& a) { return a.i; }
+    static __device__ __forceinline__ bool held(const K& a) { return a.i != NO_NEIGHBOR; }
+    static __device__ __forceinline__ double bound(const K& a) { return a.d; }
+    static __device__ __forceinline__ bool tie(const K&, const K&) { return false; }
+};
+
+template <>
+struct KeyOps<true> {
+    using K = unsigned long long;
+    static __device__ __forceinline__ K none() { return ~0ull; }
+    static __device__ __forceinline__ K make(double d, uint32_t i) {
+        return ((K)__float_as_uint(__double2float_ru(d)) << 32) | i;
+    }
+    static __device__ __forceinline__ bool lt(K a, K b) { return a < b; }
+    static __device__ __forceinline__ K shfl_xor(K a, int j) { return __shfl_xor_sync(FULL, a, j); }
+    static __device__ __forceinline__ K shfl(K a, int src) { return __shfl_sync(FULL, a, src); }
+    static __device__ __forceinline__ uint32_t id(K a) { return (uint32_t)a; }
+    static __device__ __forceinline__ bool held(K a) { return a != ~0ull; }
+    static __device__ __forceinline__ double bound(K a) { return (double)__uint_as_float((uint32_t)(a >> 32)); }
+    static __device__ __forceinline__ bool tie(K a, K b) { return (a >> 32) == (b >> 32); }
+};
 
 // One warp's shared memory: the K best (rows of 32), the survivor queue and the
 // chunk's bin table.
-struct WarpKnn {
+template <bool PK>
+struct WarpKnn;
+
+template <>
+struct WarpKnn<false> {
+    using K = KeyOps<false>::K;
     double row_d[MAX_ROWS * 32];
     uint32_t row_i[MAX_ROWS * 32];
     double q_d[32];
     uint32_t q_i[32];
     uint32_t b_start[32];
     uint32_t b_excl[32];
+    __device__ __forceinline__ K row(int x) const { return {row_d[x], row_i[x]}; }
+    __device__ __forceinline__ void set_row(int x, const K& k) {
+        row_d[x] = k.d;
+        row_i[x] = k.i;
+    }
+    __device__ __forceinline__ K q(int x) const { return {q_d[x], q_i[x]}; }
+    __device__ __forceinline__ void set_q(int x, const K& k) {
+        q_d[x] = k.d;
+        q_i[x] = k.i;
+    }
 };
 
-// Merges qn queued keys into the warp's ascending rows (rows of 32 in shared
-// memory), keeping the 32 * nrows smallest.
-__device__ __noinline__ void merge_queue(double* rd, uint32_t* ri, const double* qd, const uint32_t* qi, int qn,
-                                         int nrows, int lane) {
-    double d = lane < qn ? qd[lane] : CUDART_INF;
-    uint32_t id = lane < qn ? qi[lane] : NO_NEIGHBOR;
-    bitonic_sort32(d, id, lane);
-#pragma unroll 1
-    for (int r = 0; r < nrows; r++) {
-        const double qmin = __shfl_sync(FULL, d, 0);
-        const uint32_t qmini = __shfl_sync(FULL, id, 0);
-        const double rmax = rd[r * 32 + 31];
-        const uint32_t rmaxi = ri[r * 32 + 31];
-        if (!key_less(qmin, qmini, rmax, rmaxi)) continue;  // the queue lies entirely above this row
-        double od = __shfl_sync(FULL, d, 31 - lane);
-        uint32_t oi = __shfl_sync(FULL, id, 31 - lane);
-        const double cd = rd[r * 32 + lane];
-        const uint32_t ci = ri[r * 32 + lane];
-        const bool rl = key_less(cd, ci, od, oi);
-        double lod = rl ? cd : od, hid = rl ? od : cd;
-        uint32_t loi = rl ? ci : oi, hii = rl ? oi : ci;
-        bitonic_merge32(lod, loi, lane);
-        bitonic_merge32(hid, hii, lane);
-        __syncwarp();
-        rd[r * 32 + lane] = lod;
-        ri[r * 32 + lane] = loi;
-        __syncwarp();
-        d = hid;
-        id = hii;
+template <>
+struct WarpKnn<true> {
+    using K = KeyOps<true>::K;
+    K row_k[MAX_ROWS * 32];
+    K q_k[32];
+    uint32_t b_start[32];
+    uint32_t b_excl[32];
+    __device__ __forceinline__ K row(int x) const { return row_k[x]; }
+    __device__ __forceinline__ void set_row(int x, K k) { row_k[x] = k; }
+    __device__ __forceinline__ K q(int x) const { return q_k[x]; }
+    __device__ __forceinline__ void set_q(int x, K k) { q_k[x] = k; }
+};
+
+// Ascending bitonic sort of one key per lane across the warp.
+template <bool PK>
+__device__ __forceinline__ void bitonic_sort32(typename KeyOps<PK>::K& a, int lane) {
+    using O = KeyOps<PK>;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const typename O::K o = O::shfl_xor(a, j);
+            const bool up = (lane & k) == 0;
+            const bool lower = (lane & j) == 0;
+            const bool take = (lower == up) ? O::lt(o, a) : O::lt(a, o);
+            if (take) a = o;
+        }
     }
 }
 
+// Ascending sort of a bitonic sequence held one key per lane.
+template <bool PK>
+__device__ __forceinline__ void bitonic_merge32(typename KeyOps<PK>::K& a, int lane) {
+    using O = KeyOps<PK>;
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) {
+        const typename O::K o = O::shfl_xor(a, j);
+        const bool lower = (lane & j) == 0;
+        const bool take = lower ? O::lt(o, a) : O::lt(a, o);
+        if (take) a = o;
+    }
+}
+
+// Merges qn queued keys into the warp's ascending rows, keeping the 32 * nrows
+// smallest.  Packed keys: returns whether an evicted key's rounded distance equals
+// the last held key's (a tie across the rows' end).
+template <bool PK>
+__device__ __noinline__ bool merge_queue(WarpKnn<PK>& S, int qn, int nrows, int lane) {
+    using O = KeyOps<PK>;
+    using K = typename O::K;
+    K a = lane < qn ? S.q(lane) : O::none();
+    bitonic_sort32<PK>(a, lane);
+#pragma unroll 1
+    for (int r = 0; r < nrows; r++) {
+        const K qmin = O::shfl(a, 0);
+        const K rmax = S.row(r * 32 + 31);
+        if (!O::lt(qmin, rmax)) continue;  // the queue lies entirely above this row
+        const K o = O::shfl(a, 31 - lane);
+        const K c = S.row(r * 32 + lane);
+        const bool rl = O::lt(c, o);
+        K lo = rl ? c : o, hi = rl ? o : c;
+        bitonic_merge32<PK>(lo, lane);
+        bitonic_merge32<PK>(hi, lane);
+        __syncwarp();
+        S.set_row(r * 32 + lane, lo);
+        __syncwarp();
+        a = hi;
+    }
+    if constexpr (PK) {
+        const K m = O::shfl(a, 0);
+        return O::held(m) && O::tie(m, S.row(nrows * 32 - 1));
+    }
+    return false;
+}
+
 // Processes one set of up to 32 bins (bstart, bcnt per lane) against the query.
-template <int D>
+// thr is the K-th held key (none until K are held); tie collects the packed
+// search's rejected keys whose rounded distance equals thr's.
+template <int D, bool PK>
 __device__ __forceinline__ void scan_bins(const typename PointOf<D>::type* __restrict__ spts,
                                           const uint32_t* __restrict__ perm, uint32_t bstart, uint32_t bcnt,
-                                          const typename PointOf<D>::type& p, uint32_t qid, WarpKnn& S,
-                                          int lane, int nrows, int K, int& qn, double& thr_d, uint32_t& thr_i,
-                                          unsigned long long& ncand) {
+                                          const typename PointOf<D>::type& p, uint32_t qid, WarpKnn<PK>& S,
+                                          int lane, int nrows, int K, int& qn, typename KeyOps<PK>::K& thr,
+                                          unsigned long long& ncand, bool& tie) {
     using PT = typename PointOf<D>::type;
+    using O = KeyOps<PK>;
     const uint32_t incl = warp_incl_scan_u32(bcnt, lane);
     const uint32_t total = __shfl_sync(FULL, incl, 31);
     if (total == 0) return;
@@ -151,61 +230,60 @@ __device__ __forceinline__ void scan_bins(const typename PointOf<D>::type* __res
     for (uint32_t k0 = 0; k0 < total; k0 += 32) {
         const uint32_t tt = k0 + lane;
         bool valid = tt < total;
-        double d2 = CUDART_INF;
-        uint32_t eid = NO_NEIGHBOR;
+        typename O::K key = O::none();
         if (valid) {
             int j = 0;
 #pragma unroll
             for (int step = 16; step > 0; step >>= 1)
                 if (j + step < 32 && S.b_excl[j + step] <= tt) j += step;
             const uint32_t sidx = S.b_start[j] + (tt - S.b_excl[j]);
-            eid = perm[sidx];
+            const uint32_t eid = perm[sidx];
             if (eid == qid) {
                 valid = false;
             } else {
                 const PT c = spts[sidx];
                 double ddx = p.x - c.x;
                 double ddy = p.y - c.y;
+                double d2;
                 if (D == 2) {
                     d2 = ddx * ddx + ddy * ddy;
                 } else {
                     double ddz = pz(p) - pz(c);
                     d2 = ddx * ddx + ddy * ddy + ddz * ddz;
                 }
+                if (PK && d2 != d2) valid = false;  // NaN: the exact compare drops it too
+                key = O::make(d2, eid);
             }
         }
-        bool surv = valid && key_less(d2, eid, thr_d, thr_i);
+        bool surv = valid && O::lt(key, thr);
+        if (PK) tie |= valid && !surv && O::tie(key, thr);
         unsigned bal = __ballot_sync(FULL, surv);
         if (bal == 0) continue;
         if (qn + __popc(bal) > 32) {
             __syncwarp();
-            merge_queue(S.row_d, S.row_i, S.q_d, S.q_i, qn, nrows, lane);
+            tie |= merge_queue<PK>(S, qn, nrows, lane);
             qn = 0;
             __syncwarp();
-            thr_d = S.row_d[K - 1];
-            thr_i = S.row_i[K - 1];
-            surv = surv && key_less(d2, eid, thr_d, thr_i);
+            thr = S.row(K - 1);
+            surv = surv && O::lt(key, thr);
+            if (PK) tie |= valid && !surv && O::tie(key, thr);
             bal = __ballot_sync(FULL, surv);
         }
-        if (surv) {
-            const int pos = qn + __popc(bal & ((1u << lane) - 1u));
-            S.q_d[pos] = d2;
-            S.q_i[pos] = eid;
-        }
+        if (surv) S.set_q(qn + __popc(bal & ((1u << lane) - 1u)), key);
         qn += __popc(bal);
         __syncwarp();
     }
 }
 
-__device__ __forceinline__ void flush_queue(WarpKnn& S, int lane, int nrows, int K, int& qn, double& thr_d,
-                                            uint32_t& thr_i) {
+template <bool PK>
+__device__ __forceinline__ void flush_queue(WarpKnn<PK>& S, int lane, int nrows, int K, int& qn,
+                                            typename KeyOps<PK>::K& thr, bool& tie) {
     if (qn == 0) return;
     __syncwarp();
-    merge_queue(S.row_d, S.row_i, S.q_d, S.q_i, qn, nrows, lane);
+    tie |= merge_queue<PK>(S, qn, nrows, lane);
     qn = 0;
     __syncwarp();
-    thr_d = S.row_d[K - 1];
-    thr_i = S.row_i[K - 1];
+    thr = S.row(K - 1);
 }
 
 // Squared distance from p to the box of bin (x, y, z).
@@ -258,34 +336,30 @@ __device__ __forceinline__ bool box_range(const SubGrid& g, uint32_t slot0, int 
     return true;
 }
 
-// 32 warps per SM: at most 64 registers a thread (the search is latency bound on its
-// warp-collective chains; more resident warps hide more of them)
-template <int D, int KW>
-__global__ void __launch_bounds__(KW * 32, 32 / KW)
-    k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
-          const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
-          int K, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
-          unsigned long long* __restrict__ cand_counter, int skip_upto) {
-    __shared__ WarpKnn S_all[KW];
+// One query's search by one warp (query t, budget K): the K nearest ext ids of the
+// query point, ascending, written to out[t * stride ...].  Packed keys: returns
+// true (and writes nothing) when a tie of rounded distances could make the list
+// differ from the exact one -- two equal rounded distances side by side among the
+// first K + 1 held keys, or a rejected or evicted key whose rounded distance equals
+// the K-th's at the time -- so that the query is searched again with exact keys.
+template <int D, bool PK>
+__device__ __forceinline__ bool knn_query(const typename PointOf<D>::type* __restrict__ spts,
+                                          const uint32_t* __restrict__ perm, const SubGrid& grid,
+                                          const int2* __restrict__ table, int table_n, int table_r,
+                                          const uint32_t* __restrict__ qs, int64_t t, int K, int stride,
+                                          uint32_t* __restrict__ out, WarpKnn<PK>& S, int lane,
+                                          unsigned long long& ncand) {
     using PT = typename PointOf<D>::type;
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const int64_t t = (int64_t)blockIdx.x * KW + w;
-    if (t >= nq) return;  // warp-uniform
-    WarpKnn& S = S_all[w];
-    if (kq) K = kq[t];
-    if (K <= skip_upto) return;  // done by k_knn_t
+    using O = KeyOps<PK>;
     const int nrows = (K + 31) >> 5;
-    for (int r = 0; r < nrows; r++) {
-        S.row_d[r * 32 + lane] = CUDART_INF;
-        S.row_i[r * 32 + lane] = NO_NEIGHBOR;
-    }
+    for (int r = 0; r < nrows; r++) S.set_row(r * 32 + lane, O::none());
     __syncwarp();
     const uint32_t s = qs[t];
     const PT p = spts[s];
     const uint32_t qid = perm[s];
     if (!(isfinite(p.x) && isfinite(p.y) && isfinite(pz(p)))) {  // no neighbours for a point without a position
         for (int idx = lane; idx < K; idx += 32) out[t * stride + idx] = NO_NEIGHBOR;
-        return;
+        return false;
     }
     const double pc[3] = {p.x, p.y, pz(p)};
     // the query searches its own instance's grid at its own bin's level: boxes of side 1 / (G << Lq)
@@ -297,11 +371,9 @@ __global__ void __launch_bounds__(KW * 32, 32 / KW)
     const int G = G0 << Lq;
     const int bc[3] = {sub_coord(p.x, G0, Lq), sub_coord(p.y, G0, Lq), D == 3 ? sub_coord(pz(p), G0, Lq) : 0};
     const double h = 1.0 / (double)G;
-    double thr_d = CUDART_INF;
-    uint32_t thr_i = NO_NEIGHBOR;
+    typename O::K thr = O::none();
     int qn = 0;
-    unsigned long long ncand = 0;
-    bool done = false;
+    bool tie = false;
 
     // 1. offsets in order of their lower bound
     for (int c0 = 0; c0 < table_n; c0 += 32) {
@@ -309,7 +381,7 @@ __global__ void __launch_bounds__(KW * 32, 32 / KW)
         // every remaining table bin is farther than the K-th neighbour; bins beyond the
         // table (which may be nearer than the table's last entries) are left to the
         // ring search, whose first test ends it at once when they are all too far
-        if (thr_i != NO_NEIGHBOR && (double)first.y * h * h * (1.0 - 1e-12) > thr_d) break;
+        if (O::held(thr) && (double)first.y * h * h * (1.0 - 1e-12) > O::bound(thr)) break;
         const int ci = c0 + lane;
         uint32_t bstart = 0, bcnt = 0;
         if (ci < table_n) {
@@ -318,18 +390,18 @@ __global__ void __launch_bounds__(KW * 32, 32 / KW)
                       dz = (int)(signed char)((ent.x >> 16) & 255);
             const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
             bool ok = x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G));
-            if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
+            if (ok && O::held(thr) && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > O::bound(thr)) ok = false;
             if (ok && !box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
         }
-        scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, lane, nrows, K, qn, thr_d, thr_i, ncand);
+        scan_bins<D, PK>(spts, perm, bstart, bcnt, p, qid, S, lane, nrows, K, qn, thr, ncand, tie);
         // the bound is tested at chunk boundaries: merge what is queued once it is worth a
         // merge (a staler bound only prunes less; the rows fill up first)
-        if (qn >= KNN_FLUSH_MIN || thr_i == NO_NEIGHBOR) flush_queue(S, lane, nrows, K, qn, thr_d, thr_i);
+        if (qn >= KNN_FLUSH_MIN || !O::held(thr)) flush_queue<PK>(S, lane, nrows, K, qn, thr, tie);
     }
-    flush_queue(S, lane, nrows, K, qn, thr_d, thr_i);
+    flush_queue<PK>(S, lane, nrows, K, qn, thr, tie);
 
     // 2. beyond the table: Chebyshev rings table_r + 1, table_r + 2, ... (sparse regions)
-    for (int r = table_r + 1; !done; r++) {
+    for (int r = table_r + 1;; r++) {
         double lb = CUDART_INF;
         bool all = true;
 #pragma unroll
@@ -345,7 +417,7 @@ __global__ void __launch_bounds__(KW * 32, 32 / KW)
             }
         }
         if (all || r > G + 1) break;
-        if (thr_i != NO_NEIGHBOR && lb > 0.0 && thr_d < lb * lb * (1.0 - 1e-12)) break;
+        if (O::held(thr) && lb > 0.0 && O::bound(thr) < lb * lb * (1.0 - 1e-12)) break;
         const int w1 = 2 * r + 1;
         const int ncube = D == 2 ? w1 * w1 : w1 * w1 * w1;
         for (int c0 = 0; c0 < ncube; c0 += 32) {
@@ -359,16 +431,75 @@ __global__ void __launch_bounds__(KW * 32, 32 / KW)
                 const int cheb = max(abs(dx), max(abs(dy), abs(dz)));
                 const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
                 bool ok = cheb == r && x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G));
-                if (ok && thr_i != NO_NEIGHBOR && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) ok = false;
+                if (ok && O::held(thr) && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > O::bound(thr)) ok = false;
                 if (ok && !box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) bcnt = 0;
             }
-            scan_bins<D>(spts, perm, bstart, bcnt, p, qid, S, lane, nrows, K, qn, thr_d, thr_i, ncand);
+            scan_bins<D, PK>(spts, perm, bstart, bcnt, p, qid, S, lane, nrows, K, qn, thr, ncand, tie);
         }
-        flush_queue(S, lane, nrows, K, qn, thr_d, thr_i);
+        flush_queue<PK>(S, lane, nrows, K, qn, thr, tie);
     }
     __syncwarp();
-    for (int idx = lane; idx < K; idx += 32) out[t * stride + idx] = S.row_i[idx];
-    if (cand_counter && lane == 0) atomicAdd(cand_counter, ncand);
+    if (PK) {
+        // equal rounded distances side by side among the first K + 1 held keys
+        for (int idx = lane; idx < K; idx += 32)
+            if (idx + 1 < nrows * 32) {
+                const typename O::K a = S.row(idx);
+                if (O::held(a) && O::tie(a, S.row(idx + 1))) tie = true;
+            }
+        tie = __any_sync(FULL, tie);
+        if (tie) return true;
+    }
+    for (int idx = lane; idx < K; idx += 32) out[t * stride + idx] = O::id(S.row(idx));
+    return false;
+}
+
+// 32 warps per SM: at most 64 registers a thread (the search is latency bound on its
+// warp-collective chains; more resident warps hide more of them).  Packed keys; a
+// query with a tie is listed in redo for k_knn_exact.
+template <int D, int KW>
+__global__ void __launch_bounds__(KW * 32, 32 / KW)
+    k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
+          const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
+          int K, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
+          unsigned long long* __restrict__ cand_counter, int skip_upto, uint32_t* __restrict__ redo,
+          unsigned* __restrict__ redo_n) {
+    __shared__ WarpKnn<true> S_all[KW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t t = (int64_t)blockIdx.x * KW + w;
+    if (t >= nq) return;  // warp-uniform
+    if (kq) K = kq[t];
+    if (K <= skip_upto) return;  // done by k_knn_t
+    unsigned long long ncand = 0;
+    const bool tie = knn_query<D, true>(spts, perm, grid, table, table_n, table_r, qs, t, K, stride, out, S_all[w],
+                                        lane, ncand);
+    if (lane == 0) {
+        if (tie) redo[atomicAdd(redo_n, 1u)] = (uint32_t)t;
+        if (cand_counter) atomicAdd(cand_counter, ncand);
+    }
+}
+
+// The queries k_knn listed in redo, searched again with exact keys; warps stride
+// over the list, whose length the device holds.
+template <int D, int KW>
+__global__ void __launch_bounds__(KW * 32, 32 / KW)
+    k_knn_exact(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm,
+                SubGrid grid, const int2* __restrict__ table, int table_n, int table_r,
+                const uint32_t* __restrict__ qs, int Kall, const uint16_t* __restrict__ kq, int stride,
+                uint32_t* __restrict__ out, unsigned long long* __restrict__ cand_counter,
+                const uint32_t* __restrict__ redo, const unsigned* __restrict__ redo_n,
+                unsigned* __restrict__ redo_total) {
+    __shared__ WarpKnn<false> S_all[KW];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t n = *redo_n;
+    if (blockIdx.x == 0 && threadIdx.x == 0 && n) atomicAdd(redo_total, (unsigned)n);
+    unsigned long long ncand = 0;
+    for (int64_t i = (int64_t)blockIdx.x * KW + w; i < n; i += (int64_t)gridDim.x * KW) {  // warp-uniform
+        const int64_t t = redo[i];
+        const int K = kq ? (int)kq[t] : Kall;
+        knn_query<D, false>(spts, perm, grid, table, table_n, table_r, qs, t, K, stride, out, S_all[w], lane,
+                            ncand);
+    }
+    if (cand_counter && lane == 0 && ncand) atomicAdd(cand_counter, ncand);
 }
 
 // Thread-per-query variant for small K (<= KT): the same bins in the same order,
@@ -574,17 +705,34 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
         }
     }
     const int skip = KT > 0 ? std::min(K, KT) : 0;  // the queries k_knn_t did
+    uint32_t* redo = ensure<uint32_t>(c->knn_redo, (size_t)nq, &e);
+    if (e) return e;
+    if ((e = cudaMemsetAsync(&sc->knn_redo, 0, sizeof(unsigned), c->stream))) return e;
 #define PGPU_KNN(DD, PT, WW)                                                                                 \
     k_knn<DD, WW><<<blocks, WW * 32, 0, c->stream>>>((const PT*)c->spts.p, perm, grid, tab, c->knn_table_n,     \
                                                       c->knn_table_r, qs, nq, K, kq, stride, out, &sc->knn_cand, \
-                                                      skip)
+                                                      skip, redo, &sc->knn_redo)
     if (c->prm.dim == 2) {
         if (KW == 2) PGPU_KNN(2, double2, 2); else if (KW == 8) PGPU_KNN(2, double2, 8); else PGPU_KNN(2, double2, 4);
     } else {
         if (KW == 2) PGPU_KNN(3, double4, 2); else if (KW == 8) PGPU_KNN(3, double4, 8); else PGPU_KNN(3, double4, 4);
     }
 #undef PGPU_KNN
-    count_launches(launches + 1);
+    // the tied queries again with exact keys: a fixed grid whose warps stride over the
+    // device-held list (no read-back of its length)
+    const unsigned xblocks = (unsigned)std::min<int64_t>(blocks, 148 * 4);
+#define PGPU_KNNX(DD, PT, WW)                                                                                   \
+    k_knn_exact<DD, WW><<<xblocks, WW * 32, 0, c->stream>>>((const PT*)c->spts.p, perm, grid, tab,               \
+                                                             c->knn_table_n, c->knn_table_r, qs, K, kq, stride,  \
+                                                             out, &sc->knn_cand, redo, &sc->knn_redo,            \
+                                                             &sc->knn_redo_total)
+    if (c->prm.dim == 2) {
+        if (KW == 2) PGPU_KNNX(2, double2, 2); else if (KW == 8) PGPU_KNNX(2, double2, 8); else PGPU_KNNX(2, double2, 4);
+    } else {
+        if (KW == 2) PGPU_KNNX(3, double4, 2); else if (KW == 8) PGPU_KNNX(3, double4, 8); else PGPU_KNNX(3, double4, 4);
+    }
+#undef PGPU_KNNX
+    count_launches(launches + 2);
     return cudaGetLastError();
 }
 
@@ -596,6 +744,7 @@ cudaError_t launch_knn(pgpu_ctx* c) {
     if (e) return e;
     DevScalars* sc = (DevScalars*)c->scalars.p;
     if ((e = cudaMemsetAsync(&sc->knn_cand, 0, sizeof(unsigned long long), c->stream))) return e;
+    if ((e = cudaMemsetAsync(&sc->knn_redo_total, 0, sizeof(unsigned), c->stream))) return e;
     return launch_knn_list(c, (const uint32_t*)c->qs.p, c->n_query, K, out,
                            c->use_kq ? (const uint16_t*)c->kq.p : nullptr, K);
 }

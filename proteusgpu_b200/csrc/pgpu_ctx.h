@@ -59,6 +59,8 @@ struct DevScalars {
     unsigned long long walk_points; // grid walk: points clipped (statistics; after the
     unsigned long long walk_boxes;  //   per-step counters, which are cleared up to dt)
     unsigned int sort_big;          // grid sort: sub-bins too large for one thread
+    unsigned int knn_redo;          // KNN: queries listed for the exact-key search (per launch)
+    unsigned int knn_redo_total;    // and their total over the last KNN stage (statistics)
 };
 
 // Learned neighbour budget: a per-cell MLP (8 features -> 32 -> 32 -> 6 classes,
@@ -152,6 +154,7 @@ struct pgpu_ctx {
     pgpu::DevBuf spts, perm, inv;  // sorted points, sorted->ext id, ext id->sorted
     pgpu::DevBuf qflag, qoff, qs;  // query list (sorted positions of the cells to compute)
     pgpu::DevBuf knn;          // n_query rows of knn_stride ext ids
+    pgpu::DevBuf knn_redo;     // u32 query indices whose packed-key search met a tie
     int knn_stride = 0;        // ids per row: prm.k, or the largest learned budget
     pgpu::DevBuf kq;           // u16 per query slot: learned neighbour budget
     bool use_kq = false;       // this step's lists and clip use kq

@@ -61,3 +61,83 @@ def test_reflective_ghosts_are_mirrors():
         d = (code // 3 ** a) % 3
         assert np.allclose(g[d == 1, a], -p[d == 1, a]) and np.allclose(g[d == 2, a], 2 - p[d == 2, a])
         assert np.allclose(g[d == 0, a], p[d == 0, a])
+
+
+# ---- the packed-key KNN's tie rule (knn.cu knn_query / merge_queue / scan_bins), on a host
+# model of the search: survivors queue (32) and merge into rows of 32 keeping the 32 * rows
+# smallest; the threshold is the K-th held key.  Keys are (FP32 rounded-up distance, id) in one
+# integer.  Whenever no tie is flagged, the list must be the exact (FP64 distance, id) top K.
+def _f32_up_bits(d):
+    f = np.float32(d)
+    if float(f) < d:
+        f = np.nextafter(f, np.float32(np.inf))
+    return int(np.array(f, np.float32).view(np.uint32))
+
+
+def _packed_search(cands, K, chunk=40, flush_min=24):
+    none = (1 << 64) - 1
+    nrows = (K + 31) // 32
+    st = {"rows": [none] * (nrows * 32), "thr": none, "tie": False, "q": []}
+
+    def merge():
+        keys = sorted(st["rows"] + st["q"])
+        st["rows"], evicted = keys[: nrows * 32], [k for k in keys[nrows * 32:] if k != none]
+        if evicted and st["rows"][-1] != none and (min(evicted) >> 32) == (st["rows"][-1] >> 32):
+            st["tie"] = True
+        st["q"], st["thr"] = [], st["rows"][K - 1]
+
+    def offer(k):
+        surv = k < st["thr"]
+        if not surv and st["thr"] != none and (k >> 32) == (st["thr"] >> 32):
+            st["tie"] = True
+        return surv
+
+    for c0 in range(0, len(cands), chunk):
+        for d, i in cands[c0:c0 + chunk]:
+            k = (_f32_up_bits(d) << 32) | i
+            if offer(k):
+                if len(st["q"]) == 32:
+                    merge()
+                    if not offer(k):
+                        continue
+                st["q"].append(k)
+        if st["q"] and (len(st["q"]) >= flush_min or st["thr"] == none):
+            merge()
+    if st["q"]:
+        merge()
+    rows = st["rows"]
+    for idx in range(min(K, nrows * 32 - 1)):
+        if rows[idx] != none and (rows[idx] >> 32) == (rows[idx + 1] >> 32):
+            st["tie"] = True
+    return [r & 0xFFFFFFFF for r in rows[:K]], st["tie"]
+
+
+def test_packed_knn_keys_flag_every_tie_that_could_change_a_list():
+    rng = np.random.default_rng(7)
+    flagged = 0
+    for trial in range(800):
+        K, n = int(rng.integers(1, 100)), int(rng.integers(1, 300))
+        if trial % 4 == 0:
+            d = rng.uniform(0.0, 1.0, n)
+        elif trial % 4 == 1:  # distances within an FP32 rounding step of each other
+            base = np.repeat(rng.uniform(0.1, 1.0, n // 6 + 1), 6)[:n]
+            d = base * (1 + rng.integers(0, 4, n) * 2e-17 + rng.integers(0, 3, n) * 3e-9)
+        elif trial % 4 == 2:  # exact ties
+            d = rng.integers(0, 15, n) * 0.01
+        else:  # the K-th and (K+1)-th within a rounding step, the nearer one arriving last
+            n = max(n, K + 2)
+            d = np.sort(rng.uniform(0.1, 1.0, n))
+            d[K] = d[K - 1] * (1 + 1e-9)
+        ids = rng.permutation(10 * n)[:n]
+        cands = list(zip(d.tolist(), ids.tolist()))
+        order = np.argsort(d + rng.uniform(0.0, 0.3, n))  # roughly by distance, as the bin table
+        if trial % 4 == 3:  # the nearer of the pair gets the larger id and comes last
+            cands[K - 1], cands[K] = (d[K - 1], int(max(ids[K - 1], ids[K]))), (d[K], int(min(ids[K - 1], ids[K])))
+            order = np.array([j for j in np.argsort(d) if j != K - 1] + [K - 1])
+        cands = [cands[j] for j in order]
+        exact = [i for _, i in sorted(cands)[:K]]
+        exact += [0xFFFFFFFF] * (K - len(exact))
+        got, tie = _packed_search(cands, K)
+        flagged += tie
+        assert tie or got == exact, (trial, K, n)
+    assert 0 < flagged < 800  # the adversarial inputs do raise flags; uniform ones mostly not
