@@ -453,11 +453,12 @@ __device__ __forceinline__ bool knn_query(const typename PointOf<D>::type* __res
     return false;
 }
 
-// 32 warps per SM: at most 64 registers a thread (the search is latency bound on its
-// warp-collective chains; more resident warps hide more of them).  Packed keys; a
-// query with a tie is listed in redo for k_knn_exact.
+// 40 warps per SM: at most 48 registers a thread, a few spilled (the search is latency
+// bound on its warp-collective chains; more resident warps hide more of them: 122.0 ->
+// 118.4 ms at 16.8M clustered points against 32 warps).  Packed keys; a query with a tie
+// is listed in redo for k_knn_exact.
 template <int D, int KW>
-__global__ void __launch_bounds__(KW * 32, 32 / KW)
+__global__ void __launch_bounds__(KW * 32, 40 / KW)
     k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
           const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
           int K, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
