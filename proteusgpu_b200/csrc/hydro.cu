@@ -194,6 +194,26 @@ __global__ void k_prim_dt(const double* __restrict__ mass, const double* __restr
     }
 }
 
+// Index in its cell's face list (records hp .. hp + hn - 1) of the first face whose
+// owner record is want, or -1.  Eight records are loaded per step, independently of one
+// another, so a search costs about one dependent load round trip per eight records
+// instead of one per record (16.8M clustered cells: flux 28.4 -> 22.6 ms).
+__device__ __forceinline__ int partner_face(const uint32_t* __restrict__ f_own, uint32_t hp, uint32_t hn,
+                                            uint32_t want) {
+    constexpr int W = 8;
+    for (uint32_t r0 = 0; r0 < hn; r0 += W) {
+        uint32_t v[W];
+#pragma unroll
+        for (int j = 0; j < W; j++) v[j] = r0 + j < hn ? f_own[hp + r0 + j] : BOX_FACE;
+        int hit = -1;
+#pragma unroll
+        for (int j = W - 1; j >= 0; j--)
+            if (v[j] == want) hit = (int)(r0 + j);
+        if (hit >= 0) return hit;
+    }
+    return -1;
+}
+
 // 24 warps per SM (at most 85 registers a thread; the HLL arithmetic spills a little):
 // the gathers of the neighbours' states and faces are latency bound, more resident
 // warps hide more of them (16.8M points: 31.4 -> 28.4 ms)
@@ -237,15 +257,12 @@ __global__ void __launch_bounds__(HT, 3) k_flux_update(const double4* __restrict
             if (PHYSICAL && h < (uint32_t)i) {
                 // the lower hydro id's value of this face's area
                 const uint32_t want = pack_owner((uint32_t)i, reverse_code(code, D, !mirror));
-                const uint32_t hp = fptr[h], hn = fcnt[h];
-                bool found = false;
-                for (uint32_t r = 0; r < hn; r++)
-                    if (f_own[hp + r] == want) {
-                        A = f_geo[hp + r].w;
-                        found = true;
-                        break;
-                    }
-                if (!found && w4[h].x >= 0.0) nunp++;
+                const uint32_t hp = fptr[h];
+                const int r = partner_face(f_own, hp, fcnt[h], want);
+                if (r >= 0)
+                    A = f_geo[hp + r].w;
+                else if (w4[h].x >= 0.0)
+                    nunp++;
             }
         }
         const double4 wj4 = w4[h];
@@ -483,20 +500,18 @@ __global__ void k_ale_flux(const double4* __restrict__ w4, const double* __restr
         ale_offset<D>(ext, f_nb[fp + q], (uint32_t)i, scale, d);
         if (h < (uint32_t)i) {
             const uint32_t want = pack_owner((uint32_t)i, reverse_code(code, D, true));
-            const uint32_t hp = fptr[h], hn = fcnt[h];
-            bool found = false;
-            for (uint32_t r = 0; r < hn; r++)
-                if (f_own[hp + r] == want) {
-                    double dh[3];
-                    ale_offset<D>(ext, f_nb[hp + r], h, scale, dh);
-                    d[0] = -dh[0];
-                    d[1] = -dh[1];
-                    d[2] = -dh[2];
-                    A = f_geo[hp + r].w;
-                    found = true;
-                    break;
-                }
-            if (!found) nunp++;
+            const uint32_t hp = fptr[h];
+            const int r = partner_face(f_own, hp, fcnt[h], want);
+            if (r >= 0) {
+                double dh[3];
+                ale_offset<D>(ext, f_nb[hp + r], h, scale, dh);
+                d[0] = -dh[0];
+                d[1] = -dh[1];
+                d[2] = -dh[2];
+                A = f_geo[hp + r].w;
+            } else {
+                nunp++;
+            }
         }
         double L[NV], R[NV];
         if (ORDER == 1) {

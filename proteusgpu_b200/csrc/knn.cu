@@ -509,22 +509,27 @@ __global__ void __launch_bounds__(KW * 32, 32 / KW)
 // final K-th, so the list equals the warp kernel's.  Queries with a larger K return
 // at once here and are done by k_knn, which skips the ones done here.
 // The lists live in shared memory, entry i of thread t at [i * KNN_T_THREADS + t]
-// (conflict-free; per-thread local arrays of this size spill out of L1).
+// (conflict-free; per-thread local arrays of this size spill out of L1).  Keys are
+// packed like k_knn's, with the same tie rule for a list of exactly K: a rejected key
+// whose rounded distance equals the K-th's, a key pushed out whose rounded distance
+// equals the new K-th's, or two equal rounded distances side by side in the list send
+// the query to redo for k_knn_exact.
 constexpr int KNN_T_THREADS = 64;
 
-// Dynamic shared memory: kcap * KNN_T_THREADS doubles, then as many u32, with
-// kcap = min(Kall, KT) (at most 48 KB).
+// Dynamic shared memory: kcap * KNN_T_THREADS packed keys, kcap = min(Kall, KT).
 template <int D>
 __global__ void __launch_bounds__(KNN_T_THREADS)
     k_knn_t(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
             const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
             int Kall, int KT, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
-            unsigned long long* __restrict__ cand_counter) {
+            unsigned long long* __restrict__ cand_counter, uint32_t* __restrict__ redo,
+            unsigned* __restrict__ redo_n) {
     using PT = typename PointOf<D>::type;
+    using O = KeyOps<true>;
+    using Key = O::K;
     extern __shared__ __align__(16) unsigned char knn_t_smem[];
     const int kcap = min(Kall, KT);
-    double* kd = (double*)knn_t_smem + threadIdx.x;
-    uint32_t* ki = (uint32_t*)(knn_t_smem + (size_t)kcap * KNN_T_THREADS * sizeof(double)) + threadIdx.x;
+    Key* kk = (Key*)knn_t_smem + threadIdx.x;
     constexpr int S = KNN_T_THREADS;
     const int64_t t = (int64_t)blockIdx.x * KNN_T_THREADS + threadIdx.x;
     unsigned long long ncand = 0;
@@ -532,8 +537,8 @@ __global__ void __launch_bounds__(KNN_T_THREADS)
         const int K = kq ? (int)kq[t] : Kall;
         if (K <= kcap) {  // the rest: k_knn
             int cnt = 0;
-            double thr_d = CUDART_INF;  // the K-th key once K are held, else (inf, none)
-            uint32_t thr_i = NO_NEIGHBOR;
+            Key thr = O::none();  // the K-th key once K are held
+            bool tie = false;
             const uint32_t s = qs[t];
             const PT p = spts[s];
             const uint32_t qid = perm[s];
@@ -548,7 +553,6 @@ __global__ void __launch_bounds__(KNN_T_THREADS)
                 const int bc[3] = {sub_coord(p.x, G0, Lq), sub_coord(p.y, G0, Lq),
                                    D == 3 ? sub_coord(pz(p), G0, Lq) : 0};
                 const double h = 1.0 / (double)G;
-                auto full = [&]() { return cnt >= K; };  // thr_* then hold the K-th key
                 auto scan_range = [&](uint32_t bstart, uint32_t bcnt) {
                     ncand += bcnt;
                     for (uint32_t q = bstart; q < bstart + bcnt; q++) {
@@ -563,35 +567,37 @@ __global__ void __launch_bounds__(KNN_T_THREADS)
                             const double ddz = pz(p) - pz(c);
                             d2 = ddx * ddx + ddy * ddy + ddz * ddz;
                         }
-                        // the warp kernel's test: against (inf, none) until K are held (drops NaN)
-                        if (!key_less(d2, eid, thr_d, thr_i)) continue;
+                        if (d2 != d2) continue;  // NaN: the exact compare drops it too
+                        const Key key = O::make(d2, eid);
+                        if (!(key < thr)) {
+                            if (O::held(thr) && O::tie(key, thr)) tie = true;
+                            continue;
+                        }
+                        const Key out_key = cnt == K ? kk[(K - 1) * S] : O::none();
                         int i = cnt < K ? cnt : K - 1;
                         while (i > 0) {
-                            const double od = kd[(i - 1) * S];
-                            const uint32_t oi = ki[(i - 1) * S];
-                            if (!key_less(d2, eid, od, oi)) break;
-                            kd[i * S] = od;
-                            ki[i * S] = oi;
+                            const Key o = kk[(i - 1) * S];
+                            if (!(key < o)) break;
+                            kk[i * S] = o;
                             i--;
                         }
-                        kd[i * S] = d2;
-                        ki[i * S] = eid;
+                        kk[i * S] = key;
                         if (cnt < K) cnt++;
                         if (cnt == K) {
-                            thr_d = kd[(K - 1) * S];
-                            thr_i = ki[(K - 1) * S];
+                            thr = kk[(K - 1) * S];
+                            if (O::held(out_key) && O::tie(out_key, thr)) tie = true;
                         }
                     }
                 };
                 // 1. offsets in order of their lower bound
                 for (int ci = 0; ci < table_n; ci++) {
                     const int2 ent = table[ci];
-                    if (full() && (double)ent.y * h * h * (1.0 - 1e-12) > thr_d) break;
+                    if (O::held(thr) && (double)ent.y * h * h * (1.0 - 1e-12) > O::bound(thr)) break;
                     const int dx = (int)(signed char)(ent.x & 255), dy = (int)(signed char)((ent.x >> 8) & 255),
                               dz = (int)(signed char)((ent.x >> 16) & 255);
                     const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
                     if (!(x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G)))) continue;
-                    if (full() && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) continue;
+                    if (O::held(thr) && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > O::bound(thr)) continue;
                     uint32_t bstart, bcnt;
                     if (box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) scan_range(bstart, bcnt);
                 }
@@ -611,7 +617,7 @@ __global__ void __launch_bounds__(KNN_T_THREADS)
                         }
                     }
                     if (all || r > G + 1) break;
-                    if (full() && lb > 0.0 && thr_d < lb * lb * (1.0 - 1e-12)) break;
+                    if (O::held(thr) && lb > 0.0 && O::bound(thr) < lb * lb * (1.0 - 1e-12)) break;
                     const int w1 = 2 * r + 1;
                     const int ncube = D == 2 ? w1 * w1 : w1 * w1 * w1;
                     for (int ci = 0; ci < ncube; ci++) {
@@ -620,13 +626,18 @@ __global__ void __launch_bounds__(KNN_T_THREADS)
                         if (max(abs(dx), max(abs(dy), abs(dz))) != r) continue;
                         const int x = bc[0] + dx, y = bc[1] + dy, z = bc[2] + dz;
                         if (!(x >= 0 && x < G && y >= 0 && y < G && (D == 2 || (z >= 0 && z < G)))) continue;
-                        if (full() && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > thr_d) continue;
+                        if (O::held(thr) && box_d2<D>(pc, x, y, z, h) * (1.0 - 1e-12) > O::bound(thr)) continue;
                         uint32_t bstart, bcnt;
                         if (box_range<D>(grid, slot0, Lq, x, y, z, bc, bstart, bcnt)) scan_range(bstart, bcnt);
                     }
                 }
             }
-            for (int i = 0; i < K; i++) out[t * stride + i] = i < cnt ? ki[i * S] : NO_NEIGHBOR;
+            for (int i = 0; i + 1 < cnt; i++)
+                if (O::tie(kk[i * S], kk[(i + 1) * S])) tie = true;
+            if (tie)
+                redo[atomicAdd(redo_n, 1u)] = (uint32_t)t;
+            else
+                for (int i = 0; i < K; i++) out[t * stride + i] = i < cnt ? O::id(kk[i * S]) : NO_NEIGHBOR;
         }
     }
     if (cand_counter) {
@@ -689,36 +700,36 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
                           (const uint8_t*)c->bin_lvl.p, (const uint32_t*)c->sub_off.p,
                           (const uint32_t*)c->sub_start.p};
     const int2* tab = (const int2*)c->knn_table.p;
-    int launches = 0;
-    if (KT > 0) {
-        const unsigned tblocks = (unsigned)((nq + KNN_T_THREADS - 1) / KNN_T_THREADS);
-        const size_t smem = (size_t)std::min(K, KT) * KNN_T_THREADS * (sizeof(double) + sizeof(uint32_t));
-#define PGPU_KNN_T(DD, PT)                                                                                    \
-    k_knn_t<DD><<<tblocks, KNN_T_THREADS, smem, c->stream>>>((const PT*)c->spts.p, perm, grid, tab,            \
-                                                              c->knn_table_n, c->knn_table_r, qs, nq, K, KT, kq, \
-                                                              stride, out, &sc->knn_cand)
-        if (c->prm.dim == 2) PGPU_KNN_T(2, double2); else PGPU_KNN_T(3, double4);
-#undef PGPU_KNN_T
-        launches++;
-        if (all_small) {
-            count_launches(launches);
-            return cudaGetLastError();
-        }
-    }
-    const int skip = KT > 0 ? std::min(K, KT) : 0;  // the queries k_knn_t did
+    // queries whose packed-key search met a tie, for the exact-key search at the end
     uint32_t* redo = ensure<uint32_t>(c->knn_redo, (size_t)nq, &e);
     if (e) return e;
     if ((e = cudaMemsetAsync(&sc->knn_redo, 0, sizeof(unsigned), c->stream))) return e;
+    int launches = 0;
+    if (KT > 0) {
+        const unsigned tblocks = (unsigned)((nq + KNN_T_THREADS - 1) / KNN_T_THREADS);
+        const size_t smem = (size_t)std::min(K, KT) * KNN_T_THREADS * sizeof(unsigned long long);
+#define PGPU_KNN_T(DD, PT)                                                                                    \
+    k_knn_t<DD><<<tblocks, KNN_T_THREADS, smem, c->stream>>>((const PT*)c->spts.p, perm, grid, tab,            \
+                                                              c->knn_table_n, c->knn_table_r, qs, nq, K, KT, kq, \
+                                                              stride, out, &sc->knn_cand, redo, &sc->knn_redo)
+        if (c->prm.dim == 2) PGPU_KNN_T(2, double2); else PGPU_KNN_T(3, double4);
+#undef PGPU_KNN_T
+        launches++;
+    }
+    if (!all_small) {
+        const int skip = KT > 0 ? std::min(K, KT) : 0;  // the queries k_knn_t did
 #define PGPU_KNN(DD, PT, WW)                                                                                 \
     k_knn<DD, WW><<<blocks, WW * 32, 0, c->stream>>>((const PT*)c->spts.p, perm, grid, tab, c->knn_table_n,     \
                                                       c->knn_table_r, qs, nq, K, kq, stride, out, &sc->knn_cand, \
                                                       skip, redo, &sc->knn_redo)
-    if (c->prm.dim == 2) {
-        if (KW == 2) PGPU_KNN(2, double2, 2); else if (KW == 8) PGPU_KNN(2, double2, 8); else PGPU_KNN(2, double2, 4);
-    } else {
-        if (KW == 2) PGPU_KNN(3, double4, 2); else if (KW == 8) PGPU_KNN(3, double4, 8); else PGPU_KNN(3, double4, 4);
-    }
+        if (c->prm.dim == 2) {
+            if (KW == 2) PGPU_KNN(2, double2, 2); else if (KW == 8) PGPU_KNN(2, double2, 8); else PGPU_KNN(2, double2, 4);
+        } else {
+            if (KW == 2) PGPU_KNN(3, double4, 2); else if (KW == 8) PGPU_KNN(3, double4, 8); else PGPU_KNN(3, double4, 4);
+        }
 #undef PGPU_KNN
+        launches++;
+    }
     // the tied queries again with exact keys: a fixed grid whose warps stride over the
     // device-held list (no read-back of its length)
     const unsigned xblocks = (unsigned)std::min<int64_t>(blocks, 148 * 4);
@@ -733,7 +744,7 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
         if (KW == 2) PGPU_KNNX(3, double4, 2); else if (KW == 8) PGPU_KNNX(3, double4, 8); else PGPU_KNNX(3, double4, 4);
     }
 #undef PGPU_KNNX
-    count_launches(launches + 2);
+    count_launches(launches + 1);
     return cudaGetLastError();
 }
 
