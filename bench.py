@@ -290,7 +290,9 @@ HEADLINE, PLAIN_FORM = "learned_fp32", "plain_fp64"
 # of the clustered 1,048,576-cell case on learned-K lists, used for `traffic`.
 CLIP32_DRAM_BYTES_PER_CELL = (669.431296e6 + 774.266112e6) / 1_048_576
 # and of one k_flux_update launch on the same case (the hydro stage's dominant kernel)
-FLUX_DRAM_BYTES_PER_CELL = (1293.150976e6 + 146.343168e6) / 1_048_576
+FLUX_DRAM_BYTES_PER_CELL = (1545.615360e6 + 212.092160e6) / 1_048_576
+# and of one k_knn launch on the same case (learned budgets), per query
+KNN_DRAM_BYTES_PER_QUERY = (71.634944e6 + 243.834368e6) / 1_048_576
 
 
 def _barrier(dist):
@@ -570,7 +572,9 @@ def run_ours(args, rank, world, local_rank):
     cand = stats["knn_candidates"] / max(n_query, 1)
     ach = n_query * cand * W["knn_flop_per_cand"] / (stage[2] * 1e-3) / 1e12
     roof_knn = {"kernel": "k_knn", "bound": "fp64", "achieved": ach, "peak": fp64.value, "unit": "TFLOP/s",
-                "frac": ach / fp64.value, "traffic": None,
+                "frac": ach / fp64.value, "traffic": KNN_DRAM_BYTES_PER_QUERY * n_query if D == 3 else None,
+                "traffic_note": "DRAM bytes per launch: ncu capture of the clustered 1,048,576-query case "
+                                "(learned budgets) scaled by queries",
                 "peak_source": "FP64 FMA rate measured in this run (pgpu_fp64_peak)",
                 "work": f"{cand:.1f} candidates per query (this run's) x {W['knn_flop_per_cand']} flop x "
                         f"{n_query} queries"}
@@ -587,7 +591,7 @@ def run_ours(args, rank, world, local_rank):
                   "unit": "GB/s", "frac": hyd / hbm,
                   "traffic": FLUX_DRAM_BYTES_PER_CELL * n_query if D == 3 else None,
                   "traffic_note": "k_flux_update DRAM bytes per launch: ncu capture of the clustered 1,048,576-cell "
-                                  "case scaled by cells (1,372 B per cell against 683 compulsory)",
+                                  "case scaled by cells (1,676 B per cell against 683 compulsory)",
                   "work": f"{W['hydro_bytes_per_cell']} compulsory bytes per cell-update"}
 
     cpu = None
