@@ -157,7 +157,9 @@ __device__ __forceinline__ void bitonic_sort32(typename KeyOps<PK>::K& a, int la
             const typename O::K o = O::shfl_xor(a, j);
             const bool up = (lane & k) == 0;
             const bool lower = (lane & j) == 0;
-            const bool take = (lower == up) ? O::lt(o, a) : O::lt(a, o);
+            // packed keys are distinct but for the empty key, so "a < o" is "not o < a" up to
+            // swapping two equal keys: one integer compare per stage
+            const bool take = PK ? (O::lt(o, a) == (lower == up)) : ((lower == up) ? O::lt(o, a) : O::lt(a, o));
             if (take) a = o;
         }
     }
@@ -171,7 +173,7 @@ __device__ __forceinline__ void bitonic_merge32(typename KeyOps<PK>::K& a, int l
     for (int j = 16; j > 0; j >>= 1) {
         const typename O::K o = O::shfl_xor(a, j);
         const bool lower = (lane & j) == 0;
-        const bool take = lower ? O::lt(o, a) : O::lt(a, o);
+        const bool take = PK ? (O::lt(o, a) == lower) : (lower ? O::lt(o, a) : O::lt(a, o));
         if (take) a = o;
     }
 }
