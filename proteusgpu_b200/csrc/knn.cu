@@ -147,11 +147,11 @@ struct WarpKnn<true> {
 };
 
 // Ascending bitonic sort of one key per lane across the warp.
-template <bool PK>
+template <bool PK, int KMAX = 32>
 __device__ __forceinline__ void bitonic_sort32(typename KeyOps<PK>::K& a, int lane) {
     using O = KeyOps<PK>;
 #pragma unroll
-    for (int k = 2; k <= 32; k <<= 1) {
+    for (int k = 2; k <= KMAX; k <<= 1) {
 #pragma unroll
         for (int j = k >> 1; j > 0; j >>= 1) {
             const typename O::K o = O::shfl_xor(a, j);
@@ -186,7 +186,12 @@ __device__ __noinline__ bool merge_queue(WarpKnn<PK>& S, int qn, int nrows, int 
     using O = KeyOps<PK>;
     using K = typename O::K;
     K a = lane < qn ? S.q(lane) : O::none();
-    bitonic_sort32<PK>(a, lane);
+    // at most 16 queued keys: lanes 16-31 hold the empty key, so the first four levels leave
+    // lanes 0-15 ascending and the sequence sorted (the last level would change nothing)
+    if (qn <= 16)
+        bitonic_sort32<PK, 16>(a, lane);
+    else
+        bitonic_sort32<PK>(a, lane);
 #pragma unroll 1
     for (int r = 0; r < nrows; r++) {
         const K qmin = O::shfl(a, 0);
@@ -234,10 +239,11 @@ __device__ __forceinline__ void scan_bins(const typename PointOf<D>::type* __res
         bool valid = tt < total;
         typename O::K key = O::none();
         if (valid) {
+            // after the steps 16 .. 2s, j is a multiple of 2s and at most 32 - 2s, so j + s <= 31
             int j = 0;
 #pragma unroll
             for (int step = 16; step > 0; step >>= 1)
-                if (j + step < 32 && S.b_excl[j + step] <= tt) j += step;
+                if (S.b_excl[j + step] <= tt) j += step;
             const uint32_t sidx = S.b_start[j] + (tt - S.b_excl[j]);
             const uint32_t eid = perm[sidx];
             if (eid == qid) {

@@ -145,3 +145,18 @@ def test_knn_sub_bin_beyond_the_deepest_level():
         assert np.array_equal(at, np.arange(at[0], at[0] + len(at)))  # contiguous: one sub-bin
         assert np.array_equal(perm[at], np.arange(lo, hi))            # ids ascending inside it
     assert np.array_equal(sp, pts[perm])
+
+
+@pytest.mark.parametrize("kt", [0, 64])
+def test_knn_packed_key_ties_are_redone_exactly(kt):
+    """A regular lattice puts exact distance ties everywhere: the packed-key search (warp
+    kernel, or the thread-per-query kernel with kt) flags those queries and the exact-key
+    search redoes them; the lists equal the oracle's, ties by index."""
+    g1 = (np.arange(24) + 0.5) / 24
+    pts = np.ascontiguousarray(np.stack(np.meshgrid(g1, g1, g1, indexing="ij"), -1).reshape(-1, 3))
+    with Context(dim=3, k=40) as ctx:
+        ctx.set_tuning(knn_thread=kt)
+        g = ctx.knn(pts)
+        st = ctx.stats()
+    assert st["knn_redone"] > 0
+    assert np.array_equal(g, om.knn(pts, 40))
