@@ -443,18 +443,32 @@ __global__ void k_mlp_bf16_all(const float* __restrict__ w, uint16_t* __restrict
     if (p < KB_NPARAM) write_bf16(p, w[p], wbf);
 }
 
-template <int D>
+// Features of each query slot's cell.  BY_ID: one thread per hydro cell in hydro-id
+// order (every query is a hydro cell), so that the per-cell arrays indexed by id are read
+// in order and only the sorted position, its query slot and the feature row are
+// scattered; else one thread per query slot.  The values are the same either way.
+template <int D, bool BY_ID>
 __global__ void k_kb_features(const uint32_t* __restrict__ qs, const uint32_t* __restrict__ perm,
+                              const uint32_t* __restrict__ inv, const uint32_t* __restrict__ qoff,
                               const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ bin_start,
                               const uint8_t* __restrict__ lvl, const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst, int64_t nq,
                               int64_t n_hydro, const int* __restrict__ certk,
                               const double* __restrict__ vol, const uint32_t* __restrict__ fcnt,
                               const double* __restrict__ centroid, const double* __restrict__ pos,
                               float* __restrict__ hist_vol, uint8_t* __restrict__ miss, float* __restrict__ feat) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nq) return;
-    const uint32_t s = qs[t];
-    const uint32_t e = perm[s];
+    const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= (BY_ID ? n_hydro : nq)) return;
+    uint32_t s, e;
+    int64_t t;
+    if (BY_ID) {
+        e = (uint32_t)u;
+        s = inv[e];
+        t = qoff ? (int64_t)qoff[s] : (int64_t)s;
+    } else {
+        t = u;
+        s = qs[t];
+        e = perm[s];
+    }
     float f[KB_FEATURES] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
     if (e < (uint32_t)n_hydro) {
         const typename PointOf<D>::type p = spts[s];
@@ -577,20 +591,24 @@ cudaError_t kb_features(pgpu_ctx* c) {
     if (kb.hist_vol.bytes != hv_before && (e = cudaMemsetAsync(hv, 0, (nh + 1) * sizeof(float), c->stream))) return e;
     if (kb.miss.bytes != ms_before && (e = cudaMemsetAsync(ms, 0, nh + 1, c->stream))) return e;
     if (nq == 0) return cudaSuccess;
-    if (c->prm.dim == 2)
-        k_kb_features<2><<<nblk(nq, 256), 256, 0, c->stream>>>(
-            (const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p, (const double2*)c->spts.p,
-            (const uint32_t*)c->bin_start.p, (const uint8_t*)c->bin_lvl.p, (const InstPar*)c->inst.d_par.p,
-            (const uint16_t*)c->inst.d_inst_e.p,
-            nq, nh, (const int*)c->certk.p, (const double*)c->vol.p,
-            (const uint32_t*)c->fcnt.p, (const double*)c->centroid.p, (const double*)c->pos.p, hv, ms, feat);
-    else
-        k_kb_features<3><<<nblk(nq, 256), 256, 0, c->stream>>>(
-            (const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p, (const double4*)c->spts.p,
-            (const uint32_t*)c->bin_start.p, (const uint8_t*)c->bin_lvl.p, (const InstPar*)c->inst.d_par.p,
-            (const uint16_t*)c->inst.d_inst_e.p,
-            nq, nh, (const int*)c->certk.p, (const double*)c->vol.p,
-            (const uint32_t*)c->fcnt.p, (const double*)c->centroid.p, (const double*)c->pos.p, hv, ms, feat);
+    // every query a hydro cell: walk the cells in id order (query slot = the sorted position
+    // when every point is a query, else its rank among the hydro points)
+    const bool by_id = nq == nh;
+    const uint32_t* qoff = (c->all_cells || c->n_ext == nh) ? nullptr : (const uint32_t*)c->qoff.p;
+    const unsigned blocks = nblk(by_id ? nh : nq, 256);
+#define PGPU_KBF(DD, PT, BI)                                                                                  \
+    k_kb_features<DD, BI><<<blocks, 256, 0, c->stream>>>(                                                     \
+        (const uint32_t*)c->qs.p, (const uint32_t*)c->perm.p, (const uint32_t*)c->inv.p, qoff,               \
+        (const PT*)c->spts.p, (const uint32_t*)c->bin_start.p, (const uint8_t*)c->bin_lvl.p,                 \
+        (const InstPar*)c->inst.d_par.p, (const uint16_t*)c->inst.d_inst_e.p, nq, nh, (const int*)c->certk.p, \
+        (const double*)c->vol.p, (const uint32_t*)c->fcnt.p, (const double*)c->centroid.p,                  \
+        (const double*)c->pos.p, hv, ms, feat)
+    if (c->prm.dim == 2) {
+        if (by_id) PGPU_KBF(2, double2, true); else PGPU_KBF(2, double2, false);
+    } else {
+        if (by_id) PGPU_KBF(3, double4, true); else PGPU_KBF(3, double4, false);
+    }
+#undef PGPU_KBF
     count_launches(1);
     return cudaGetLastError();
 }
