@@ -88,6 +88,9 @@ struct WarpCell32 {
             uint32_t stage[MAX_P];
             uint32_t rl[MAX_T];
             unsigned char nxt[MAX_P];
+            float4 sb_eq[32];  // the current batch of neighbour planes (local frame)
+            float sb_d2[32];   // their squared distances to the seed
+            uint32_t sb_z[32]; // their ext ids
         } c;
         struct {  // FP64 extraction
             double4 hp[MAX_P];
@@ -1372,20 +1375,38 @@ __global__ void __launch_bounds__(CW * 32, (D == 3 ? 32 : 28) / CW) k_clip32(Cli
                 cfw = 0.5f * fmaf(cfx, cfx, fmaf(cfy, cfy, cfz * cfz));
                 cd2 = (float)seed_d2(Bc.x, Bc.y, pz(Bc), sx, sy, sz);
             }
+            if constexpr (D == 3) {
+                __syncwarp();
+                W.c.sb_eq[lane] = make_float4(-cfx, -cfy, -cfz, cfw);
+                W.c.sb_d2[lane] = cd2;
+                W.c.sb_z[lane] = zc;
+                __syncwarp();
+            }
         }
-        const uint32_t z = __shfl_sync(FULL, zc, k & 31);
+        uint32_t z;
+        float d2Bf;
+        float4 eq;
+        if constexpr (D == 3) {
+            z = W.c.sb_z[k & 31];
+            d2Bf = W.c.sb_d2[k & 31];
+            eq = W.c.sb_eq[k & 31];
+        } else {
+            z = __shfl_sync(FULL, zc, k & 31);
+            d2Bf = __shfl_sync(FULL, cd2, k & 31);
+            eq = make_float4(-__shfl_sync(FULL, cfx, k & 31), -__shfl_sync(FULL, cfy, k & 31),
+                             -__shfl_sync(FULL, cfz, k & 31), __shfl_sync(FULL, cfw, k & 31));
+        }
         if (z == NO_NEIGHBOR) break;
         k_stop = k + 1;
-        const float d2Bf = __shfl_sync(FULL, cd2, k & 31);
         if (nb_v >= MAX_P) {
             reclip = true;
             break;
         }
-        const float4 eq = make_float4(-__shfl_sync(FULL, cfx, k & 31), -__shfl_sync(FULL, cfy, k & 31),
-                                      -__shfl_sync(FULL, cfz, k & 31), __shfl_sync(FULL, cfw, k & 31));
         const int cur = nb_v;
-        if (lane == 0) hp[cur] = eq;
-        __syncwarp();
+        if constexpr (D == 2) {
+            if (lane == 0) hp[cur] = eq;
+            __syncwarp();
+        }
 
         uint32_t cm[3];
         bool undecided = false;
@@ -1414,6 +1435,10 @@ __global__ void __launch_bounds__(CW * 32, (D == 3 ? 32 : 28) / CW) k_clip32(Cli
             continue;
         }
         k_last = k + 1;
+        if constexpr (D == 3) {  // the plane cuts: it joins the cell's plane list
+            if (lane == 0) hp[cur] = eq;
+            __syncwarp();
+        }
         const int kept = nb_t - nb_r;
         int n_new = 0;
         bool bad = false;
