@@ -445,7 +445,7 @@ static void extract(const cell_t *c, cell_out_t *o) {
     if (dim == 2) o->volume = area_2d((const double (*)[4])vert, c->nb_t, o->centroid);
     o->nf = 0;
     for (int p = 0; p < c->nb_v; p++) {
-        int idx[OM_MAX_T], cnt = 0;
+        int idx[OM_MAX_T] = {0}, cnt = 0;
         for (int i = 0; i < c->nb_t; i++)
             if (refs_plane(c, i, p)) idx[cnt++] = i;
         if (cnt < dim) continue;
