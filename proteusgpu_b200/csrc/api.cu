@@ -1173,9 +1173,9 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
             if (t < bt) bt = t, best.knn_thread = kt;
         }
         c->tune.knn_thread = best.knn_thread;
-        // 3. clipping: a warp per cell with 2 or 4 cells per block, or (2D) a thread per cell
+        // 3. clipping: a warp per cell with 1, 2 or 4 cells per block, or (2D) a thread per cell
         bt = 1e30f;
-        for (int cw : {2, 4}) {
+        for (int cw : {1, 2, 4}) {
             c->tune.clip_warps = cw;
             if ((r = timed_build(c, 0x8, &t))) return r;
             if (t < bt) bt = t, best.clip_warps = cw;
@@ -1209,7 +1209,7 @@ int pgpu_set_tuning(pgpu_ctx* c, const pgpu_tuning* t) {
     int r = check_ctx(c);
     if (r) return r;
     if (!t || !(t->ppb >= 0.5 && t->ppb <= 64.0) || (t->knn_warps != 2 && t->knn_warps != 4 && t->knn_warps != 8) ||
-        (t->clip_warps != 2 && t->clip_warps != 4) ||
+        (t->clip_warps != 1 && t->clip_warps != 2 && t->clip_warps != 4) ||
         (t->knn_thread != 0 && t->knn_thread != 32 && t->knn_thread != 64))
         return fail(c, PGPU_EINVAL, "pgpu_set_tuning: bad launch shapes");
     c->tune.ppb = t->ppb;

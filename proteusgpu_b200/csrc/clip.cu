@@ -1958,7 +1958,7 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
     P.walk_certk = c->prm.k + 1;
     if (nq > 0) {
         const unsigned blocks = (unsigned)((nq + CLIP_WARPS - 1) / CLIP_WARPS);
-        const int CW = c->tune.clip_warps;  // cells (warps) per block: autotuned, 2 or 4
+        const int CW = c->tune.clip_warps;  // cells (warps) per block: autotuned, 1, 2 or 4
         const unsigned blocks_cw = (unsigned)((nq + CW - 1) / CW);
         if (thread2d && D == 2 && !slots) {
             k_clip2t<<<(unsigned)((nq + T2_THREADS - 1) / T2_THREADS), T2_THREADS, 0, c->stream>>>(P);
@@ -1974,19 +1974,25 @@ cudaError_t clip_pass(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, const 
                 k_clip_pruned<3><<<blocks, CLIP_WARPS * 32, 0, c->stream>>>(P, g, tab, c->knn_table_n,
                                                                             c->knn_table_r);
         } else if (fp32) {
+            // one cell per block frees each warp's slot as soon as its own cell is done
+            // (no warp waits for its block mates); the autotuner picks
             if (D == 2) {
-                if (CW == 2) k_clip32<2, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
+                if (CW == 1) k_clip32<2, 1><<<blocks_cw, 32, 0, c->stream>>>(P);
+                else if (CW == 2) k_clip32<2, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
                 else k_clip32<2, 4><<<blocks_cw, 128, 0, c->stream>>>(P);
             } else {
-                if (CW == 2) k_clip32<3, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
+                if (CW == 1) k_clip32<3, 1><<<blocks_cw, 32, 0, c->stream>>>(P);
+                else if (CW == 2) k_clip32<3, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
                 else k_clip32<3, 4><<<blocks_cw, 128, 0, c->stream>>>(P);
             }
         } else {
             if (D == 2) {
-                if (CW == 2) k_clip<2, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
+                if (CW == 1) k_clip<2, 1><<<blocks_cw, 32, 0, c->stream>>>(P);
+                else if (CW == 2) k_clip<2, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
                 else k_clip<2, 4><<<blocks_cw, 128, 0, c->stream>>>(P);
             } else {
-                if (CW == 2) k_clip<3, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
+                if (CW == 1) k_clip<3, 1><<<blocks_cw, 32, 0, c->stream>>>(P);
+                else if (CW == 2) k_clip<3, 2><<<blocks_cw, 64, 0, c->stream>>>(P);
                 else k_clip<3, 4><<<blocks_cw, 128, 0, c->stream>>>(P);
             }
         }

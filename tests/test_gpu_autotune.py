@@ -21,7 +21,7 @@ def test_autotuned_shapes_give_identical_steps(precision):
     ic = ics.sedov_3d(n=25000, seed=12)
     _, ref, mref = _run(ic, False, precision)
     t, got, mgot = _run(ic, True, precision)
-    assert t["ppb"] in (1.5, 2.0, 3.0, 4.0) and t["knn_warps"] in (2, 4, 8) and t["clip_warps"] in (2, 4)
+    assert t["ppb"] in (1.5, 2.0, 3.0, 4.0) and t["knn_warps"] in (2, 4, 8) and t["clip_warps"] in (1, 2, 4)
     assert t["knn_thread"] in (0, 32, 64)
     assert t["ms_tuned"] > 0 and t["ms_default"] > 0
     for a, b in zip(ref, got):
@@ -74,3 +74,18 @@ def test_thread_per_cell_2d_moving_mesh_and_batch():
             outs.append(ctx.sim_get())
     for u, v in zip(*outs):
         assert np.array_equal(u, v)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_clip_block_shapes_change_no_bit(precision):
+    """One, two or four cells (warps) per clipping block give the same 3D mesh bit for bit,
+    with the FP64 and with the FP32 clip."""
+    pts = ics.clustered_3d(n=20000, seed=8).pos
+    meshes = []
+    for cw in (1, 2, 4):
+        with Context(dim=3, k=96, buff=0.1, precision=precision) as ctx:
+            ctx.set_tuning(clip_warps=cw)
+            meshes.append(ctx.compute_periodic_mesh(pts))
+    for m in meshes[1:]:
+        for f in ("status", "cert_k", "face_counts", "neighbor", "normal", "area", "volumes", "centroid", "seeds"):
+            assert np.array_equal(getattr(meshes[0], f), getattr(m, f)), f
