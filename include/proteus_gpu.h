@@ -347,7 +347,7 @@ typedef struct {
     int32_t from_cache;
 } pgpu_tuning;
 int pgpu_autotune(pgpu_ctx *ctx, pgpu_tuning *out);
-/* Sets the launch shapes directly (ppb in [0.5, 64], knn_warps 2/4/8, clip_warps 1/2/4,
+/* Sets the launch shapes directly (ppb in [0.5, 64], knn_warps 1/2/4/8, clip_warps 1/2/4,
  * clip_thread 0/1, knn_thread 0/32/64; the timing fields are ignored). */
 int pgpu_set_tuning(pgpu_ctx *ctx, const pgpu_tuning *t);
 

@@ -1161,7 +1161,7 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
         // 2. KNN block size, then one thread per query for the small K
         bt = 1e30f;
         c->tune.knn_thread = 0;
-        for (int kw : {2, 4, 8}) {
+        for (int kw : {1, 2, 4, 8}) {
             c->tune.knn_warps = kw;
             if ((r = timed_build(c, 0x4, &t))) return r;
             if (t < bt) bt = t, best.knn_warps = kw, best.knn_thread = 0;
@@ -1208,7 +1208,7 @@ int pgpu_autotune(pgpu_ctx* c, pgpu_tuning* out) {
 int pgpu_set_tuning(pgpu_ctx* c, const pgpu_tuning* t) {
     int r = check_ctx(c);
     if (r) return r;
-    if (!t || !(t->ppb >= 0.5 && t->ppb <= 64.0) || (t->knn_warps != 2 && t->knn_warps != 4 && t->knn_warps != 8) ||
+    if (!t || !(t->ppb >= 0.5 && t->ppb <= 64.0) || (t->knn_warps != 1 && t->knn_warps != 2 && t->knn_warps != 4 && t->knn_warps != 8) ||
         (t->clip_warps != 1 && t->clip_warps != 2 && t->clip_warps != 4) ||
         (t->knn_thread != 0 && t->knn_thread != 32 && t->knn_thread != 64))
         return fail(c, PGPU_EINVAL, "pgpu_set_tuning: bad launch shapes");

@@ -466,7 +466,7 @@ __device__ __forceinline__ bool knn_query(const typename PointOf<D>::type* __res
 // 118.4 ms at 16.8M clustered points against 32 warps).  Packed keys; a query with a tie
 // is listed in redo for k_knn_exact.
 template <int D, int KW>
-__global__ void __launch_bounds__(KW * 32, 40 / KW)
+__global__ void __launch_bounds__(KW * 32, KW == 1 ? 32 : 40 / KW)
     k_knn(const typename PointOf<D>::type* __restrict__ spts, const uint32_t* __restrict__ perm, SubGrid grid,
           const int2* __restrict__ table, int table_n, int table_r, const uint32_t* __restrict__ qs, int64_t nq,
           int K, const uint16_t* __restrict__ kq, int stride, uint32_t* __restrict__ out,
@@ -699,7 +699,7 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
     cudaError_t e = cudaSuccess;
     if (c->knn_table_n == 0 && (e = build_knn_table(c))) return e;
     DevScalars* sc = (DevScalars*)c->scalars.p;
-    const int KW = c->tune.knn_warps;  // warps (queries) per block: autotuned, 2, 4 or 8
+    const int KW = c->tune.knn_warps;  // warps (queries) per block: autotuned, 1, 2, 4 or 8
     const int KT = c->tune.knn_thread;  // queries with K <= KT: one thread each (0 = none)
     const bool all_small = KT > 0 && K <= KT;  // K bounds every per-query kq
     const unsigned blocks = (unsigned)((nq + KW - 1) / KW);
@@ -730,10 +730,12 @@ cudaError_t launch_knn_list(pgpu_ctx* c, const uint32_t* qs, int64_t nq, int K, 
     k_knn<DD, WW><<<blocks, WW * 32, 0, c->stream>>>((const PT*)c->spts.p, perm, grid, tab, c->knn_table_n,     \
                                                       c->knn_table_r, qs, nq, K, kq, stride, out, &sc->knn_cand, \
                                                       skip, redo, &sc->knn_redo)
+        // one query per block (at most 32 blocks, so 32 warps, per SM) frees each warp's slot as
+        // soon as its own query is done; two or more allow 40 warps per SM: the autotuner picks
         if (c->prm.dim == 2) {
-            if (KW == 2) PGPU_KNN(2, double2, 2); else if (KW == 8) PGPU_KNN(2, double2, 8); else PGPU_KNN(2, double2, 4);
+            if (KW == 1) PGPU_KNN(2, double2, 1); else if (KW == 2) PGPU_KNN(2, double2, 2); else if (KW == 8) PGPU_KNN(2, double2, 8); else PGPU_KNN(2, double2, 4);
         } else {
-            if (KW == 2) PGPU_KNN(3, double4, 2); else if (KW == 8) PGPU_KNN(3, double4, 8); else PGPU_KNN(3, double4, 4);
+            if (KW == 1) PGPU_KNN(3, double4, 1); else if (KW == 2) PGPU_KNN(3, double4, 2); else if (KW == 8) PGPU_KNN(3, double4, 8); else PGPU_KNN(3, double4, 4);
         }
 #undef PGPU_KNN
         launches++;
