@@ -216,9 +216,11 @@ __device__ __forceinline__ int partner_face(const uint32_t* __restrict__ f_own, 
 
 // 24 warps per SM (at most 85 registers a thread; the HLL arithmetic spills a little):
 // the gathers of the neighbours' states and faces are latency bound, more resident
-// warps hide more of them (16.8M points: 31.4 -> 28.4 ms)
+// warps hide more of them (16.8M points: 31.4 -> 28.4 ms).  Blocks of two warps, so that
+// a block's slot is free again soon after its own slowest cell (23.7 -> 23.1 ms).
+constexpr int FT = 64;  // flux threads per block
 template <int D, bool PHYSICAL, int MIRROR>
-__global__ void __launch_bounds__(HT, 3) k_flux_update(const double4* __restrict__ w4, const double* __restrict__ we,
+__global__ void __launch_bounds__(FT, 12) k_flux_update(const double4* __restrict__ w4, const double* __restrict__ we,
                               const uint32_t* __restrict__ fptr, const uint32_t* __restrict__ fcnt,
                               const uint32_t* __restrict__ f_own, const double4* __restrict__ f_geo, int64_t n,
                               const InstPar* __restrict__ ip, const uint16_t* __restrict__ inst,
@@ -226,7 +228,7 @@ __global__ void __launch_bounds__(HT, 3) k_flux_update(const double4* __restrict
                               double* __restrict__ mass, double* __restrict__ mom, double* __restrict__ en,
                               double* __restrict__ pos, DevScalars* __restrict__ sc,
                               const uint32_t* __restrict__ order, const uint32_t* __restrict__ perm) {
-    const int64_t t = (int64_t)blockIdx.x * HT + threadIdx.x;
+    const int64_t t = (int64_t)blockIdx.x * FT + threadIdx.x;
     if (t >= n) return;
     // cells in the mesh's spatial order when given (the query list: sorted positions of
     // the hydro cells): neighbouring threads then read neighbouring faces and share
@@ -795,7 +797,7 @@ cudaError_t launch_flux_update(pgpu_ctx* c, double fixed_dt) {
     for (const auto& q : c->inst.par)
         if (q.mirror != c->inst.par[0].mirror) mir = 2;
 #define PGPU_FLUX(DD, PH, MI)                                                                                     \
-    k_flux_update<DD, PH, MI><<<nblk(n, HT), HT, 0, c->stream>>>(                                                \
+    k_flux_update<DD, PH, MI><<<nblk(n, FT), FT, 0, c->stream>>>(                                                \
         (const double4*)c->w4.p, (const double*)c->we.p, (const uint32_t*)c->fptr.p, (const uint32_t*)c->fcnt.p, \
         (const uint32_t*)c->f_own.p, (const double4*)c->f_geo.p, n, (const InstPar*)c->inst.d_par.p,              \
         (const uint16_t*)c->inst.d_inst_h.p, (const unsigned long long*)c->inst.d_dt.p, fixed_dt,                 \
