@@ -327,8 +327,8 @@ int pgpu_batch_dt(pgpu_ctx *ctx, double *dt_per_instance);
 /* -------------------------------------------------------- autotuner ---
  * Extension.  Times mesh builds of the current simulation state (nothing
  * advances) and picks the coarse grid's mean points per bin (1.5, 2, 3, 4), the
- * KNN block size (2, 4, 8 queries; or one thread per query for the queries whose
- * K is at most 32 or 64) and the clipping block size (2, 4 cells; in 2D
+ * KNN block size (1, 2, 4, 8 queries; or one thread per query for the queries whose
+ * K is at most 32 or 64) and the clipping block size (1, 2, 4 cells; in 2D
  * also one thread per cell instead of one warp), one
  * after the other; the choice is cached for the process by (dim, log2 n, batch,
  * precision, learned K, k) and reused without timing.  The block sizes and the
