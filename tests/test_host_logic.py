@@ -141,3 +141,72 @@ def test_packed_knn_keys_flag_every_tie_that_could_change_a_list():
         flagged += tie
         assert tie or got == exact, (trial, K, n)
     assert 0 < flagged < 800  # the adversarial inputs do raise flags; uniform ones mostly not
+
+
+def _packed_insertion_search(cands, K):
+    """Host model of the thread-per-query KNN (knn.cu k_knn_t): a sorted list of exactly K
+    packed keys kept by insertion, with its tie rule."""
+    none = (1 << 64) - 1
+    lst, thr, tie = [], none, False
+    for d, i in cands:
+        k = (_f32_up_bits(d) << 32) | i
+        if not k < thr:
+            if thr != none and (k >> 32) == (thr >> 32):
+                tie = True
+            continue
+        out = lst[K - 1] if len(lst) == K else none
+        lst = sorted(lst + [k])[:K]
+        if len(lst) == K:
+            thr = lst[K - 1]
+            if out != none and (out >> 32) == (thr >> 32):
+                tie = True
+    for a, b in zip(lst, lst[1:]):
+        if (a >> 32) == (b >> 32):
+            tie = True
+    return [x & 0xFFFFFFFF for x in lst] + [0xFFFFFFFF] * (K - len(lst)), tie
+
+
+def test_packed_knn_keys_insertion_list_flags_every_tie():
+    """The same guarantee for the thread-per-query kernel's list of exactly K."""
+    rng = np.random.default_rng(11)
+    flagged = 0
+    for trial in range(800):
+        K, n = int(rng.integers(1, 64)), int(rng.integers(1, 200))
+        if trial % 5 == 4 and K >= 2:
+            # the nearer of a tied pair (larger id) is held as the K-th, then pushed out by a
+            # nearer key while the farther one (smaller id) stays: only the eviction rule sees it
+            d = np.sort(rng.uniform(0.1, 1.0, K + 1))
+            d[K] = d[K - 1] * (1 + 1e-9)
+            ids = rng.permutation(10 * (K + 1))[:K + 1]
+            a, b = (float(d[K - 1]), int(max(ids[K - 1], ids[K]))), (float(d[K]), int(min(ids[K - 1], ids[K])))
+            rest = [(float(d[j]), int(ids[j])) for j in range(K - 1)]
+            cands = rest[:-1] + [a, b] + rest[-1:]
+            exact = [i for _, i in sorted(cands)[:K]]
+            got, tie = _packed_insertion_search(cands, K)
+            flagged += tie
+            assert tie or got == exact, (trial, K)
+            continue
+        if trial % 4 == 0:
+            d = rng.uniform(0.0, 1.0, n)
+        elif trial % 4 == 1:
+            base = np.repeat(rng.uniform(0.1, 1.0, n // 6 + 1), 6)[:n]
+            d = base * (1 + rng.integers(0, 4, n) * 2e-17 + rng.integers(0, 3, n) * 3e-9)
+        elif trial % 4 == 2:
+            d = rng.integers(0, 15, n) * 0.01
+        else:
+            n = max(n, K + 2)
+            d = np.sort(rng.uniform(0.1, 1.0, n))
+            d[K] = d[K - 1] * (1 + 1e-9)
+        ids = rng.permutation(10 * n)[:n]
+        cands = list(zip(d.tolist(), ids.tolist()))
+        order = np.argsort(d + rng.uniform(0.0, 0.3, n))
+        if trial % 4 == 3:
+            cands[K - 1], cands[K] = (d[K - 1], int(max(ids[K - 1], ids[K]))), (d[K], int(min(ids[K - 1], ids[K])))
+            order = np.array([j for j in np.argsort(d) if j != K - 1] + [K - 1])
+        cands = [cands[j] for j in order]
+        exact = [i for _, i in sorted(cands)[:K]]
+        exact += [0xFFFFFFFF] * (K - len(exact))
+        got, tie = _packed_insertion_search(cands, K)
+        flagged += tie
+        assert tie or got == exact, (trial, K, n)
+    assert 0 < flagged < 800
