@@ -1290,9 +1290,11 @@ __device__ __forceinline__ double4 plane64(int p, int vid, const typename PointO
 }
 
 // Resident warps per SM: 32 in 3D (64 registers a thread, 6.9 KB of shared memory a
-// warp: the overlaid cell), 28 in 2D (72 registers, 7.8 KB).
+// warp: the overlaid cell), 28 in 2D (72 registers, 7.8 KB).  One cell per block: 28
+// one-warp blocks fit an SM's shared memory (each block also reserves 1 KB), so the
+// registers are set for 28 (72 a thread, nearly no spills).
 template <int D, int CW>
-__global__ void __launch_bounds__(CW * 32, (D == 3 ? 32 : 28) / CW) k_clip32(ClipParams P) {
+__global__ void __launch_bounds__(CW * 32, CW == 1 ? 28 : (D == 3 ? 32 : 28) / CW) k_clip32(ClipParams P) {
     using PT = typename PointOf<D>::type;
     using Cell = typename std::conditional<D == 3, WarpCell32, WarpCell>::type;
     __shared__ Cell cells[CW];
