@@ -352,8 +352,12 @@ def time_form(args, cfg, ic, local_rank, dist, form, want_e2e=False, want_clocks
                   gamma=1.4 if batch else ic.gamma, device=local_rank, precision=spec["precision"],
                   predicates="robust" if batch else "reference")
     if spec["kbudget"]:
-        # the warm-up steps but the last train the proposal; the last one already uses it
-        ctx.kbudget_enable(train_steps=max(1, args.warmup - 1), iters_per_step=256, quantile=0.98, seed=1)
+        # the warm-up steps but the last train the proposal; the last one already uses it.  The
+        # class is the smallest whose predicted probability mass reaches the quantile: 0.9 in 3D
+        # (16.8M clustered points: mean K 59, 0.30 % misses, 410 ms a step; 0.98: mean K 66,
+        # 0.28 %, 418 ms), 0.98 in 2D
+        q = 0.9 if cfg["dim"] == 3 else 0.98
+        ctx.kbudget_enable(train_steps=max(1, args.warmup - 1), iters_per_step=256, quantile=q, seed=1)
     # the initial condition is generated on the device (pgpu_sim_init_ic / pgpu_batch_init_ic):
     # the same arrays, bit for bit, as proteusgpu_b200/ics.py builds on the host
     if batch:
